@@ -1,0 +1,278 @@
+"""TEST INFRASTRUCTURE: the CPU checkers of the solve phase.
+
+Two libraries, both built by oracle/Makefile:
+  * `Ref`  -- the apxchol reference's own CPU solve phase (cpu_solver +
+    omp_sptrsv, src/solve.cpp and include/apxchol/solver/sptrsv/omp.h),
+    compiled unchanged from its sources into _ref/libapxref.so;
+  * `Oracle` -- the plain-C restatement in apxoracle.c, pinned byte-for-byte
+    against `Ref` by tests/test_oracle_pin.py.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this package; the CUDA product never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+REF_LIB = os.path.join(_HERE, "_ref", "libapxref.so")
+ORACLE_LIB = os.path.join(_HERE, "_build", "liboracle.so")
+
+c_p = ctypes.c_void_p
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+def build(ref_root: str = "/root/reference") -> None:
+    import subprocess
+    targets = ["oracle"] + (["ref"] if os.path.isdir(ref_root) else [])
+    subprocess.check_call(["make", "-s", "-C", _HERE, f"REF={ref_root}"] + targets)
+
+
+# --------------------------------------------------------------------- reference
+
+_ref = None
+
+
+def _load_ref():
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_LIB):
+            raise RuntimeError(f"reference CPU library missing: {REF_LIB}")
+        lib = ctypes.CDLL(REF_LIB)
+        lib.apxref_last_error.restype = ctypes.c_char_p
+        lib.apxref_set_threads.argtypes = [ctypes.c_int]
+        lib.apxref_solver_create.argtypes = [ctypes.c_int, c_p, c_p, c_p, c_p, c_p, c_p, c_p,
+                                             ctypes.c_int, c_p, ctypes.c_uint32, ctypes.c_int,
+                                             ctypes.POINTER(c_p)]
+        lib.apxref_solver_free.argtypes = [c_p]
+        lib.apxref_solve.argtypes = [c_p, c_p, c_p, ctypes.c_double, ctypes.c_int, c_p, c_p, c_p]
+        lib.apxref_apply.argtypes = [c_p, c_p, c_p, ctypes.c_int]
+        lib.apxref_apply_fused.argtypes = [c_p, c_p, ctypes.c_double, c_p, ctypes.c_int]
+        lib.apxref_apply_fused.restype = ctypes.c_double
+        lib.apxref_forward.argtypes = [c_p, c_p, c_p]
+        lib.apxref_transpose.argtypes = [c_p, c_p, c_p]
+        lib.apxref_pair_seconds.argtypes = [c_p, c_p, c_p, c_p, ctypes.c_int]
+        lib.apxref_pair_seconds.restype = ctypes.c_double
+        lib.apxref_sptrsv_info.argtypes = [c_p, c_p, c_p, c_p, c_p]
+        lib.apxref_sptrsv_arrays.argtypes = [c_p] * 7
+        lib.apxref_level_sizes.argtypes = [c_p, ctypes.c_int, c_p]
+        _ref = lib
+    return _ref
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+def set_threads(t: int) -> int:
+    return _load_ref().apxref_set_threads(t)
+
+
+class Ref:
+    """The reference cpu_solver built on a given factor (cpu_solver(L, F),
+    src/solve.cpp:295-318)."""
+
+    def __init__(self, mat, fac):
+        lib = _load_ref()
+        self.lib = lib
+        self.n = mat.n
+        self._keep = [np.ascontiguousarray(a) for a in
+                      (mat.colptr, mat.rowidx, mat.vals, fac.colptr, fac.rowidx, fac.vals, fac.perm,
+                       fac.rounds)]
+        a_p, a_i, a_v, f_p, f_i, f_v, perm, rounds = self._keep
+        h = c_p()
+        rc = lib.apxref_solver_create(mat.n, _ptr(a_p), _ptr(a_i), _ptr(a_v), _ptr(f_p), _ptr(f_i),
+                                      _ptr(f_v), _ptr(perm), int(fac.sddm),
+                                      _ptr(rounds) if rounds.size else None, rounds.size, 0,
+                                      ctypes.byref(h))
+        if rc != 0:
+            raise RuntimeError("reference cpu_solver failed: " + lib.apxref_last_error().decode())
+        self.h = h
+        m = ctypes.c_uint32(); nnz = ctypes.c_uint64(); fl = ctypes.c_int(); bl = ctypes.c_int()
+        lib.apxref_sptrsv_info(h, ctypes.byref(m), ctypes.byref(nnz), ctypes.byref(fl), ctypes.byref(bl))
+        self.m, self.nnz_stored, self.fwd_levels, self.bck_levels = m.value, nnz.value, fl.value, bl.value
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.apxref_solver_free(self.h)
+            self.h = None
+
+    def solve(self, b, tol=1e-8, max_iter=500):
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.empty(self.n)
+        it = ctypes.c_int(); res = ctypes.c_double(); secs = ctypes.c_double()
+        rc = self.lib.apxref_solve(self.h, _ptr(b), _ptr(x), tol, max_iter, ctypes.byref(it),
+                                   ctypes.byref(res), ctypes.byref(secs))
+        if rc != 0:
+            raise RuntimeError(self.lib.apxref_last_error().decode())
+        return x, it.value, res.value, secs.value
+
+    def apply(self, r, reset=True):
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.empty(self.n)
+        self.lib.apxref_apply(self.h, _ptr(r), _ptr(z), int(reset))
+        return z
+
+    def apply_fused(self, r, r_sum, reset=True):
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.empty(self.n)
+        rz = self.lib.apxref_apply_fused(self.h, _ptr(r), float(r_sum), _ptr(z), int(reset))
+        return z, rz
+
+    def forward(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(self.m)
+        self.lib.apxref_forward(self.h, _ptr(x), _ptr(y))
+        return y
+
+    def transpose(self, y):
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        z = np.empty(self.m)
+        self.lib.apxref_transpose(self.h, _ptr(y), _ptr(z))
+        return z
+
+    def pair_seconds(self, x, reps=5):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        t = np.empty(self.m); z = np.empty(self.m)
+        return self.lib.apxref_pair_seconds(self.h, _ptr(x), _ptr(t), _ptr(z), reps)
+
+    def arrays(self):
+        m, nnz = self.m, self.nnz_stored
+        out = dict(csr_ptr=np.empty(m + 1, np.uint32), csr_idx=np.empty(nnz, np.uint32),
+                   csr_val=np.empty(nnz, np.float32), csc_ptr=np.empty(m + 1, np.uint32),
+                   csc_idx=np.empty(nnz, np.uint32), csc_val=np.empty(nnz, np.float32))
+        self.lib.apxref_sptrsv_arrays(self.h, *[_ptr(out[k]) for k in
+                                                ("csr_ptr", "csr_idx", "csr_val", "csc_ptr", "csc_idx", "csc_val")])
+        return out
+
+    def level_sizes(self, fwd=True):
+        s = np.empty(self.fwd_levels if fwd else self.bck_levels, np.int32)
+        self.lib.apxref_level_sizes(self.h, int(fwd), _ptr(s))
+        return s
+
+
+# --------------------------------------------------------------------- restatement
+
+_ora = None
+
+
+class _System(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_uint32), ("a_ptr", c_p), ("a_idx", c_p), ("a_val", c_p),
+                ("m", ctypes.c_uint32), ("sddm", ctypes.c_int32), ("perm", c_p),
+                ("csr_ptr", c_p), ("csr_idx", c_p), ("csr_val", c_p),
+                ("csc_ptr", c_p), ("csc_idx", c_p), ("csc_val", c_p),
+                ("fwd_thin", c_p), ("bck_thin", c_p),
+                ("nt", ctypes.c_int32), ("center_k", ctypes.c_int32), ("apply_count", ctypes.c_uint64)]
+
+
+def _load_oracle():
+    global _ora
+    if _ora is None:
+        if not os.path.exists(ORACLE_LIB):
+            raise RuntimeError(f"oracle library missing: {ORACLE_LIB}")
+        lib = ctypes.CDLL(ORACLE_LIB)
+        lib.ora_prepare.restype = ctypes.c_int64
+        lib.ora_prepare.argtypes = [ctypes.c_uint32, ctypes.c_uint32, c_p, c_p, c_p, ctypes.c_double] + [c_p] * 6
+        lib.ora_levels.restype = ctypes.c_int32
+        lib.ora_levels.argtypes = [ctypes.c_uint32, c_p, c_p, c_p, c_p, c_p, ctypes.c_uint32, c_p, c_p, c_p]
+        lib.ora_thin_flags.argtypes = [ctypes.c_uint32, c_p, ctypes.c_int32, ctypes.c_uint32, c_p]
+        lib.ora_sweep.argtypes = [ctypes.c_int, ctypes.c_uint32, c_p, c_p, c_p, c_p, c_p, c_p]
+        lib.ora_apply_core.restype = ctypes.c_double
+        lib.ora_apply_core.argtypes = [ctypes.POINTER(_System), c_p, ctypes.c_double, ctypes.c_int, c_p, ctypes.c_int]
+        lib.ora_apply_fused.restype = ctypes.c_double
+        lib.ora_apply_fused.argtypes = [ctypes.POINTER(_System), c_p, ctypes.c_double, c_p]
+        lib.ora_apply.argtypes = [ctypes.POINTER(_System), c_p, c_p]
+        lib.ora_pcg.argtypes = [ctypes.POINTER(_System), c_p, ctypes.c_double, ctypes.c_int, c_p, c_p, c_p]
+        _ora = lib
+    return _ora
+
+
+THIN_THRESHOLD = 1024   # kSpTRSVOMPThreshold, include/apxchol/solver/sptrsv/omp.h:32
+DROP_REL = 1e-4         # kFactorDropRelDefault, include/apxchol/solver/sptrsv/factor_drop.h:70
+
+
+def prepare(fac, rel=DROP_REL):
+    """Host prep + levels + per-row sum modes, as the reference's omp_sptrsv."""
+    lib = _load_oracle()
+    n, m = fac.n, fac.m
+    cap = max(fac.nnz, 1)
+    a = dict(csr_ptr=np.empty(m + 1, np.uint32), csr_idx=np.empty(cap, np.uint32),
+             csr_val=np.empty(cap, np.float32), csc_ptr=np.empty(m + 1, np.uint32),
+             csc_idx=np.empty(cap, np.uint32), csc_val=np.empty(cap, np.float32))
+    nnz = lib.ora_prepare(n, m, _ptr(fac.colptr), _ptr(fac.rowidx), _ptr(fac.vals), rel,
+                          *[_ptr(a[k]) for k in ("csr_ptr", "csr_idx", "csr_val", "csc_ptr", "csc_idx", "csc_val")])
+    if nnz < 0:
+        raise ValueError("malformed factor")
+    for k in ("csr_idx", "csr_val", "csc_idx", "csc_val"):
+        a[k] = a[k][:nnz].copy()
+    fl = np.zeros(m, np.int32); bl = np.zeros(m, np.int32); nb = ctypes.c_int32()
+    rounds = np.ascontiguousarray(fac.rounds, dtype=np.uint64)
+    nf = lib.ora_levels(m, _ptr(a["csr_ptr"]), _ptr(a["csr_idx"]), _ptr(a["csc_ptr"]), _ptr(a["csc_idx"]),
+                        _ptr(rounds) if rounds.size else None, rounds.size, _ptr(fl), _ptr(bl), ctypes.byref(nb))
+    a["fwd_level"], a["bck_level"], a["n_fwd_levels"], a["n_bck_levels"] = fl, bl, nf, nb.value
+    a["fwd_thin"] = np.empty(m, np.uint8); a["bck_thin"] = np.empty(m, np.uint8)
+    lib.ora_thin_flags(m, _ptr(fl), nf, THIN_THRESHOLD, _ptr(a["fwd_thin"]))
+    lib.ora_thin_flags(m, _ptr(bl), nb.value, THIN_THRESHOLD, _ptr(a["bck_thin"]))
+    a["nnz"] = int(nnz)
+    return a
+
+
+class Oracle:
+    """The C restatement over one (matrix, factor) pair."""
+
+    def __init__(self, mat, fac, nt=1, center_k=10, prep=None):
+        self.lib = _load_oracle()
+        self.n, self.m, self.sddm = mat.n, fac.m, fac.sddm
+        self.p = prep if prep is not None else prepare(fac)
+        self._keep = [np.ascontiguousarray(mat.colptr, np.int32), np.ascontiguousarray(mat.rowidx, np.int32),
+                      np.ascontiguousarray(mat.vals, np.float64), np.ascontiguousarray(fac.perm, np.uint32)]
+        a_p, a_i, a_v, perm = self._keep
+        p = self.p
+        self.s = _System(mat.n, _ptr(a_p), _ptr(a_i), _ptr(a_v), fac.m, int(fac.sddm), _ptr(perm),
+                         _ptr(p["csr_ptr"]), _ptr(p["csr_idx"]), _ptr(p["csr_val"]),
+                         _ptr(p["csc_ptr"]), _ptr(p["csc_idx"]), _ptr(p["csc_val"]),
+                         _ptr(p["fwd_thin"]), _ptr(p["bck_thin"]), nt, center_k, 0)
+
+    def sweep(self, direction, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(self.m)
+        p = self.p
+        if direction == 0:
+            self.lib.ora_sweep(0, self.m, _ptr(p["csr_ptr"]), _ptr(p["csr_idx"]), _ptr(p["csr_val"]),
+                               _ptr(p["fwd_thin"]), _ptr(x), _ptr(y))
+        else:
+            self.lib.ora_sweep(1, self.m, _ptr(p["csc_ptr"]), _ptr(p["csc_idx"]), _ptr(p["csc_val"]),
+                               _ptr(p["bck_thin"]), _ptr(x), _ptr(y))
+        return y
+
+    def pair(self, x):
+        return self.sweep(1, self.sweep(0, x))
+
+    def apply(self, r, reset=True):
+        if reset:
+            self.s.apply_count = 0
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.empty(self.n)
+        self.lib.ora_apply(ctypes.byref(self.s), _ptr(r), _ptr(z))
+        return z
+
+    def apply_fused(self, r, r_sum, reset=True):
+        if reset:
+            self.s.apply_count = 0
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.empty(self.n)
+        rz = self.lib.ora_apply_fused(ctypes.byref(self.s), _ptr(r), float(r_sum), _ptr(z))
+        return z, rz
+
+    def solve(self, b, tol=1e-8, max_iter=500):
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.empty(self.n)
+        it = ctypes.c_int(); res = ctypes.c_double()
+        self.lib.ora_pcg(ctypes.byref(self.s), _ptr(b), tol, max_iter, _ptr(x), ctypes.byref(it), ctypes.byref(res))
+        return x, it.value, res.value
