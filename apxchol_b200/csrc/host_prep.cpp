@@ -1,0 +1,219 @@
+// Host-side factor preparation; see host_prep.hpp for the contract.
+#include "host_prep.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+namespace apxb {
+
+namespace {
+
+// Per-column scale: max |off-diagonal| over [first+1, last) in double,
+// stored fp32; 1.0f when the column has none (factor_drop.h:90-96).
+float column_scale(const float* v, uint32_t first, uint32_t last) {
+    double mx = 0.0;
+    for (uint32_t p = first + 1; p < last; ++p) mx = std::max(mx, std::fabs(static_cast<double>(v[p])));
+    return mx > 0.0 ? static_cast<float>(mx) : 1.0f;
+}
+
+// fp32 storage keep rule (omp.h:476-481): |v| >= rel*s and v != 0.
+bool keep_offdiag(float v, float s, double rel) {
+    return std::fabs(static_cast<double>(v)) >= rel * static_cast<double>(s) && v != 0.0f;
+}
+
+void level_bits(const std::vector<int32_t>& level, int32_t n_levels, std::vector<uint32_t>& bits) {
+    std::vector<uint32_t> cnt(static_cast<size_t>(n_levels) + 1, 0);
+    for (int32_t l : level) cnt[l]++;
+    bits.assign((level.size() + 31) / 32, 0u);
+    for (size_t r = 0; r < level.size(); ++r)
+        if (cnt[level[r]] <= kThinLevelRows) bits[r >> 5] |= 1u << (r & 31);
+}
+
+}  // namespace
+
+std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* rowidx, const float* vals,
+                           const uint32_t* perm, bool sddm, const uint64_t* rounds, uint32_t n_rounds,
+                           double drop_rel, prepared_factor& out) {
+    if (n == 0) return "empty factor";
+    if (!sddm && n < 2) return "a Laplacian factor needs n >= 2";
+    const uint32_t m = sddm ? n : n - 1;
+    out = prepared_factor{};
+    out.n = n; out.m = m; out.sddm = sddm;
+    const double rel = drop_rel < 0.0 ? kDropRelDefault : drop_rel;
+
+    // Validate the storage contract: colptr monotone, each column starts
+    // with its diagonal, rows strictly ascending and < n.
+    if (colptr[0] != 0) return "colptr[0] != 0";
+    for (uint32_t j = 0; j < n; ++j) {
+        const uint32_t b = colptr[j], e = colptr[j + 1];
+        if (e <= b) return "column " + std::to_string(j) + " is empty (no diagonal)";
+        if (rowidx[b] != j) return "column " + std::to_string(j) + " does not start with its diagonal";
+        for (uint32_t p = b + 1; p < e; ++p)
+            if (rowidx[p] <= rowidx[p - 1] || rowidx[p] >= n)
+                return "column " + std::to_string(j) + " rows not ascending / out of range";
+        if (!(vals[b] > 0.0f) || !std::isfinite(vals[b]))
+            return "column " + std::to_string(j) + " has a non-positive or non-finite diagonal";
+    }
+
+    // L11 (drop row n-1 for a Laplacian), then the compacting drop, written
+    // straight into the CSC arrays.
+    std::vector<uint32_t>& cp = out.csc_ptr;
+    std::vector<uint32_t>& ci = out.csc_idx;
+    std::vector<float>& cv = out.csc_val;
+    cp.assign(static_cast<size_t>(m) + 1, 0);
+    ci.reserve(colptr[m]);
+    cv.reserve(colptr[m]);
+    std::vector<uint32_t> rows;
+    std::vector<float> vs;
+    uint64_t nnz_factor = 0, dropped = 0;
+    for (uint32_t j = 0; j < m; ++j) {
+        rows.clear(); vs.clear();
+        for (uint32_t p = colptr[j]; p < colptr[j + 1]; ++p) {
+            if (!sddm && rowidx[p] == n - 1) continue;
+            rows.push_back(rowidx[p]); vs.push_back(vals[p]);
+        }
+        nnz_factor += rows.size();
+        if (rel > 0.0) {
+            const float s = column_scale(vs.data(), 0, static_cast<uint32_t>(vs.size()));
+            double dropped_sum = 0.0, kept_abs = 0.0;
+            const size_t first = ci.size();
+            for (size_t t = 0; t < rows.size(); ++t) {
+                const float v = vs[t];
+                if (rows[t] != j) {
+                    if (!keep_offdiag(v, s, rel)) { dropped_sum += static_cast<double>(v); ++dropped; continue; }
+                    kept_abs += std::fabs(static_cast<double>(v));
+                }
+                ci.push_back(rows[t]); cv.push_back(v);
+            }
+            if (dropped_sum != 0.0 && kept_abs > 0.0) {
+                const double per_abs = dropped_sum / kept_abs;
+                for (size_t q = first; q < ci.size(); ++q) {
+                    if (ci[q] == j) continue;
+                    const double v = static_cast<double>(cv[q]);
+                    cv[q] = static_cast<float>(v + per_abs * std::fabs(v));
+                }
+            }
+        } else {
+            ci.insert(ci.end(), rows.begin(), rows.end());
+            cv.insert(cv.end(), vs.begin(), vs.end());
+        }
+        cp[j + 1] = static_cast<uint32_t>(ci.size());
+    }
+    out.nnz_factor = nnz_factor;
+    out.nnz_stored = ci.size();
+    out.dropped = dropped;
+
+    // CSR by the column-order scatter: columns ascend within each row.
+    const uint64_t nnz = ci.size();
+    out.csr_ptr.assign(static_cast<size_t>(m) + 1, 0);
+    for (uint64_t p = 0; p < nnz; ++p) out.csr_ptr[ci[p] + 1]++;
+    for (uint32_t i = 0; i < m; ++i) out.csr_ptr[i + 1] += out.csr_ptr[i];
+    out.csr_idx.resize(nnz);
+    out.csr_val.resize(nnz);
+    {
+        std::vector<uint32_t> cur(out.csr_ptr.begin(), out.csr_ptr.end() - 1);
+        for (uint32_t j = 0; j < m; ++j)
+            for (uint32_t p = cp[j]; p < cp[j + 1]; ++p) {
+                const uint32_t slot = cur[ci[p]]++;
+                out.csr_idx[slot] = j;
+                out.csr_val[slot] = cv[p];
+            }
+    }
+
+    // Levels: round-as-level when the round bounds fit (omp.h:880-932), with
+    // the bounds built as apx_cholesky::install_factor does
+    // (preconditioner.h:247-258); else topological depths.
+    std::vector<int32_t> fl(m), bl(m);
+    bool done = false;
+    if (n_rounds > 0) {
+        std::vector<uint64_t> b(static_cast<size_t>(n_rounds) + 1, 0);
+        uint64_t acc = 0;
+        for (uint32_t r = 0; r < n_rounds; ++r) {
+            acc += rounds[r];
+            if (acc > m) acc = m;
+            b[r + 1] = acc;
+        }
+        const uint64_t last = b[n_rounds];
+        int32_t maxd = 0;
+        uint32_t r = 0;
+        for (uint32_t c = 0; c < m; ++c) {
+            int32_t d;
+            if (c >= last) {
+                d = static_cast<int32_t>(n_rounds + (c - last));
+            } else {
+                while (r + 1 < n_rounds + 1 && c >= b[r + 1]) ++r;
+                d = static_cast<int32_t>(r);
+            }
+            fl[c] = d;
+            maxd = std::max(maxd, d);
+        }
+        for (uint32_t c = 0; c < m; ++c) bl[c] = maxd - fl[c];
+        out.fwd_levels = out.bck_levels = maxd + 1;
+        done = true;
+    }
+    if (!done) {
+        int32_t maxf = 0, maxb = 0;
+        for (uint32_t i = 0; i < m; ++i) {
+            int32_t d = 0;
+            for (uint32_t p = out.csr_ptr[i]; p + 1 < out.csr_ptr[i + 1]; ++p) d = std::max(d, fl[out.csr_idx[p]] + 1);
+            fl[i] = d;
+            maxf = std::max(maxf, d);
+        }
+        for (uint32_t j = m; j-- > 0;) {
+            int32_t d = 0;
+            for (uint32_t p = cp[j]; p < cp[j + 1]; ++p)
+                if (ci[p] > j) d = std::max(d, bl[ci[p]] + 1);
+            bl[j] = d;
+            maxb = std::max(maxb, d);
+        }
+        out.fwd_levels = maxf + 1;
+        out.bck_levels = maxb + 1;
+    }
+    level_bits(fl, out.fwd_levels, out.fwd_thin_bits);
+    level_bits(bl, out.bck_levels, out.bck_thin_bits);
+
+    // Permutation: must be a bijection of [0, n).
+    out.perm.assign(perm, perm + n);
+    {
+        std::vector<uint8_t> seen(n, 0);
+        for (uint32_t v = 0; v < n; ++v) {
+            if (perm[v] >= n || seen[perm[v]]) return "perm is not a permutation of [0, n)";
+            seen[perm[v]] = 1;
+        }
+    }
+    return {};
+}
+
+std::string permute_operator(uint32_t n, const int32_t* colptr, const int32_t* rowidx, const double* vals,
+                             const uint32_t* perm, std::vector<int32_t>& ptr, std::vector<int32_t>& idx,
+                             std::vector<double>& val) {
+    if (colptr[0] != 0) return "operator colptr[0] != 0";
+    const int64_t nnz = colptr[n];
+    if (nnz < 0 || nnz > INT32_MAX) return "operator nnz out of the int32 range";
+    // A is symmetric, so its CSC column j is its CSR row j. Row perm[j] of
+    // P A P^T holds the entries of row j with columns mapped through perm.
+    ptr.assign(static_cast<size_t>(n) + 1, 0);
+    for (uint32_t j = 0; j < n; ++j) {
+        if (colptr[j + 1] < colptr[j]) return "operator colptr not monotone";
+        ptr[perm[j] + 1] = colptr[j + 1] - colptr[j];
+    }
+    for (uint32_t i = 0; i < n; ++i) ptr[i + 1] += ptr[i];
+    idx.resize(nnz);
+    val.resize(nnz);
+    std::vector<std::pair<int32_t, double>> row;
+    for (uint32_t j = 0; j < n; ++j) {
+        row.clear();
+        for (int32_t p = colptr[j]; p < colptr[j + 1]; ++p) {
+            const int32_t r = rowidx[p];
+            if (r < 0 || static_cast<uint32_t>(r) >= n) return "operator row index out of range";
+            row.emplace_back(static_cast<int32_t>(perm[r]), vals[p]);
+        }
+        std::sort(row.begin(), row.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+        int32_t o = ptr[perm[j]];
+        for (const auto& [c, v] : row) { idx[o] = c; val[o] = v; ++o; }
+    }
+    return {};
+}
+
+}  // namespace apxb

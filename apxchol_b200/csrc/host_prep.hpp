@@ -1,0 +1,57 @@
+// Host-side preparation of the factor for the sweep kernels.
+//
+// Produces the exact arrays the reference's CPU SpTRSV sweeps over
+// (omp_sptrsv::setup_impl, include/apxchol/solver/sptrsv/omp.h:505-861):
+//   * L11 = the leading m x m block of the factor (Laplacian: row/column n-1
+//     dropped, omp.h:543-581);
+//   * the compacting drop with column-sum compensation
+//     (include/apxchol/solver/sptrsv/factor_drop.h:90-211), scale taken before
+//     the drop (omp.h:627-650);
+//   * CSC(L11) (the backward sweep, diagonal first) and CSR(L11) by the
+//     column-order scatter (include/apxchol/solver/sptrsv/transpose.h:116-246;
+//     diagonal last);
+//   * the level of every row per direction -- from the elimination rounds
+//     (omp.h:880-932) or the topological depth (omp.h:933-975) -- and from it
+//     the per-row sum mode: rows of levels with <= 1024 rows use the 4-way
+//     split sum, the others one serial sum (omp.h:32, 1094-1119, 1425-1445).
+// With these the fp64 sweep kernels reproduce the reference's bytes.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace apxb {
+
+constexpr uint32_t kThinLevelRows = 1024;   // kSpTRSVOMPThreshold, omp.h:32
+constexpr double kDropRelDefault = 1e-4;    // kFactorDropRelDefault, factor_drop.h:70
+
+struct prepared_factor {
+    uint32_t n = 0, m = 0;
+    bool sddm = false;
+    uint64_t nnz_factor = 0;     // L11 before the drop
+    uint64_t nnz_stored = 0;     // after the drop
+    uint64_t dropped = 0;
+    // forward: CSR(L11), diagonal last in each row
+    std::vector<uint32_t> csr_ptr, csr_idx;
+    std::vector<float> csr_val;
+    // backward: CSC(L11), diagonal first in each column
+    std::vector<uint32_t> csc_ptr, csc_idx;
+    std::vector<float> csc_val;
+    // per-row 4-way-sum flag, bit-packed (bit r&31 of word r>>5)
+    std::vector<uint32_t> fwd_thin_bits, bck_thin_bits;
+    int32_t fwd_levels = 0, bck_levels = 0;
+    std::vector<uint32_t> perm;  // perm[original] = position
+};
+
+// Returns an empty string on success, else the reason the factor was rejected.
+std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* rowidx, const float* vals,
+                           const uint32_t* perm, bool sddm, const uint64_t* rounds, uint32_t n_rounds,
+                           double drop_rel, prepared_factor& out);
+
+// Full symmetric CSR of P A P^T (rows sorted) from A's full symmetric CSC and
+// perm (what cuda_pcg::setup builds, include/apxchol/solver/pcg_cuda.h:304-404).
+std::string permute_operator(uint32_t n, const int32_t* colptr, const int32_t* rowidx, const double* vals,
+                             const uint32_t* perm, std::vector<int32_t>& ptr, std::vector<int32_t>& idx,
+                             std::vector<double>& val);
+
+}  // namespace apxb

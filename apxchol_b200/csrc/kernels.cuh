@@ -1,0 +1,119 @@
+// Launch interfaces of the solve-phase kernels (implemented in sweep.cu and pcg.cu).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+
+namespace apxb {
+
+// Work-claim counters of one persistent sweep launch; the last warp to leave
+// resets both, so a launch always starts from zero.
+struct sweep_ctl {
+    unsigned ticket;
+    unsigned done;
+};
+
+// One sync-free sweep over a prepared direction of the factor.
+//   forward (dir 0): CSR(L11) rows ascending, diagonal last;
+//   backward (dir 1): CSC(L11) columns descending, diagonal first.
+// `out` must hold the not-yet-solved marker in rows [0, m) on entry; the
+// kernel writes the marker into `reset` (when given) at every row it solves,
+// which re-arms the buffer the other direction writes next.
+template <class T>
+struct sweep_args {
+    uint32_t m;
+    uint32_t nchunks;                 // ceil(m / 32) * K-groups (one warp per chunk)
+    const uint32_t* ptr;
+    const uint32_t* idx;
+    const float* val;
+    const uint32_t* thin;             // per-row 4-way-sum bits (fp64 exact sweep)
+    const T* in;                      // right-hand side, row-major [row][k]
+    const double* rhs_sub;            // nullable: device scalar(s) subtracted from every rhs
+    T* out;                           // tracked solution [row][k]
+    T* reset;                         // nullable: re-armed at every solved row
+    T* copy_out;                      // nullable: untracked copy of the solution
+    sweep_ctl* ctl;
+    dev_error* err;
+    const int* skip;                  // nullable: the launch is a no-op when *skip != 0
+    unsigned long long budget_ns;     // spin budget of every wait
+    int k;                            // right-hand sides per row (fp32 multi-RHS sweep)
+};
+
+// fp64 sweep reproducing the reference CPU arithmetic (exact sum order).
+void launch_sweep64(int dir, const sweep_args<double>& a, int grid, cudaStream_t s);
+// fp32 sweep, fp32 accumulation, k in {1, 2, 4, 8, 16} right-hand sides.
+void launch_sweep32(int dir, const sweep_args<float>& a, int grid, cudaStream_t s);
+// Resident grid (blocks) of the persistent sweeps.
+int sweep_grid64(int num_sms);
+int sweep_grid32(int k, int num_sms);
+constexpr int kSweepThreads = 256;
+
+void launch_fill64(double* p, size_t n, double v, cudaStream_t s);
+void launch_fill32(float* p, size_t n, float v, cudaStream_t s);
+void launch_fill_sent64(double* p, size_t n, cudaStream_t s);
+void launch_fill_sent32(float* p, size_t n, cudaStream_t s);
+
+// ---- PCG / apply kernels (pcg.cu) ----
+
+// Device-resident PCG state (one solve); see pcg.cu for the field meanings.
+struct pcg_state {
+    double rz, pAp, alpha, beta, rr, rs, bnorm, rnorm, prev_check, mean_in, shift, tol, xmean;
+    int iters, max_iter, done, status, center, laplacian, pmode, stag_window, center_k, pad;
+    unsigned long long apply_count;
+    unsigned n, m;
+};
+
+struct reduce_ws {
+    double* partials;   // [grid * 4]
+    unsigned* counter;  // one per reduction site
+};
+
+struct pcg_ptrs {
+    // operator (permuted ordering)
+    const int32_t* a_ptr; const int32_t* a_idx; const double* a_val;
+    const uint32_t* perm;
+    // vectors, permuted ordering
+    double* x; double* r; double* p; double* Ap; const double* z;
+    // original-ordering input / output
+    const double* b_orig; double* x_orig;
+    pcg_state* st;
+    dev_error* err;
+    double* partials;
+    unsigned* counters;   // [8]
+    unsigned n;
+    int grid;
+};
+
+void launch_pcg_init(const pcg_ptrs& p, cudaStream_t s);
+void launch_pcg_zsum(const pcg_ptrs& p, cudaStream_t s);
+void launch_pcg_rz(const pcg_ptrs& p, cudaStream_t s);
+void launch_pcg_update_p(const pcg_ptrs& p, cudaStream_t s, unsigned long long cond_handle, int use_cond);
+void launch_pcg_spmv(const pcg_ptrs& p, cudaStream_t s);
+void launch_pcg_update_xr(const pcg_ptrs& p, cudaStream_t s);
+void launch_pcg_finish(const pcg_ptrs& p, cudaStream_t s);
+
+// apply in the original ordering: permute-in (with optional centring), gather-out.
+struct apply_ptrs {
+    const uint32_t* perm;
+    const double* b;        // original ordering
+    double* zp;             // permuted rhs buffer [n]
+    const double* zsol;     // permuted solution (tracked buffer) [n], zsol[m] = 0 for a Laplacian
+    double* z;              // original ordering output
+    double* scal;           // [0] = b mean, [1] = z shift, [2] = b.z (device)
+    int center;             // Laplacian centring on this application
+    double* partials;
+    unsigned* counters;
+    unsigned n;
+    int grid;
+};
+void launch_apply_bsum(const apply_ptrs& a, cudaStream_t s);      // scal[0] = sum(b)/n if center
+void launch_apply_permute(const apply_ptrs& a, cudaStream_t s);   // zp[perm[v]] = b[v] - scal[0]
+void launch_apply_zsum(const apply_ptrs& a, cudaStream_t s);      // scal[1] = sum(zsol)/n if center
+void launch_apply_gather(const apply_ptrs& a, cudaStream_t s);    // z[v] = zsol[perm[v]] - scal[1]; scal[2] = b.z
+
+// y = A x over the permuted operator with permute / unpermute (residual checks).
+void launch_spmv_plain(const int32_t* ptr, const int32_t* idx, const double* val, const double* x, double* y,
+                       unsigned n, int grid, cudaStream_t s);
+
+}  // namespace apxb

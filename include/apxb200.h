@@ -1,0 +1,173 @@
+/* apxb200 -- the apxchol solve phase on NVIDIA B200 (sm_100a), as a C ABI.
+ *
+ * Replaces, behind plain pointers and sizes, the reference's GPU solve-phase
+ * classes and the CPU preconditioner application they back:
+ *   cuda_sptrsv::setup / solve_LLt / solve_LLt_dev
+ *       include/apxchol/solver/sptrsv/cuda.h:233-487
+ *   apx_cholesky::apply_core / apply_fused / _solve_impl / reset_apply_count
+ *       include/apxchol/solver/preconditioner.h:317, 344-529
+ *   cuda_pcg::setup / solve (GPU-resident PCG)
+ *       include/apxchol/solver/pcg_cuda.h:68-261
+ *   cpu_solver::solve / apxchol::solve (the PCG semantics followed)
+ *       src/solve.cpp:478-654, 681-737
+ * The factor is the reference factorization's own output
+ * (apxchol::factorization, include/apxchol/solver/factorization.h:22-56),
+ * uploaded once.
+ *
+ * Conventions: every call returns an int status (APXB_OK = 0, negative on
+ * failure) and never throws; apxb_last_error() gives the message of the last
+ * failure on the calling thread. Pointers flagged as device pointers must be
+ * device memory of the engine's GPU; all others are host memory. Calls on one
+ * engine are not thread-safe (as the reference: solve.h:96-97).
+ */
+#ifndef APXB200_H
+#define APXB200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define APXB_OK               0
+#define APXB_ERR_INVALID     -1  /* bad argument or malformed input */
+#define APXB_ERR_CUDA        -2  /* a CUDA runtime call failed */
+#define APXB_ERR_OOM         -3  /* device allocation failed */
+#define APXB_ERR_TIMEOUT     -4  /* a device wait ran out of its spin budget */
+#define APXB_ERR_BAD_FACTOR  -5  /* factor violates the storage contract */
+#define APXB_ERR_NONFINITE   -6  /* NaN / Inf met where a finite value is required */
+#define APXB_ERR_BUDGET      -7  /* the engine's device-memory budget is exhausted */
+#define APXB_ERR_BUSY        -8  /* no free slot (serving) */
+
+/* ---- sweep precisions ---- */
+#define APXB_PREC_FP64  0  /* fp32-stored factor, fp64 sweeps: the reference's CPU arithmetic */
+#define APXB_PREC_FP32  1  /* fp32 factor and sweeps, fp32 accumulation (mixed precision) */
+
+/* ---- apply flags ---- */
+#define APXB_DEVICE_PTRS      1  /* b / z are device pointers */
+#define APXB_CENTER_SCHEDULE  0  /* Laplacian centring per the center-k counter (default) */
+#define APXB_CENTER_ALWAYS    2
+#define APXB_CENTER_NEVER     4
+
+typedef struct apxb_engine apxb_engine;
+typedef struct apxb_factor apxb_factor;
+typedef struct apxb_operator apxb_operator;
+
+typedef struct apxb_factor_info {
+    uint32_t n;              /* operator dimension */
+    uint32_t m;              /* factor dimension: n (SDDM) or n-1 (Laplacian) */
+    uint64_t nnz_factor;     /* nnz of L11 before the drop */
+    uint64_t nnz_stored;     /* nnz each sweep direction stores (after the drop) */
+    uint64_t dropped;        /* off-diagonals removed by the drop */
+    int32_t  fwd_levels;     /* level count of each direction (row sum modes) */
+    int32_t  bck_levels;
+    int32_t  precision;      /* APXB_PREC_* */
+    int32_t  sddm;
+    uint64_t device_bytes;   /* device memory held by the factor */
+    uint64_t apply_count;    /* center-k application counter */
+} apxb_factor_info;
+
+typedef struct apxb_pcg_result {
+    int32_t  iterations;
+    int32_t  status;         /* 0 converged, 1 max_iter, 2 stagnated, 3 pAp <= 0, 4 non-finite */
+    double   residual;       /* recurrence relative residual sqrt(r.r)/||b|| at exit */
+    double   true_residual;  /* ||b - A x|| / ||b|| recomputed in fp64 (when requested) */
+    double   seconds;        /* device time of the solve (CUDA events) */
+} apxb_pcg_result;
+
+const char* apxb_last_error(void);
+const char* apxb_version(void);
+
+/* ---- engine: one GPU, one stream, an error word and workspaces ---- */
+int apxb_engine_create(int device, apxb_engine** out);
+int apxb_engine_destroy(apxb_engine* e);
+int apxb_engine_sync(apxb_engine* e);
+/* The engine's CUDA stream (cudaStream_t), for callers that order their own work around it. */
+void* apxb_engine_stream(apxb_engine* e);
+/* Spin budget of every device wait, in nanoseconds (default 2e9). */
+int apxb_engine_set_spin_budget(apxb_engine* e, uint64_t ns);
+/* Blocks of the persistent sweep launches (0 = the resident grid). Any value
+ * gives the same bytes; tests use it to show the result is schedule-free. */
+int apxb_engine_set_sweep_grid(apxb_engine* e, int blocks);
+/* Device-memory budget for factors and operators created on this engine (0 = unlimited). */
+int apxb_engine_set_memory_budget(apxb_engine* e, uint64_t bytes);
+uint64_t apxb_engine_memory_used(apxb_engine* e);
+
+/* ---- factor (replaces cuda_sptrsv::setup, cuda.h:233-459) ----
+ * colptr[n+1], rowidx[nnz], vals[nnz]: the factor CSC, each column starting
+ * with its diagonal, rows ascending (u32 / f32). perm[n]: perm[v] = position.
+ * sddm: full-rank (m = n) vs Laplacian (m = n-1, row/column n-1 dropped).
+ * rounds[n_rounds]: per-round independent-set sizes (factorization.h:43-51);
+ * they fix the sum order of each row exactly as the reference CPU sweep
+ * (n_rounds = 0 uses topological levels, as the reference without rounds).
+ * drop_rel: compacting drop threshold (< 0 = the reference default 1e-4,
+ * 0 = off). precision: APXB_PREC_*. */
+int apxb_factor_create(apxb_engine* e, uint32_t n, const uint32_t* colptr, const uint32_t* rowidx,
+                       const float* vals, const uint32_t* perm, int sddm,
+                       const uint64_t* rounds, uint32_t n_rounds, double drop_rel, int precision,
+                       apxb_factor** out);
+int apxb_factor_destroy(apxb_factor* f);
+int apxb_factor_info_get(const apxb_factor* f, apxb_factor_info* info);
+/* Host copies of the prepared sweep arrays (CSR(L11), CSC(L11)); any pointer may be NULL. */
+int apxb_factor_arrays(const apxb_factor* f, uint32_t* csr_ptr, uint32_t* csr_idx, float* csr_val,
+                       uint32_t* csc_ptr, uint32_t* csc_idx, float* csc_val,
+                       uint8_t* fwd_thin, uint8_t* bck_thin);
+/* apx_cholesky::reset_apply_count (preconditioner.h:317). */
+int apxb_factor_reset_apply_count(apxb_factor* f);
+/* Host-only preparation (no GPU): the arrays apxb_factor_create would upload.
+ * Call once with NULL arrays to get *m and *nnz_stored, then with buffers of
+ * m+1 / nnz_stored / m entries. levels[2] receives the level counts. */
+int apxb_prepare_host(uint32_t n, const uint32_t* colptr, const uint32_t* rowidx, const float* vals,
+                      const uint32_t* perm, int sddm, const uint64_t* rounds, uint32_t n_rounds,
+                      double drop_rel, uint32_t* m, uint64_t* nnz_stored, int32_t* levels,
+                      uint32_t* csr_ptr, uint32_t* csr_idx, float* csr_val,
+                      uint32_t* csc_ptr, uint32_t* csc_idx, float* csc_val,
+                      uint8_t* fwd_thin, uint8_t* bck_thin);
+
+/* ---- sweeps, permuted space, m entries (cuda_sptrsv::solve_LLt_dev, cuda.h:480-487) ---- */
+/* dir 0: forward L y = x; dir 1: backward L^T z = y. Device pointers; fp64. */
+int apxb_sweep(apxb_engine* e, apxb_factor* f, int dir, const double* d_in, double* d_out);
+/* Both sweeps: out = (L L^T)^-1 in. Device pointers (in and out may alias). */
+int apxb_sweep_pair(apxb_engine* e, apxb_factor* f, const double* d_in, double* d_out);
+/* The same with host pointers (cuda_sptrsv::solve_LLt, cuda.h:464-473). */
+int apxb_sweep_pair_host(apxb_engine* e, apxb_factor* f, const double* in, double* out);
+/* reps back-to-back pairs on the engine stream, timed with CUDA events; *seconds = per pair. */
+int apxb_sweep_pair_timed(apxb_engine* e, apxb_factor* f, const double* d_in, double* d_out, int reps,
+                          double* seconds);
+/* k right-hand sides at once, row-interleaved in[i*k + s] (device pointers). */
+int apxb_sweep_pair_multi(apxb_engine* e, apxb_factor* f, int k, const double* d_in, double* d_out);
+
+/* ---- preconditioner application in the original ordering (apply_core) ----
+ * z = P^T (L L^T)^-1 P (b - mean) (- mean), see preconditioner.h:403-529.
+ * flags: APXB_DEVICE_PTRS | APXB_CENTER_*; rz_out (may be NULL) receives b.z. */
+int apxb_apply(apxb_engine* e, apxb_factor* f, const double* b, double* z, int flags, double* rz_out);
+
+/* ---- operator: A in the factor's permuted ordering (cuda_pcg::setup, pcg_cuda.h:68-152) ----
+ * colptr[n+1], rowidx[nnz], vals[nnz]: full symmetric CSC (int32, rows ascending). */
+int apxb_operator_create(apxb_engine* e, uint32_t n, const int32_t* colptr, const int32_t* rowidx,
+                         const double* vals, const uint32_t* perm, apxb_operator** out);
+int apxb_operator_destroy(apxb_operator* a);
+/* y = A x in the original ordering (host pointers), for residual checks. */
+int apxb_operator_matvec(apxb_engine* e, apxb_operator* a, const double* x, double* y);
+
+/* ---- GPU-resident PCG (apxchol::solve on the device; cpu_solver semantics) ----
+ * b, x in the original ordering; host pointers unless APXB_DEVICE_PTRS.
+ * The stop rule, stagnation window (50) and center-k schedule follow
+ * src/solve.cpp:478-654. want_true_residual: recompute ||b - A x||/||b||. */
+int apxb_pcg(apxb_engine* e, apxb_factor* f, apxb_operator* a, const double* b, double* x,
+             double tol, int max_iter, int flags, int want_true_residual, apxb_pcg_result* res);
+
+/* ---- failure detection test hook ----
+ * Runs one forward sweep whose first 32 rows are never solved (the work
+ * counter starts past them), so every row that depends on them waits on a
+ * value nothing writes. Each wait gives up after budget_ns, the kernel records
+ * APXB_ERR_TIMEOUT and drains; the call returns that status and leaves the
+ * engine usable. Used by the tests to show a stalled wait ends in an error,
+ * not a hang. */
+int apxb_test_stalled_sweep(apxb_engine* e, apxb_factor* f, uint64_t budget_ns);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,121 @@
+"""Parity of the CUDA sweeps with the reference arithmetic (gpu).
+
+fp64 sweeps must reproduce the reference CPU sweep (omp_sptrsv) byte for
+byte: same arrays, same per-row sum order, every product and sum rounded on
+its own. The fp32 sweeps are checked against the fp64 result with a stated
+tolerance."""
+import numpy as np
+import pytest
+
+from apxchol_b200 import native
+from tests import golden_cases as gc
+from tests.problems import problem
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+FP32_SWEEP_RTOL = 1e-4   # fp32 factor values are exact; fp32 accumulation over the two sweeps
+
+
+@pytest.fixture(scope="module")
+def eng():
+    import torch
+    torch.cuda.init()
+    e = native.Engine(0)
+    yield e
+    e.close()
+
+
+def _dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _pair_dev(eng, D, x):
+    import torch
+    dx = _dev(x)
+    dz = torch.empty_like(dx)
+    torch.cuda.synchronize()
+    D.sweep_pair(dx, dz)
+    eng.sync()
+    return dz.cpu().numpy()
+
+
+@pytest.mark.parametrize("name", gc.NAMES)
+def test_fp64_sweeps_match_reference_golden(eng, name):
+    import torch
+    A, F, g = gc.case(name)
+    D = native.DeviceFactor(eng, F)
+    dx = _dev(g["x"])
+    dy = torch.empty_like(dx)
+    torch.cuda.synchronize()
+    D.sweep(0, dx, dy)
+    eng.sync()
+    assert np.array_equal(dy.cpu().numpy(), g["fwd"])
+    dz = torch.empty_like(dx)
+    D.sweep(1, dy, dz)
+    eng.sync()
+    assert np.array_equal(dz.cpu().numpy(), g["pair"])
+    assert np.array_equal(_pair_dev(eng, D, g["x"]), g["pair"])
+    assert np.array_equal(D.sweep_pair_host(g["x"]), g["pair"])
+
+
+@pytest.mark.parametrize("name", ["grid2d_256", "grid3d_48", "regular_3000", "rmat_12", "path_200"])
+def test_fp64_pair_matches_oracle_and_is_schedule_free(eng, name):
+    A, F = problem(name)
+    O = oracle.Oracle(A, F)
+    D = native.DeviceFactor(eng, F)
+    x = np.random.default_rng(2).standard_normal(F.m)
+    want = O.pair(x)
+    got = _pair_dev(eng, D, x)
+    assert np.array_equal(got, want)
+    # bit-identical run to run and for any grid (1 block, 7 blocks, resident)
+    for grid in (1, 7, 0):
+        eng.set_sweep_grid(grid)
+        assert np.array_equal(_pair_dev(eng, D, x), want), grid
+    eng.set_sweep_grid(0)
+
+
+@pytest.mark.parametrize("name", ["grid2d_256", "grid3d_48", "regular_3000"])
+def test_fp32_pair_within_tolerance(eng, name):
+    A, F = problem(name)
+    O = oracle.Oracle(A, F)
+    D = native.DeviceFactor(eng, F, precision=native.PREC_FP32)
+    x = np.random.default_rng(3).standard_normal(F.m)
+    want = O.pair(x)
+    got = _pair_dev(eng, D, x)
+    err = np.linalg.norm(got - want) / np.linalg.norm(want)
+    assert err < FP32_SWEEP_RTOL, err
+    assert np.array_equal(_pair_dev(eng, D, x), got)      # deterministic
+
+
+@pytest.mark.parametrize("k", [1, 2, 4, 8, 16])
+def test_fp32_multi_rhs_equals_single(eng, k):
+    import torch
+    A, F = problem("grid3d_24")
+    D = native.DeviceFactor(eng, F, precision=native.PREC_FP32)
+    X = np.random.default_rng(4).standard_normal((F.m, k))
+    dX = _dev(X)
+    dZ = torch.empty_like(dX)
+    torch.cuda.synchronize()
+    D.sweep_pair_multi(k, dX, dZ)
+    eng.sync()
+    Z = dZ.cpu().numpy()
+    for s in range(k):
+        # same entry order and fp32 arithmetic per column: identical to a k=1 sweep
+        assert np.array_equal(Z[:, s], _pair_dev(eng, D, X[:, s])), s
+
+
+def test_apply_sddm_is_bit_exact_and_laplacian_close(eng):
+    A, F, g = gc.case("grid3d_10")          # SDDM: no centring, every op exact
+    D = native.DeviceFactor(eng, F)
+    z, rz = D.apply(g["b"])
+    assert np.array_equal(z, g["apply"])
+    A, F, g = gc.case("grid2d_32")          # Laplacian: permute/gather exact, means differ in association
+    D = native.DeviceFactor(eng, F)
+    O = oracle.Oracle(A, F)
+    for k in range(12):                     # the center-k schedule: only the 10th application centres
+        z, rz = D.apply(g["b"])
+        zo = O.apply(g["b"], reset=(k == 0))
+        assert np.linalg.norm(z - zo) <= 1e-12 * np.linalg.norm(zo), k

@@ -1,0 +1,84 @@
+"""Host logic of the product, no GPU: the C ABI loads and exports every
+symbol of include/apxb200.h, and its factor preparation (drop, transpose,
+levels, sum modes) is byte-identical to the reference's SpTRSV setup."""
+import numpy as np
+import pytest
+
+from apxchol_b200 import native, refsetup
+from tests import golden_cases as gc
+from tests.problems import problem
+
+import oracle
+
+
+def test_library_exports_every_header_symbol():
+    lib = native.load()
+    syms = native.header_symbols()
+    assert len(syms) >= 20
+    missing = [s for s in syms if not hasattr(lib, s)]
+    assert not missing, missing
+    assert b"sm_100a" in lib.apxb_version()
+
+
+@pytest.mark.parametrize("name", gc.NAMES)
+def test_prepare_matches_reference_golden(name):
+    A, F, g = gc.case(name)
+    hp = native.prepare_host(F)
+    for k in ("csr_ptr", "csr_idx", "csr_val", "csc_ptr", "csc_idx", "csc_val"):
+        assert np.array_equal(hp[k], g[k]), k
+
+
+@pytest.mark.parametrize("name", ["grid2d_256", "grid3d_48", "regular_3000", "rmat_12", "path_200"])
+def test_prepare_matches_oracle(name):
+    A, F = problem(name)
+    hp = native.prepare_host(F)
+    op = oracle.prepare(F)
+    for k in ("csr_ptr", "csr_idx", "csr_val", "csc_ptr", "csc_idx", "csc_val", "fwd_thin", "bck_thin"):
+        assert np.array_equal(hp[k], op[k]), k
+    assert hp["levels"] == (op["n_fwd_levels"], op["n_bck_levels"])
+
+
+def test_prepare_without_rounds_uses_topological_levels():
+    A, F = problem("grid2d_64")
+    F2 = refsetup.Factor(n=F.n, colptr=F.colptr, rowidx=F.rowidx, vals=F.vals, perm=F.perm, sddm=F.sddm,
+                         rounds=np.zeros(0, np.uint64))
+    hp = native.prepare_host(F2)
+    op = oracle.prepare(F2)
+    assert np.array_equal(hp["fwd_thin"], op["fwd_thin"]) and np.array_equal(hp["bck_thin"], op["bck_thin"])
+    assert hp["levels"] == (op["n_fwd_levels"], op["n_bck_levels"])
+
+
+def test_prepare_drop_off_keeps_every_entry():
+    A, F = problem("grid3d_24")
+    hp = native.prepare_host(F, drop_rel=0.0)
+    assert hp["nnz"] == F.nnz           # SDDM: L11 is the whole factor
+
+
+def _broken(F, how):
+    colptr, rowidx, vals, perm = F.colptr.copy(), F.rowidx.copy(), F.vals.copy(), F.perm.copy()
+    if how == "diag":
+        rowidx[colptr[3]], rowidx[colptr[3] + 1] = rowidx[colptr[3] + 1], rowidx[colptr[3]]
+    elif how == "perm":
+        perm[0] = perm[1]
+    elif how == "negdiag":
+        vals[colptr[5]] = -1.0
+    elif how == "range":
+        rowidx[colptr[F.n] - 1] = F.n + 7
+    return refsetup.Factor(n=F.n, colptr=colptr, rowidx=rowidx, vals=vals, perm=perm, sddm=F.sddm, rounds=F.rounds)
+
+
+@pytest.mark.parametrize("how", ["diag", "perm", "negdiag", "range"])
+def test_malformed_factor_is_rejected(how):
+    A, F = problem("grid2d_64")
+    with pytest.raises(native.ApxbError) as ei:
+        native.prepare_host(_broken(F, how))
+    assert ei.value.code == native.ERR_BAD_FACTOR
+
+
+def test_factorization_is_deterministic_for_fixed_threads():
+    from apxchol_b200 import gen
+    A = gen.grid3d(16, seed=1)
+    F1 = refsetup.factorize(A, seed=0, threads=4)
+    F2 = refsetup.factorize(A, seed=0, threads=4)
+    for k in ("colptr", "rowidx", "vals", "perm", "rounds"):
+        assert np.array_equal(getattr(F1, k), getattr(F2, k)), k
