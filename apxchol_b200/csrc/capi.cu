@@ -66,6 +66,10 @@ struct apxb_engine {
     // staging for host-pointer entry points
     double* d_stage_a = nullptr; double* d_stage_b = nullptr; size_t stage_n = 0;
     double* h_stage_a = nullptr; double* h_stage_b = nullptr; size_t h_stage_n = 0;
+    // Factors and operators alive on this engine. apxb_engine_destroy with
+    // live children only marks the engine closing; the last child frees it.
+    int children = 0;
+    bool closing = false;
 
     int alloc(void** p, size_t bytes) {
         if (mem_budget && mem_used + bytes > mem_budget)
@@ -130,14 +134,17 @@ struct apxb_factor {
     uint64_t apply_count = 0;
     uint64_t dev_bytes = 0;
     std::vector<std::pair<void*, size_t>> owned;
-    uint32_t *fptr = nullptr, *fidx = nullptr, *fthin = nullptr;
-    uint32_t *bptr = nullptr, *bidx = nullptr, *bthin = nullptr;
     uint32_t* perm = nullptr;
-    float *fval = nullptr, *bval = nullptr;
     double *Y = nullptr, *Z = nullptr, *zp = nullptr;   // fp64 tracked buffers, permuted rhs
     bool y_armed = false, z_armed = false;
     apxb::sweep_ctl* ctl = nullptr;                    // [2]
     int grid64 = 0;
+    // sweep plans (the kernels' layout), per direction
+    uint32_t* info[2] = {nullptr, nullptr};
+    uint32_t* ord[2] = {nullptr, nullptr};
+    uint32_t* ptr[2] = {nullptr, nullptr};
+    uint32_t* idx[2] = {nullptr, nullptr};
+    float* val[2] = {nullptr, nullptr};
     // fp32 sweeps, k right-hand sides
     float *Yf = nullptr, *Zf = nullptr;
     size_t f32_cap = 0;                                // floats per buffer
@@ -229,8 +236,10 @@ int apxb_engine_create(int device, apxb_engine** out) {
     return APXB_OK;
 }
 
-int apxb_engine_destroy(apxb_engine* e) {
-    if (!e) return APXB_OK;
+}  // extern "C"
+
+namespace {
+void engine_free(apxb_engine* e) {
     cudaSetDevice(e->device);
     cudaStreamSynchronize(e->stream);
     cudaFree(e->d_err); cudaFree(e->d_partials); cudaFree(e->d_counters); cudaFree(e->d_scal);
@@ -242,6 +251,22 @@ int apxb_engine_destroy(apxb_engine* e) {
     cudaEventDestroy(e->ev0); cudaEventDestroy(e->ev1);
     cudaStreamDestroy(e->stream);
     delete e;
+}
+
+void release_child(apxb_engine* e) {
+    if (--e->children == 0 && e->closing) engine_free(e);
+}
+}  // namespace
+
+extern "C" {
+
+int apxb_engine_destroy(apxb_engine* e) {
+    if (!e) return APXB_OK;
+    if (e->children > 0) {
+        e->closing = true;
+        return APXB_OK;
+    }
+    engine_free(e);
     return APXB_OK;
 }
 
@@ -319,25 +344,25 @@ int apxb_factor_create(apxb_engine* e, uint32_t n, const uint32_t* colptr, const
                                                  drop_rel, f->h);
     if (!why.empty()) return fail(APXB_ERR_BAD_FACTOR, why);
     const auto& h = f->h;
-    const size_t m = h.m, nnz = h.nnz_stored, words = (m + 31) / 32;
+    const size_t m = h.m, nnz = h.nnz_stored;
     if (nnz >= 0xffffffffull) return fail(APXB_ERR_BAD_FACTOR, "factor nnz exceeds the 32-bit offset range");
     int rc;
-    if ((rc = f->dalloc(&f->fptr, m + 1)) || (rc = f->dalloc(&f->fidx, nnz)) || (rc = f->dalloc(&f->fval, nnz)) ||
-        (rc = f->dalloc(&f->fthin, words)) || (rc = f->dalloc(&f->bptr, m + 1)) ||
-        (rc = f->dalloc(&f->bidx, nnz)) || (rc = f->dalloc(&f->bval, nnz)) || (rc = f->dalloc(&f->bthin, words)) ||
-        (rc = f->dalloc(&f->perm, n)) || (rc = f->dalloc(&f->ctl, 2)))
-        return rc;
+    if ((rc = f->dalloc(&f->perm, n)) || (rc = f->dalloc(&f->ctl, 2))) return rc;
     cudaStream_t s = e->stream;
-    APXB_CK(cudaMemcpyAsync(f->fptr, h.csr_ptr.data(), 4 * (m + 1), cudaMemcpyHostToDevice, s));
-    APXB_CK(cudaMemcpyAsync(f->fidx, h.csr_idx.data(), 4 * nnz, cudaMemcpyHostToDevice, s));
-    APXB_CK(cudaMemcpyAsync(f->fval, h.csr_val.data(), 4 * nnz, cudaMemcpyHostToDevice, s));
-    APXB_CK(cudaMemcpyAsync(f->fthin, h.fwd_thin_bits.data(), 4 * words, cudaMemcpyHostToDevice, s));
-    APXB_CK(cudaMemcpyAsync(f->bptr, h.csc_ptr.data(), 4 * (m + 1), cudaMemcpyHostToDevice, s));
-    APXB_CK(cudaMemcpyAsync(f->bidx, h.csc_idx.data(), 4 * nnz, cudaMemcpyHostToDevice, s));
-    APXB_CK(cudaMemcpyAsync(f->bval, h.csc_val.data(), 4 * nnz, cudaMemcpyHostToDevice, s));
-    APXB_CK(cudaMemcpyAsync(f->bthin, h.bck_thin_bits.data(), 4 * words, cudaMemcpyHostToDevice, s));
     APXB_CK(cudaMemcpyAsync(f->perm, h.perm.data(), 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s));
     APXB_CK(cudaMemsetAsync(f->ctl, 0, sizeof(apxb::sweep_ctl) * 2, s));
+    for (int dir = 0; dir < 2; ++dir) {
+        const apxb::sweep_plan& pl = dir == 0 ? h.fwd_plan : h.bck_plan;
+        if ((rc = f->dalloc(&f->info[dir], pl.info.size())) || (rc = f->dalloc(&f->ord[dir], pl.ord.size())) ||
+            (rc = f->dalloc(&f->ptr[dir], pl.ptr.size())) || (rc = f->dalloc(&f->idx[dir], pl.idx.size())) ||
+            (rc = f->dalloc(&f->val[dir], pl.val.size())))
+            return rc;
+        APXB_CK(cudaMemcpyAsync(f->info[dir], pl.info.data(), 4 * pl.info.size(), cudaMemcpyHostToDevice, s));
+        APXB_CK(cudaMemcpyAsync(f->ord[dir], pl.ord.data(), 4 * pl.ord.size(), cudaMemcpyHostToDevice, s));
+        APXB_CK(cudaMemcpyAsync(f->ptr[dir], pl.ptr.data(), 4 * pl.ptr.size(), cudaMemcpyHostToDevice, s));
+        APXB_CK(cudaMemcpyAsync(f->idx[dir], pl.idx.data(), 4 * pl.idx.size(), cudaMemcpyHostToDevice, s));
+        APXB_CK(cudaMemcpyAsync(f->val[dir], pl.val.data(), 4 * pl.val.size(), cudaMemcpyHostToDevice, s));
+    }
     if ((rc = f->dalloc(&f->Y, n)) || (rc = f->dalloc(&f->Z, n)) || (rc = f->dalloc(&f->zp, n))) return rc;
     // Z[m] (the grounded entry of a Laplacian) is 0 for good; rows < m start armed.
     APXB_CK(cudaMemsetAsync(f->Z, 0, 8 * static_cast<size_t>(n), s));
@@ -347,15 +372,18 @@ int apxb_factor_create(apxb_engine* e, uint32_t n, const uint32_t* colptr, const
     APXB_CK(cudaGetLastError());
     f->grid64 = apxb::sweep_grid64(e->num_sms);
     APXB_CK(cudaStreamSynchronize(s));
+    e->children++;
     *out = f.release();
     return APXB_OK;
 }
 
 int apxb_factor_destroy(apxb_factor* f) {
     if (!f) return APXB_OK;
-    cudaSetDevice(f->e->device);
-    cudaStreamSynchronize(f->e->stream);
+    apxb_engine* e = f->e;
+    cudaSetDevice(e->device);
+    cudaStreamSynchronize(e->stream);
     delete f;
+    release_child(e);
     return APXB_OK;
 }
 
@@ -401,14 +429,21 @@ namespace {
 
 int grid64_of(const apxb_factor* f) { return f->e->sweep_grid > 0 ? f->e->sweep_grid : f->grid64; }
 
+template <class T>
+void plan_args(const apxb_factor* f, int dir, apxb::sweep_args<T>& a) {
+    const apxb::sweep_plan& pl = dir == 0 ? f->h.fwd_plan : f->h.bck_plan;
+    a.m = f->h.m;
+    a.n_items = pl.n_items;
+    a.info = f->info[dir];
+    a.ord = f->ord[dir];
+    a.ptr = f->ptr[dir];
+    a.idx = f->idx[dir];
+    a.val = f->val[dir];
+}
+
 apxb::sweep_args<double> sweep64_args(apxb_factor* f, int dir) {
     apxb::sweep_args<double> a{};
-    a.m = f->h.m;
-    a.nchunks = (f->h.m + 31) / 32;
-    a.ptr = dir == 0 ? f->fptr : f->bptr;
-    a.idx = dir == 0 ? f->fidx : f->bidx;
-    a.val = dir == 0 ? f->fval : f->bval;
-    a.thin = dir == 0 ? f->fthin : f->bthin;
+    plan_args(f, dir, a);
     a.ctl = f->ctl + dir;
     a.err = f->e->d_err;
     a.budget_ns = f->e->budget_ns;
@@ -508,7 +543,6 @@ int ensure_f32(apxb_factor* f, int k) {
 }  // namespace
 
 namespace apxb {
-void launch_sweep32_from64(const sweep_args<float>& a, const double* in64, int grid, cudaStream_t s);
 void launch_cast32to64(const float* in, double* out, size_t n, cudaStream_t s);
 }
 
@@ -523,12 +557,14 @@ int pair_fp32(apxb_factor* f, int k, const double* d_in, double* d_out) {
     if (!f->zf_armed) apxb::launch_fill_sent32(f->Zf, mk, s);
     const int grid = f->e->sweep_grid > 0 ? f->e->sweep_grid : apxb::sweep_grid32(k, f->e->num_sms);
     apxb::sweep_args<float> a{};
-    a.m = f->h.m; a.nchunks = (f->h.m + 31) / 32; a.k = k;
+    a.k = k;
     a.err = f->e->d_err; a.budget_ns = f->e->budget_ns;
-    a.ptr = f->fptr; a.idx = f->fidx; a.val = f->fval; a.thin = f->fthin; a.ctl = f->ctl;
+    plan_args(f, 0, a);
+    a.ctl = f->ctl;
     a.out = f->Yf; a.reset = f->Zf;
-    apxb::launch_sweep32_from64(a, d_in, grid, s);
-    a.ptr = f->bptr; a.idx = f->bidx; a.val = f->bval; a.thin = f->bthin; a.ctl = f->ctl + 1;
+    apxb::launch_sweep32_from64(0, a, d_in, grid, s);
+    plan_args(f, 1, a);
+    a.ctl = f->ctl + 1;
     a.in = f->Yf; a.out = f->Zf; a.reset = f->Yf;
     apxb::launch_sweep32(1, a, grid, s);
     f->yf_armed = true;
@@ -660,15 +696,18 @@ int apxb_operator_create(apxb_engine* e, uint32_t n, const int32_t* colptr, cons
     APXB_CK(cudaMemcpyAsync(a->val, val.data(), 8 * a->nnz, cudaMemcpyHostToDevice, s));
     APXB_CK(cudaMemcpyAsync(a->perm, perm, 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s));
     APXB_CK(cudaStreamSynchronize(s));
+    e->children++;
     *out = a.release();
     return APXB_OK;
 }
 
 int apxb_operator_destroy(apxb_operator* a) {
     if (!a) return APXB_OK;
-    cudaSetDevice(a->e->device);
-    cudaStreamSynchronize(a->e->stream);
+    apxb_engine* e = a->e;
+    cudaSetDevice(e->device);
+    cudaStreamSynchronize(e->stream);
     delete a;
+    release_child(e);
     return APXB_OK;
 }
 

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <numeric>
 
 namespace apxb {
@@ -20,6 +21,99 @@ float column_scale(const float* v, uint32_t first, uint32_t last) {
 // fp32 storage keep rule (omp.h:476-481): |v| >= rel*s and v != 0.
 bool keep_offdiag(float v, float s, double rel) {
     return std::fabs(static_cast<double>(v)) >= rel * static_cast<double>(s) && v != 0.0f;
+}
+
+// Plan of one direction (see sweep_plan). level[r] = level of row r in this
+// direction; (ptr, idx, val) = the canonical arrays of the direction (forward:
+// CSR(L11), diagonal last; backward: CSC(L11), diagonal first).
+void build_plan(uint32_t m, const std::vector<int32_t>& level, int32_t n_levels, const std::vector<uint32_t>& bits,
+                const std::vector<uint32_t>& ptr, const std::vector<uint32_t>& idx, const std::vector<float>& val,
+                bool forward, sweep_plan& plan) {
+    std::vector<std::vector<uint32_t>> by_level(static_cast<size_t>(n_levels));
+    for (uint32_t r = 0; r < m; ++r) by_level[level[r]].push_back(r);
+    plan = sweep_plan{};
+    // items first: (level, G) groups cut into 32/G rows
+    std::vector<uint32_t> item_rows;   // rows, item by item (count from info)
+    item_rows.reserve(m);
+    for (int32_t l = 0; l < n_levels; ++l) {
+        auto& rows = by_level[l];
+        if (rows.empty()) continue;
+        const uint32_t thin = (bits[rows[0] >> 5] >> (rows[0] & 31)) & 1u;
+        for (uint32_t g : {32u, 16u, 8u, 4u, 1u}) {
+            const uint32_t cap = 32 / g;
+            uint32_t lg = 0;
+            while ((1u << lg) < g) ++lg;
+            uint32_t in_item = 0;
+            for (uint32_t r : rows) {
+                if (group_width(ptr[r + 1] - ptr[r] - 1) != g) continue;
+                item_rows.push_back(r);
+                if (++in_item == cap) {
+                    plan.info.push_back(in_item | (lg << 8) | (thin << 16));
+                    in_item = 0;
+                }
+            }
+            if (in_item) plan.info.push_back(in_item | (lg << 8) | (thin << 16));
+        }
+        std::vector<uint32_t>().swap(rows);
+    }
+    plan.n_items = static_cast<uint32_t>(plan.info.size());
+    const size_t npos = static_cast<size_t>(plan.n_items) * 32;
+    plan.ord.assign(npos, kNoRow);
+    plan.ptr.assign(npos + 1, 0);
+    plan.idx.resize(idx.size());
+    plan.val.resize(val.size());
+    size_t k = 0;      // index into item_rows
+    uint32_t e = 0;    // entry cursor
+    for (uint32_t c = 0; c < plan.n_items; ++c) {
+        const uint32_t cnt = plan.info[c] & 0xffu;
+        for (uint32_t s = 0; s < 32; ++s) {
+            const size_t pos = static_cast<size_t>(c) * 32 + s;
+            plan.ptr[pos] = e;
+            if (s < cnt) {
+                const uint32_t r = item_rows[k++];
+                plan.ord[pos] = r;
+                const uint32_t b = ptr[r], en = ptr[r + 1];
+                const uint32_t d = forward ? en - 1 : b;                 // diagonal slot
+                for (uint32_t p = b; p < en; ++p) {
+                    if (p == d) continue;
+                    plan.idx[e] = idx[p]; plan.val[e] = val[p]; ++e;
+                }
+                plan.idx[e] = idx[d]; plan.val[e] = val[d]; ++e;       // diagonal last
+            }
+        }
+    }
+    plan.ptr[npos] = e;
+}
+
+// Plan invariants the kernels rely on (checked at every setup): every row is
+// in exactly one slot; items hold 1..32/G rows of one level, in nondecreasing
+// level order; every slot's entries end with its own diagonal.
+std::string check_plan(uint32_t m, const std::vector<int32_t>& level, const sweep_plan& pl) {
+    std::vector<uint8_t> seen(m, 0);
+    int32_t prev = -1;
+    for (uint32_t c = 0; c < pl.n_items; ++c) {
+        const uint32_t cnt = pl.info[c] & 0xffu, lg = (pl.info[c] >> 8) & 0xffu;
+        if (cnt == 0 || lg > 5 || lg == 1 || cnt > (32u >> lg)) return "bad plan item";
+        int32_t l = -1;
+        for (uint32_t s = 0; s < 32; ++s) {
+            const size_t pos = static_cast<size_t>(c) * 32 + s;
+            const uint32_t r = pl.ord[pos];
+            if (s >= cnt) {
+                if (r != kNoRow || pl.ptr[pos + 1] != pl.ptr[pos]) return "non-empty padding slot";
+                continue;
+            }
+            if (r >= m || seen[r]) return "plan lists a row twice or out of range";
+            seen[r] = 1;
+            if (pl.ptr[pos + 1] <= pl.ptr[pos] || pl.idx[pl.ptr[pos + 1] - 1] != r) return "slot diagonal misplaced";
+            if (l < 0) l = level[r];
+            else if (level[r] != l) return "plan item spans two levels";
+        }
+        if (l < prev) return "plan items out of level order";
+        prev = l;
+    }
+    for (uint32_t r = 0; r < m; ++r)
+        if (!seen[r]) return "plan misses row " + std::to_string(r);
+    return {};
 }
 
 void level_bits(const std::vector<int32_t>& level, int32_t n_levels, std::vector<uint32_t>& bits) {
@@ -172,6 +266,13 @@ std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* r
     }
     level_bits(fl, out.fwd_levels, out.fwd_thin_bits);
     level_bits(bl, out.bck_levels, out.bck_thin_bits);
+    // Sweep plans (the kernels' layout), checked before anything is uploaded.
+    build_plan(m, fl, out.fwd_levels, out.fwd_thin_bits, out.csr_ptr, out.csr_idx, out.csr_val, true, out.fwd_plan);
+    build_plan(m, bl, out.bck_levels, out.bck_thin_bits, cp, ci, cv, false, out.bck_plan);
+    for (int dir = 0; dir < 2; ++dir) {
+        const std::string bad = check_plan(m, dir == 0 ? fl : bl, dir == 0 ? out.fwd_plan : out.bck_plan);
+        if (!bad.empty()) return "internal sweep plan error: " + bad;
+    }
 
     // Permutation: must be a bijection of [0, n).
     out.perm.assign(perm, perm + n);

@@ -25,6 +25,32 @@ namespace apxb {
 constexpr uint32_t kThinLevelRows = 1024;   // kSpTRSVOMPThreshold, omp.h:32
 constexpr double kDropRelDefault = 1e-4;    // kFactorDropRelDefault, factor_drop.h:70
 
+// Execution plan of one sweep direction, in the layout the dataflow kernels
+// read.
+//  * Rows are scheduled level by level; inside a level by lane-group width G
+//    (the lanes that share one row: 1, 4, 8, 16 or 32 -- 1 for rows of <= 8
+//    off-diagonals, else the smallest with 8 * G >= row length), widest first.
+//    Rows of one level never depend on each other, so any order inside a
+//    level gives the same result.
+//  * A work item is up to 32 / G rows of one level and one G. Item c owns the
+//    32 "positions" 32c .. 32c+31; slot s < count holds one row.
+//  * Per position: `ord` = the row (kNoRow for an empty slot), and the row's
+//    entries re-laid in processing order: off-diagonals in the reference's
+//    order (forward: CSR row, columns ascending; backward: CSC column, rows
+//    ascending), then the diagonal last, at [ptr[pos], ptr[pos + 1]).
+//  * `info[c]` = count | log2(G) << 8 | thin << 16 (thin: the level uses the
+//    4-way split sum; a level property, so uniform in an item).
+struct sweep_plan {
+    uint32_t n_items = 0;
+    std::vector<uint32_t> info;
+    std::vector<uint32_t> ord;
+    std::vector<uint32_t> ptr;
+    std::vector<uint32_t> idx;
+    std::vector<float> val;
+};
+
+constexpr uint32_t kNoRow = 0xffffffffu;
+
 struct prepared_factor {
     uint32_t n = 0, m = 0;
     bool sddm = false;
@@ -41,7 +67,16 @@ struct prepared_factor {
     std::vector<uint32_t> fwd_thin_bits, bck_thin_bits;
     int32_t fwd_levels = 0, bck_levels = 0;
     std::vector<uint32_t> perm;  // perm[original] = position
+    sweep_plan fwd_plan, bck_plan;
 };
+
+// Lane-group width for a row with `len` off-diagonals (see sweep_plan).
+inline uint32_t group_width(uint32_t len) {
+    if (len <= 8) return 1;
+    uint32_t g = 4;
+    while (g < 32 && g * 8 < len) g *= 2;
+    return g;
+}
 
 // Returns an empty string on success, else the reason the factor was rejected.
 std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* rowidx, const float* vals,

@@ -14,20 +14,21 @@ struct sweep_ctl {
     unsigned done;
 };
 
-// One sync-free sweep over a prepared direction of the factor.
-//   forward (dir 0): CSR(L11) rows ascending, diagonal last;
-//   backward (dir 1): CSC(L11) columns descending, diagonal first.
+// One sync-free sweep over a prepared direction of the factor (forward:
+// L y = x over CSR(L11); backward: L^T z = y over CSC(L11)), driven by the
+// direction's plan (host_prep.hpp, sweep_plan).
 // `out` must hold the not-yet-solved marker in rows [0, m) on entry; the
 // kernel writes the marker into `reset` (when given) at every row it solves,
 // which re-arms the buffer the other direction writes next.
 template <class T>
 struct sweep_args {
     uint32_t m;
-    uint32_t nchunks;                 // ceil(m / 32) * K-groups (one warp per chunk)
-    const uint32_t* ptr;
+    uint32_t n_items;                 // work items of the plan
+    const uint32_t* info;             // per item: count | log2(G) << 8 | thin << 16
+    const uint32_t* ord;              // per position (32 per item): row or ~0
+    const uint32_t* ptr;              // per position: entry range in idx / val (diagonal last)
     const uint32_t* idx;
     const float* val;
-    const uint32_t* thin;             // per-row 4-way-sum bits (fp64 exact sweep)
     const T* in;                      // right-hand side, row-major [row][k]
     const double* rhs_sub;            // nullable: device scalar(s) subtracted from every rhs
     T* out;                           // tracked solution [row][k]
@@ -44,6 +45,8 @@ struct sweep_args {
 void launch_sweep64(int dir, const sweep_args<double>& a, int grid, cudaStream_t s);
 // fp32 sweep, fp32 accumulation, k in {1, 2, 4, 8, 16} right-hand sides.
 void launch_sweep32(int dir, const sweep_args<float>& a, int grid, cudaStream_t s);
+// The same with the right-hand side read from fp64 (minus rhs_sub[s] when given).
+void launch_sweep32_from64(int dir, const sweep_args<float>& a, const double* in64, int grid, cudaStream_t s);
 // Resident grid (blocks) of the persistent sweeps.
 int sweep_grid64(int num_sms);
 int sweep_grid32(int k, int num_sms);

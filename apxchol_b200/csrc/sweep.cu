@@ -1,54 +1,61 @@
 // Sync-free persistent triangular sweeps over the approximate-Cholesky factor
-// (the preconditioner's forward and backward solves, the reference's
+// (the preconditioner's forward and backward solves; the reference's
 // dataflow_kernel, src/cuda_dataflow.cu:321-478, and its CPU counterpart
 // omp_sptrsv::solve_levelset, include/apxchol/solver/sptrsv/omp.h:1094-1119).
 //
 // Design (B200):
-//  * One launch per sweep, a resident grid of 256-thread blocks. Each warp
-//    claims 32 consecutive rows in sweep order from an atomic ticket, one
-//    thread per row. A row only waits on rows earlier in sweep order, which
-//    were claimed earlier by warps that are running, so progress never
-//    depends on scheduling.
+//  * One launch per sweep: a resident grid whose warps work off the
+//    direction's plan (host_prep.hpp, sweep_plan): work items of up to 32 rows
+//    of one level and one lane-group width G, G lanes per row, with the rows'
+//    entries re-laid in processing order. A warp claims items from an atomic
+//    ticket in level order, so a row only waits on rows of earlier items; the
+//    lowest unfinished item is always being run by its owner, so progress
+//    never depends on scheduling.
+//  * Latency pipeline: a warp runs item i while the entries and right-hand
+//    sides of item i+1 and the row descriptors of item i+2 are in flight, and
+//    the ticket for item i+3 is being claimed. A row's critical path is then
+//    its dependency loads, the arithmetic and one store.
 //  * No level barriers and no separate ready flags: the output vector starts
 //    filled with a signalling-NaN marker and a solved value replaces it, so one
-//    relaxed 64-bit load both tests a dependency and fetches it. The kernel
-//    re-arms the buffer the next sweep writes (reset), so no extra fill pass
-//    runs between applications.
-//  * Each thread streams its row's column indices and values through the
-//    read-only path and keeps up to 8 dependency loads in flight. A thread
-//    whose operands are ready consumes them and moves on; the others re-poll
-//    only the missing ones on the warp's next pass (with a nanosleep backoff
-//    when no lane of the warp progressed). Threads never wait for each other,
-//    so a row may depend on a row of the same warp.
+//    relaxed load both tests a dependency and fetches it. The kernel re-arms
+//    the buffer the next sweep writes (reset), so no fill pass runs between
+//    applications.
 //  * Every wait has a time budget (globaltimer): a warp that makes no progress
-//    for the budget records APXB_ERR_TIMEOUT in the engine's error word, and
-//    every warp drains; the host turns it into an error status. Nothing spins
-//    unbounded.
+//    for the budget records APXB_ERR_TIMEOUT in the engine's error word and
+//    every warp drains; the host turns it into an error status.
 //  * fp64 sweep: products and sums are individually rounded (__dmul_rn /
 //    __dadd_rn, no contraction) in the reference's order -- rows of "thin"
 //    levels use the 4-way split sum of dot_thin (omp.h:1343-1357), rows of
-//    "fat" levels one serial sum (omp.h:1434-1439) -- and the row is finished
-//    with one correctly rounded subtract and divide (omp.h:1440). The result is
-//    the reference CPU sweep's bytes.
-//  * fp32 sweep: fp32 values, fp32 fused multiply-add accumulation in entry
-//    order, k right-hand sides per row interleaved [row][k]: each factor entry
-//    is read once for all k.
+//    "fat" levels one serial sum (omp.h:1434-1439), finished by one correctly
+//    rounded subtract and divide (omp.h:1440). With G lanes per row the
+//    products are formed in parallel and the order is replayed through
+//    shuffles: the result is the reference CPU sweep's bytes.
+//  * fp32 sweep: fp32 values and fp32 fused multiply-add accumulation, each
+//    lane adding its entries in order as they arrive, lane partials combined
+//    by a fixed butterfly (deterministic); k right-hand sides per row
+//    interleaved [row][k]: each factor entry is read once for all k.
+//  * Rows are consumed progressively: in the fp64 sweep the reference's sum
+//    order is advanced step by step as operands arrive, so most of a row's
+//    arithmetic is done before its last dependency lands.
+#include <cstdlib>
+
 #include "kernels.cuh"
 
 namespace apxb {
 
 namespace {
 
-constexpr int kBatch = 8;   // dependency loads in flight per thread (fp64)
+constexpr int kBatch = 8;               // entries in flight per lane
+constexpr uint32_t kNoRowDev = 0xffffffffu;
 
 __device__ __forceinline__ unsigned backoff_ns(int spins) {
-    return spins < 2 ? 0u : min(32u << min(spins >> 1, 4), 512u);
+    return spins < 4 ? 0u : min(16u << min((spins - 4) >> 1, 3), 128u);
 }
 
 // Warp-uniform check of the error word and the time budget. Returns true when
 // the warp must drain (budget exhausted -> error raised, or another warp failed).
-__device__ __forceinline__ bool wait_must_stop(dev_error* err, unsigned long long t0,
-                                               unsigned long long budget, int where, uint32_t row) {
+__device__ __forceinline__ bool wait_must_stop(dev_error* err, unsigned long long t0, unsigned long long budget,
+                                               int where, uint32_t row) {
     int stop = 0;
     if ((threadIdx.x & 31) == 0) {
         if (ld_relaxed_int(&err->code) != 0) {
@@ -61,6 +68,20 @@ __device__ __forceinline__ bool wait_must_stop(dev_error* err, unsigned long lon
     return __shfl_sync(kFull, stop, 0) != 0;
 }
 
+// Idle bookkeeping of a warp-uniform polling loop; returns true to drain.
+struct idle_clock {
+    int spins = 0;
+    unsigned long long t0 = 0;
+    __device__ __forceinline__ bool idle(dev_error* err, unsigned long long budget, int where, uint32_t row) {
+        if (spins == 0 && (threadIdx.x & 31) == 0) t0 = globaltimer();
+        ++spins;
+        if ((spins & 15) == 0 && wait_must_stop(err, __shfl_sync(kFull, t0, 0), budget, where, row)) return true;
+        const unsigned ns = backoff_ns(spins);
+        if (ns) __nanosleep(ns);
+        return false;
+    }
+};
+
 __device__ __forceinline__ void leave(sweep_ctl* ctl) {
     if ((threadIdx.x & 31) == 0) {
         const unsigned total = gridDim.x * (blockDim.x >> 5);
@@ -71,134 +92,302 @@ __device__ __forceinline__ void leave(sweep_ctl* ctl) {
     }
 }
 
-template <int DIR>
-__global__ void __launch_bounds__(kSweepThreads) k_sweep64(const sweep_args<double> a) {
-    if (a.skip && *a.skip) return;
-    const int lane = threadIdx.x & 31;
+__device__ __forceinline__ double dadd4(double a, double b, double c, double d) {
+    return __dadd_rn(__dadd_rn(a, b), __dadd_rn(c, d));
+}
+
+// ---------------------------------------------------------------------------
+// Exact-order accumulation for a G-lane group (G = 2^LG = 4..32). Lane u of
+// the group holds the product of entry t = t0 + u of the current step.
+// thin: chain c (entries t = c mod 4, t < gend) accumulates in lane c in entry
+// order; the step holding gend (when the row has a tail, gend < len) then
+// combines the chains as (s0 + s1) + (s2 + s3) and adds the <= 3 tail entries
+// in order. fat: lane 0 adds every entry in order. Steps are consumed in
+// order, each as soon as all of its operands are ready, so most of a row's
+// arithmetic is done before its last dependency arrives.
+struct exact_state {
+    double s = 0.0, sum = 0.0;
+    bool combined = false;
+};
+
+template <unsigned LG>
+__device__ __forceinline__ void exact_step(bool thin, bool consume, unsigned u, uint32_t t0, uint32_t len,
+                                           uint32_t gend, double pk, exact_state& e) {
+    constexpr unsigned G = 1u << LG;
+    if (thin) {
+        const unsigned c = u & 3u;
+#pragma unroll
+        for (unsigned i = 0; i < G / 4; ++i) {
+            const double v = __shfl_sync(kFull, pk, static_cast<int>(c + 4u * i), static_cast<int>(G));
+            if (consume && u < 4 && t0 + c + 4u * i < gend) e.s = __dadd_rn(e.s, v);
+        }
+        const bool tail = consume && !e.combined && gend < len && (gend >> LG) == (t0 >> LG);
+        if (__any_sync(kFull, tail)) {
+            const double s1 = __shfl_sync(kFull, e.s, 1, static_cast<int>(G));
+            const double s2 = __shfl_sync(kFull, e.s, 2, static_cast<int>(G));
+            const double s3 = __shfl_sync(kFull, e.s, 3, static_cast<int>(G));
+            if (tail && u == 0) e.sum = dadd4(e.s, s1, s2, s3);
+#pragma unroll
+            for (unsigned i = 0; i < 3; ++i) {
+                const double v = __shfl_sync(kFull, pk, static_cast<int>((gend + i) & (G - 1u)), static_cast<int>(G));
+                if (tail && u == 0 && gend + i < len) e.sum = __dadd_rn(e.sum, v);
+            }
+            if (tail) e.combined = true;
+        }
+    } else {
+#pragma unroll
+        for (unsigned i = 0; i < G; ++i) {
+            const double v = __shfl_sync(kFull, pk, static_cast<int>(i), static_cast<int>(G));
+            if (consume && u == 0 && t0 + i < len) e.s = __dadd_rn(e.s, v);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Pipeline stages shared by both precisions.
+
+// Stage D: the item's descriptor words, loaded by every lane for its own slot.
+struct stage_desc {
+    unsigned c;          // item (>= n_items: none)
+    uint32_t info, row, q, e;
+};
+
+template <class T>
+__device__ __forceinline__ void load_desc(const sweep_args<T>& a, unsigned c, stage_desc& d) {
+    const unsigned lane = threadIdx.x & 31u;
+    d.c = c;
+    d.info = 0; d.row = kNoRowDev; d.q = 0; d.e = 0;
+    if (c < a.n_items) {
+        const size_t pos = static_cast<size_t>(c) * 32 + lane;
+        d.info = __ldg(a.info + c);
+        d.row = __ldg(a.ord + pos);
+        d.q = __ldg(a.ptr + pos);
+        d.e = __ldg(a.ptr + pos + 1);
+    }
+}
+
+// Lane view of an item after stage D: the lane's group, its row, and its range.
+struct lane_view {
+    unsigned c, lg, G, u, gid;
+    bool valid, thin;
+    uint32_t row, q, len;   // off-diagonals at [q, q + len); diagonal at q + len
+};
+
+__device__ __forceinline__ lane_view view_of(const stage_desc& d) {
+    const unsigned lane = threadIdx.x & 31u;
+    lane_view v;
+    v.c = d.c;
+    v.lg = (d.info >> 8) & 0xffu;
+    v.G = 1u << v.lg;
+    v.u = lane & (v.G - 1u);
+    v.gid = lane >> v.lg;
+    v.thin = (d.info >> 16) & 1u;
+    // slot gid's descriptor lives in lane gid
+    v.row = __shfl_sync(kFull, d.row, static_cast<int>(v.gid));
+    v.q = __shfl_sync(kFull, d.q, static_cast<int>(v.gid));
+    const uint32_t e = __shfl_sync(kFull, d.e, static_cast<int>(v.gid));
+    v.valid = v.row != kNoRowDev;
+    v.len = v.valid ? e - v.q - 1u : 0u;
+    return v;
+}
+
+// ---------------------------------------------------------------------------
+// fp64 dataflow sweep.
+
+// Stage L data of one item (fp64).
+struct stage_data64 {
+    lane_view v;
+    double rhs, d;
+    uint32_t jj[kBatch];
+    float ww[kBatch];
+};
+
+__device__ __forceinline__ void load_data64(const sweep_args<double>& a, const stage_desc& ds, stage_data64& s) {
+    s.v = view_of(ds);
+    const lane_view& v = s.v;
+    s.rhs = 0.0; s.d = 1.0;
+    if (v.c >= a.n_items) return;
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+        const uint32_t t = (static_cast<uint32_t>(k) << v.lg) + v.u;
+        if (t < v.len) { s.jj[k] = __ldg(a.idx + v.q + t); s.ww[k] = __ldg(a.val + v.q + t); }
+    }
+    if (v.valid && v.u == 0) {
+        s.rhs = a.in[v.row];
+        s.d = static_cast<double>(__ldg(a.val + v.q + v.len));
+        if (a.reset) a.reset[v.row] = sent_of(0.0);
+    }
+}
+
+// Group rows (G = 2^LG lanes per row): batches of kBatch steps; inside a
+// batch the steps are consumed in order as their operands arrive.
+template <unsigned LG>
+__device__ __forceinline__ bool run_group64(const sweep_args<double>& a, stage_data64& s, int where,
+                                            double& total) {
+    constexpr unsigned G = 1u << LG;
+    const lane_view& v = s.v;
+    const unsigned gmask = G == 32 ? kFull : (((1u << G) - 1u) << (v.gid * G));
+    const uint32_t J = (v.len + G - 1u) >> LG;
+    const uint32_t Jmax = __reduce_max_sync(kFull, J);
+    const uint32_t gend = v.thin ? (v.len & ~3u) : 0u;
+    exact_state e;
+    idle_clock clk;
+    for (uint32_t jb = 0; jb < Jmax; jb += kBatch) {
+        if (jb > 0) {
+#pragma unroll
+            for (int k = 0; k < kBatch; ++k) {
+                const uint32_t t = ((jb + k) << LG) + v.u;
+                if (t < v.len) { s.jj[k] = __ldg(a.idx + v.q + t); s.ww[k] = __ldg(a.val + v.q + t); }
+            }
+        }
+        const uint32_t nsteps = J > jb ? min(static_cast<uint32_t>(kBatch), J - jb) : 0u;
+        double p[kBatch];
+        unsigned rdy = 0;   // bit k: entry of step k absent or its product is in p[k]
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+            const uint32_t t = ((jb + k) << LG) + v.u;
+            p[k] = 0.0;
+            if (t < v.len) p[k] = ld_relaxed(a.out + s.jj[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+            const uint32_t t = ((jb + k) << LG) + v.u;
+            if (t >= v.len) rdy |= 1u << k;
+            else if (!is_sent(p[k])) { p[k] = __dmul_rn(static_cast<double>(s.ww[k]), p[k]); rdy |= 1u << k; }
+        }
+        uint32_t kpos = 0;
+        for (;;) {
+            bool progressed = false;
+#pragma unroll
+            for (int k = 0; k < kBatch; ++k) {
+                const unsigned bal = __ballot_sync(kFull, (rdy >> k) & 1u);
+                const bool consume = kpos == static_cast<uint32_t>(k) && static_cast<uint32_t>(k) < nsteps &&
+                                     (bal & gmask) == gmask;
+                if (__any_sync(kFull, consume)) {
+                    exact_step<LG>(v.thin, consume, v.u, (jb + k) << LG, v.len, gend, p[k], e);
+                    progressed = true;
+                }
+                if (consume) ++kpos;
+            }
+            if (__all_sync(kFull, kpos >= nsteps)) break;
+            if (progressed) clk.spins = 0;
+            else if (clk.idle(a.err, a.budget_ns, where, v.row)) return false;
+#pragma unroll
+            for (int k = 0; k < kBatch; ++k) {
+                if (!((rdy >> k) & 1u)) {
+                    const double y = ld_relaxed(a.out + s.jj[k]);
+                    if (!is_sent(y)) { p[k] = __dmul_rn(static_cast<double>(s.ww[k]), y); rdy |= 1u << k; }
+                }
+            }
+        }
+    }
+    const double s1 = __shfl_sync(kFull, e.s, 1, static_cast<int>(G));
+    const double s2 = __shfl_sync(kFull, e.s, 2, static_cast<int>(G));
+    const double s3 = __shfl_sync(kFull, e.s, 3, static_cast<int>(G));
+    total = !v.thin ? e.s : (e.combined ? e.sum : dadd4(e.s, s1, s2, s3));
+    return true;
+}
+
+// One lane per row (<= kBatch off-diagonals): each lane consumes its entries
+// in order as they arrive, 4-way rotating chains then the serial tail.
+__device__ __forceinline__ bool run_lane64(const sweep_args<double>& a, stage_data64& s, int where, double& total) {
+    const lane_view& v = s.v;
+    const uint32_t n = v.len;   // <= kBatch for these rows
+    const uint32_t gend = v.thin ? (n & ~3u) : 0u;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, sum = 0.0;
+    bool combined = false;
+    double yv[kBatch];
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k)
+        if (static_cast<uint32_t>(k) < n) yv[k] = ld_relaxed(a.out + s.jj[k]);
+    uint32_t kpos = 0;
+    idle_clock clk;
     for (;;) {
-        unsigned c = 0;
+        const uint32_t before = kpos;
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+            if (kpos == static_cast<uint32_t>(k) && kpos < n && !is_sent(yv[k])) {
+                const double pr = __dmul_rn(static_cast<double>(s.ww[k]), yv[k]);
+                if (kpos < gend) {
+                    const double w = __dadd_rn(s0, pr);
+                    s0 = s1; s1 = s2; s2 = s3; s3 = w;
+                } else {
+                    if (!combined) { sum = dadd4(s0, s1, s2, s3); combined = true; }
+                    sum = __dadd_rn(sum, pr);
+                }
+                ++kpos;
+            }
+        }
+        if (__all_sync(kFull, kpos >= n)) break;
+        if (__any_sync(kFull, kpos != before)) clk.spins = 0;
+        else if (clk.idle(a.err, a.budget_ns, where, v.row)) return false;
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k)
+            if (static_cast<uint32_t>(k) >= kpos && static_cast<uint32_t>(k) < n && is_sent(yv[k]))
+                yv[k] = ld_relaxed(a.out + s.jj[k]);
+    }
+    total = combined ? sum : dadd4(s0, s1, s2, s3);
+    return true;
+}
+
+// Run one item: wait for its operands, replay the reference's sum order, store.
+// Returns false when the warp must drain.
+template <int DIR>
+__device__ __forceinline__ bool run64(const sweep_args<double>& a, stage_data64& s) {
+    const lane_view& v = s.v;
+    const int where = DIR == 0 ? kFwdSweep : kBckSweep;
+    double total = 0.0;
+    bool ok;
+    switch (v.lg) {
+        case 0: ok = run_lane64(a, s, where, total); break;
+        case 2: ok = run_group64<2>(a, s, where, total); break;
+        case 3: ok = run_group64<3>(a, s, where, total); break;
+        case 4: ok = run_group64<4>(a, s, where, total); break;
+        default: ok = run_group64<5>(a, s, where, total); break;
+    }
+    if (!ok) return false;
+    if (v.valid && v.u == 0) {
+        double rhs = s.rhs;
+        if (a.rhs_sub) rhs = __dsub_rn(rhs, *a.rhs_sub);
+        const double y = __ddiv_rn(__dsub_rn(rhs, total), s.d);
+        st_relaxed(a.out + v.row, y);
+        if (a.copy_out) a.copy_out[v.row] = y;
+    }
+    return true;
+}
+
+template <int DIR>
+__global__ void __launch_bounds__(kSweepThreads, 2) k_df64(const sweep_args<double> a) {
+    if (a.skip && *a.skip) return;
+    const unsigned lane = threadIdx.x & 31u;
+    // prologue: tickets for the first three stages
+    unsigned tk = 0;
+    if (lane == 0) tk = atomicAdd(&a.ctl->ticket, 1u);
+    stage_desc dD;
+    load_desc(a, __shfl_sync(kFull, tk, 0), dD);
+    if (lane == 0) tk = atomicAdd(&a.ctl->ticket, 1u);
+    stage_data64 sL;
+    load_data64(a, dD, sL);
+    load_desc(a, __shfl_sync(kFull, tk, 0), dD);
+    if (lane == 0) tk = atomicAdd(&a.ctl->ticket, 1u);
+    while (sL.v.c < a.n_items) {
+        // rotate: run L, data for D, descriptor for the claimed ticket, claim the next
+        stage_data64 sR = sL;
+        load_data64(a, dD, sL);
+        load_desc(a, __shfl_sync(kFull, tk, 0), dD);
         int bad = 0;
         if (lane == 0) {
-            c = atomicAdd(&a.ctl->ticket, 1u);
+            tk = atomicAdd(&a.ctl->ticket, 1u);
             bad = ld_relaxed_int(&a.err->code);
         }
-        c = __shfl_sync(kFull, c, 0);
-        bad = __shfl_sync(kFull, bad, 0);
-        if (c >= a.nchunks || bad) break;
-
-        const uint32_t pos = c * 32u + lane;
-        const bool valid = pos < a.m;
-        const uint32_t r = DIR == 0 ? pos : a.m - 1u - pos;
-        uint32_t q = 0, qend = 0, gend = 0;
-        double rhs = 0.0, d = 1.0;
-        if (valid) {
-            const uint32_t p0 = __ldg(a.ptr + r), p1 = __ldg(a.ptr + r + 1);
-            q = DIR == 0 ? p0 : p0 + 1;
-            qend = DIR == 0 ? p1 - 1 : p1;
-            const uint32_t dslot = DIR == 0 ? p1 - 1 : p0;
-            const bool thin = (__ldg(a.thin + (r >> 5)) >> (r & 31)) & 1u;
-            gend = thin ? q + ((qend - q) & ~3u) : q;
-            rhs = a.in[r];
-            if (a.rhs_sub) rhs = __dsub_rn(rhs, *a.rhs_sub);
-            if (a.reset) a.reset[r] = sent_of(0.0);
-            d = static_cast<double>(__ldg(a.val + dslot));
-        }
-        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, sum = 0.0;
-        bool combined = false;
-        bool active = valid;
-        // Each lane keeps one batch of up to kBatch entries in flight. A lane
-        // whose operands are ready consumes them and moves on; the others
-        // re-poll only their missing ones on the next pass. Lanes never wait
-        // for each other, so a row may depend on a row of the same warp.
-        bool loaded = false, stop = false;
-        uint32_t cnt = 0;
-        unsigned need = 0;
-        uint32_t jj[kBatch];
-        float ww[kBatch];
-        double yv[kBatch];
-        int spins = 0;
-        unsigned long long t_idle = 0;
-        while (__any_sync(kFull, active)) {
-            bool progress = false;
-            if (active) {
-                if (!loaded) {
-                    cnt = min(static_cast<uint32_t>(kBatch), qend - q);
-#pragma unroll
-                    for (int k = 0; k < kBatch; ++k)
-                        if (k < cnt) { jj[k] = __ldg(a.idx + q + k); ww[k] = __ldg(a.val + q + k); }
-#pragma unroll
-                    for (int k = 0; k < kBatch; ++k)
-                        if (k < cnt) yv[k] = ld_relaxed(a.out + jj[k]);
-                    need = 0;
-#pragma unroll
-                    for (int k = 0; k < kBatch; ++k)
-                        if (k < cnt && is_sent(yv[k])) need |= 1u << k;
-                    loaded = true;
-                } else {
-#pragma unroll
-                    for (int k = 0; k < kBatch; ++k)
-                        if ((need >> k) & 1u) yv[k] = ld_relaxed(a.out + jj[k]);
-#pragma unroll
-                    for (int k = 0; k < kBatch; ++k)
-                        if (((need >> k) & 1u) && !is_sent(yv[k])) need &= ~(1u << k);
-                }
-                if (need == 0) {
-#pragma unroll
-                    for (int k = 0; k < kBatch; ++k) {
-                        if (k < cnt) {
-                            const double pr = __dmul_rn(static_cast<double>(ww[k]), yv[k]);
-                            if (q + k < gend) {
-                                const double t = __dadd_rn(s0, pr);
-                                s0 = s1; s1 = s2; s2 = s3; s3 = t;
-                            } else {
-                                if (!combined) {
-                                    sum = __dadd_rn(__dadd_rn(s0, s1), __dadd_rn(s2, s3));
-                                    combined = true;
-                                }
-                                sum = __dadd_rn(sum, pr);
-                            }
-                        }
-                    }
-                    q += cnt;
-                    loaded = false;
-                    progress = true;
-                    if (q == qend) {
-                        if (!combined) sum = __dadd_rn(__dadd_rn(s0, s1), __dadd_rn(s2, s3));
-                        const double v = __ddiv_rn(__dsub_rn(rhs, sum), d);
-                        st_relaxed(a.out + r, v);
-                        if (a.copy_out) a.copy_out[r] = v;
-                        active = false;
-                    }
-                }
-            }
-            if (__any_sync(kFull, progress)) {
-                spins = 0;
-            } else {
-                if (spins == 0 && lane == 0) t_idle = globaltimer();
-                ++spins;
-                if ((spins & 15) == 0 &&
-                    wait_must_stop(a.err, __shfl_sync(kFull, t_idle, 0), a.budget_ns,
-                                   DIR == 0 ? kFwdSweep : kBckSweep, r)) {
-                    stop = true;
-                    break;
-                }
-                const unsigned ns = backoff_ns(spins);
-                if (ns) __nanosleep(ns);
-            }
-        }
-        if (stop) break;
+        if (__shfl_sync(kFull, bad, 0)) break;
+        if (!run64<DIR>(a, sR)) break;
     }
     leave(a.ctl);
 }
 
-// ---- fp32, K right-hand sides per row ----
-
-template <int K> struct vecf;
-template <> struct vecf<1> { float v[1]; };
-template <> struct vecf<2> { float v[2]; };
-template <> struct vecf<4> { float v[4]; };
-template <> struct vecf<8> { float v[8]; };
-template <> struct vecf<16> { float v[16]; };
+// ---------------------------------------------------------------------------
+// fp32, K right-hand sides per row.
 
 template <int K>
 __device__ __forceinline__ void ld_row(const float* p, float (&y)[K]) {
@@ -244,126 +433,144 @@ __device__ __forceinline__ bool row_ready(const float (&y)[K]) {
     return ok;
 }
 
+template <int K>
+struct batch_of { static constexpr int value = K >= 16 ? 2 : (K >= 8 ? 4 : 8); };
+
+template <int K>
+struct stage_data32 {
+    lane_view v;
+    float rhs[K];
+    float d;
+    uint32_t jj[batch_of<K>::value];
+    float ww[batch_of<K>::value];
+};
+
+template <int K>
+__device__ __forceinline__ void load_data32(const sweep_args<float>& a, const double* in64, const stage_desc& ds,
+                                            stage_data32<K>& s) {
+    constexpr int B = batch_of<K>::value;
+    s.v = view_of(ds);
+    const lane_view& v = s.v;
+    s.d = 1.0f;
+#pragma unroll
+    for (int r = 0; r < K; ++r) s.rhs[r] = 0.0f;
+    if (v.c >= a.n_items) return;
+#pragma unroll
+    for (int k = 0; k < B; ++k) {
+        const uint32_t t = (static_cast<uint32_t>(k) << v.lg) + v.u;
+        if (t < v.len) { s.jj[k] = __ldg(a.idx + v.q + t); s.ww[k] = __ldg(a.val + v.q + t); }
+    }
+    if (v.valid && v.u == 0) {
+        const size_t base = static_cast<size_t>(v.row) * K;
+        if (in64) {
+#pragma unroll
+            for (int r = 0; r < K; ++r) {
+                double x = in64[base + r];
+                if (a.rhs_sub) x -= a.rhs_sub[r];
+                s.rhs[r] = static_cast<float>(x);
+            }
+        } else {
+#pragma unroll
+            for (int r = 0; r < K; ++r) s.rhs[r] = a.in[base + r];
+        }
+        s.d = __ldg(a.val + v.q + v.len);
+        if (a.reset) {
+            float sent[K];
+#pragma unroll
+            for (int r = 0; r < K; ++r) sent[r] = sent_of(0.0f);
+            st_row<K>(a.reset + base, sent);
+        }
+    }
+}
+
 template <int DIR, int K>
-__global__ void __launch_bounds__(kSweepThreads) k_sweep32(const sweep_args<float> a,
-                                                           const double* in64) {
-    constexpr int B = K >= 16 ? 2 : (K >= 8 ? 4 : 8);   // entries in flight per thread
+__device__ __forceinline__ bool run32(const sweep_args<float>& a, stage_data32<K>& s) {
+    constexpr int B = batch_of<K>::value;
+    const lane_view& v = s.v;
+    const int where = DIR == 0 ? kFwdSweep32 : kBckSweep32;
+    const uint32_t J = (v.len + v.G - 1u) >> v.lg;
+    const uint32_t Jmax = __reduce_max_sync(kFull, J);
+    float acc[K];
+#pragma unroll
+    for (int r = 0; r < K; ++r) acc[r] = 0.0f;
+    idle_clock clk;
+    for (uint32_t jb = 0; jb < Jmax; jb += B) {
+        if (jb > 0) {
+#pragma unroll
+            for (int k = 0; k < B; ++k) {
+                const uint32_t t = ((jb + k) << v.lg) + v.u;
+                if (t < v.len) { s.jj[k] = __ldg(a.idx + v.q + t); s.ww[k] = __ldg(a.val + v.q + t); }
+            }
+        }
+        // this lane's entries in the batch: steps 0 .. nk-1
+        const uint32_t t0 = (jb << v.lg) + v.u;
+        const uint32_t nk = t0 < v.len ? min(static_cast<uint32_t>(B), ((v.len - t0 - 1u) >> v.lg) + 1u) : 0u;
+        float yv[B][K];
+#pragma unroll
+        for (int k = 0; k < B; ++k)
+            if (static_cast<uint32_t>(k) < nk) ld_row<K>(a.out + static_cast<size_t>(s.jj[k]) * K, yv[k]);
+        // each lane consumes its own entries in order as they arrive
+        uint32_t kpos = 0;
+        for (;;) {
+            const uint32_t before = kpos;
+#pragma unroll
+            for (int k = 0; k < B; ++k) {
+                if (kpos == static_cast<uint32_t>(k) && kpos < nk && row_ready<K>(yv[k])) {
+#pragma unroll
+                    for (int r = 0; r < K; ++r) acc[r] = __fmaf_rn(s.ww[k], yv[k][r], acc[r]);
+                    ++kpos;
+                }
+            }
+            if (__all_sync(kFull, kpos >= nk)) break;
+            if (__any_sync(kFull, kpos != before)) clk.spins = 0;
+            else if (clk.idle(a.err, a.budget_ns, where, v.row)) return false;
+#pragma unroll
+            for (int k = 0; k < B; ++k)
+                if (static_cast<uint32_t>(k) >= kpos && static_cast<uint32_t>(k) < nk && !row_ready<K>(yv[k]))
+                    ld_row<K>(a.out + static_cast<size_t>(s.jj[k]) * K, yv[k]);
+        }
+    }
+    // fixed butterfly over the group's lanes
+    for (unsigned o = v.G >> 1; o > 0; o >>= 1)
+#pragma unroll
+        for (int r = 0; r < K; ++r) acc[r] += __shfl_xor_sync(kFull, acc[r], static_cast<int>(o), static_cast<int>(v.G));
+    if (v.valid && v.u == 0) {
+        float y[K];
+#pragma unroll
+        for (int r = 0; r < K; ++r) y[r] = __fdiv_rn(s.rhs[r] - acc[r], s.d);
+        st_row<K>(a.out + static_cast<size_t>(v.row) * K, y);
+        if (a.copy_out) {
+#pragma unroll
+            for (int r = 0; r < K; ++r) a.copy_out[static_cast<size_t>(v.row) * K + r] = y[r];
+        }
+    }
+    return true;
+}
+
+template <int DIR, int K>
+__global__ void __launch_bounds__(kSweepThreads, 2) k_df32(const sweep_args<float> a, const double* in64) {
     if (a.skip && *a.skip) return;
-    const int lane = threadIdx.x & 31;
-    for (;;) {
-        unsigned c = 0;
+    const unsigned lane = threadIdx.x & 31u;
+    unsigned tk = 0;
+    if (lane == 0) tk = atomicAdd(&a.ctl->ticket, 1u);
+    stage_desc dD;
+    load_desc(a, __shfl_sync(kFull, tk, 0), dD);
+    if (lane == 0) tk = atomicAdd(&a.ctl->ticket, 1u);
+    stage_data32<K> sL;
+    load_data32<K>(a, in64, dD, sL);
+    load_desc(a, __shfl_sync(kFull, tk, 0), dD);
+    if (lane == 0) tk = atomicAdd(&a.ctl->ticket, 1u);
+    while (sL.v.c < a.n_items) {
+        stage_data32<K> sR = sL;
+        load_data32<K>(a, in64, dD, sL);
+        load_desc(a, __shfl_sync(kFull, tk, 0), dD);
         int bad = 0;
         if (lane == 0) {
-            c = atomicAdd(&a.ctl->ticket, 1u);
+            tk = atomicAdd(&a.ctl->ticket, 1u);
             bad = ld_relaxed_int(&a.err->code);
         }
-        c = __shfl_sync(kFull, c, 0);
-        bad = __shfl_sync(kFull, bad, 0);
-        if (c >= a.nchunks || bad) break;
-
-        const uint32_t pos = c * 32u + lane;
-        const bool valid = pos < a.m;
-        const uint32_t r = DIR == 0 ? pos : a.m - 1u - pos;
-        uint32_t q = 0, qend = 0;
-        float rhs[K], acc[K];
-        float dinv = 1.0f, d = 1.0f;
-#pragma unroll
-        for (int s = 0; s < K; ++s) { rhs[s] = 0.0f; acc[s] = 0.0f; }
-        if (valid) {
-            const uint32_t p0 = __ldg(a.ptr + r), p1 = __ldg(a.ptr + r + 1);
-            q = DIR == 0 ? p0 : p0 + 1;
-            qend = DIR == 0 ? p1 - 1 : p1;
-            d = __ldg(a.val + (DIR == 0 ? p1 - 1 : p0));
-            (void)dinv;
-            if (in64) {
-#pragma unroll
-                for (int s = 0; s < K; ++s) {
-                    double v = in64[static_cast<size_t>(r) * K + s];
-                    if (a.rhs_sub) v -= a.rhs_sub[s];
-                    rhs[s] = static_cast<float>(v);
-                }
-            } else {
-#pragma unroll
-                for (int s = 0; s < K; ++s) rhs[s] = a.in[static_cast<size_t>(r) * K + s];
-            }
-            if (a.reset) {
-                float sent[K];
-#pragma unroll
-                for (int s = 0; s < K; ++s) sent[s] = sent_of(0.0f);
-                st_row<K>(a.reset + static_cast<size_t>(r) * K, sent);
-            }
-        }
-        bool active = valid;
-        bool loaded = false, stop = false;
-        uint32_t cnt = 0;
-        unsigned need = 0;
-        uint32_t jj[B];
-        float ww[B];
-        float yv[B][K];
-        int spins = 0;
-        unsigned long long t_idle = 0;
-        while (__any_sync(kFull, active)) {
-            bool progress = false;
-            if (active) {
-                if (!loaded) {
-                    cnt = min(static_cast<uint32_t>(B), qend - q);
-#pragma unroll
-                    for (int e = 0; e < B; ++e)
-                        if (e < cnt) { jj[e] = __ldg(a.idx + q + e); ww[e] = __ldg(a.val + q + e); }
-#pragma unroll
-                    for (int e = 0; e < B; ++e)
-                        if (e < cnt) ld_row<K>(a.out + static_cast<size_t>(jj[e]) * K, yv[e]);
-                    need = 0;
-#pragma unroll
-                    for (int e = 0; e < B; ++e)
-                        if (e < cnt && !row_ready<K>(yv[e])) need |= 1u << e;
-                    loaded = true;
-                } else {
-#pragma unroll
-                    for (int e = 0; e < B; ++e)
-                        if ((need >> e) & 1u) ld_row<K>(a.out + static_cast<size_t>(jj[e]) * K, yv[e]);
-#pragma unroll
-                    for (int e = 0; e < B; ++e)
-                        if (((need >> e) & 1u) && row_ready<K>(yv[e])) need &= ~(1u << e);
-                }
-                if (need == 0) {
-#pragma unroll
-                    for (int e = 0; e < B; ++e)
-                        if (e < cnt)
-#pragma unroll
-                            for (int s = 0; s < K; ++s) acc[s] = __fmaf_rn(ww[e], yv[e][s], acc[s]);
-                    q += cnt;
-                    loaded = false;
-                    progress = true;
-                    if (q == qend) {
-                        float v[K];
-#pragma unroll
-                        for (int s = 0; s < K; ++s) v[s] = __fdiv_rn(rhs[s] - acc[s], d);
-                        st_row<K>(a.out + static_cast<size_t>(r) * K, v);
-                        if (a.copy_out) {
-#pragma unroll
-                            for (int s = 0; s < K; ++s) a.copy_out[static_cast<size_t>(r) * K + s] = v[s];
-                        }
-                        active = false;
-                    }
-                }
-            }
-            if (__any_sync(kFull, progress)) {
-                spins = 0;
-            } else {
-                if (spins == 0 && lane == 0) t_idle = globaltimer();
-                ++spins;
-                if ((spins & 15) == 0 &&
-                    wait_must_stop(a.err, __shfl_sync(kFull, t_idle, 0), a.budget_ns,
-                                   DIR == 0 ? kFwdSweep32 : kBckSweep32, r)) {
-                    stop = true;
-                    break;
-                }
-                const unsigned ns = backoff_ns(spins);
-                if (ns) __nanosleep(ns);
-            }
-        }
-        if (stop) break;
+        if (__shfl_sync(kFull, bad, 0)) break;
+        if (!run32<DIR, K>(a, sR)) break;
     }
     leave(a.ctl);
 }
@@ -384,53 +591,47 @@ int fill_grid(size_t n) {
     return static_cast<int>(b < 4096 ? (b ? b : 1) : 4096);
 }
 
-template <int DIR, int K>
-void sweep32_k(const sweep_args<float>& a, const double* in64, int grid, cudaStream_t s) {
-    k_sweep32<DIR, K><<<grid, kSweepThreads, 0, s>>>(a, in64);
-}
-
 template <int K>
 int occ32() {
     int b0 = 0, b1 = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_sweep32<0, K>, kSweepThreads, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_sweep32<1, K>, kSweepThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_df32<0, K>, kSweepThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_df32<1, K>, kSweepThreads, 0);
     return b0 < b1 ? b0 : b1;
+}
+
+template <int K>
+void sweep32_dir(int dir, const sweep_args<float>& a, const double* in64, int grid, cudaStream_t s) {
+    if (!a.n_items) return;
+    if (dir == 0) k_df32<0, K><<<grid, kSweepThreads, 0, s>>>(a, in64);
+    else          k_df32<1, K><<<grid, kSweepThreads, 0, s>>>(a, in64);
 }
 
 }  // namespace
 
 void launch_sweep64(int dir, const sweep_args<double>& a, int grid, cudaStream_t s) {
-    if (dir == 0) k_sweep64<0><<<grid, kSweepThreads, 0, s>>>(a);
-    else          k_sweep64<1><<<grid, kSweepThreads, 0, s>>>(a);
+    if (!a.n_items) return;
+    if (dir == 0) k_df64<0><<<grid, kSweepThreads, 0, s>>>(a);
+    else          k_df64<1><<<grid, kSweepThreads, 0, s>>>(a);
 }
 
 void launch_sweep32(int dir, const sweep_args<float>& a, int grid, cudaStream_t s) {
-    // The fp32 sweep reads its rhs from `in` (fp32) -- the fp64 variant used by
-    // the PCG passes it as a double pointer through rhs-widening in pcg.cu.
-    const double* in64 = nullptr;
-    switch (a.k) {
-        case 1:  dir == 0 ? sweep32_k<0, 1>(a, in64, grid, s) : sweep32_k<1, 1>(a, in64, grid, s); break;
-        case 2:  dir == 0 ? sweep32_k<0, 2>(a, in64, grid, s) : sweep32_k<1, 2>(a, in64, grid, s); break;
-        case 4:  dir == 0 ? sweep32_k<0, 4>(a, in64, grid, s) : sweep32_k<1, 4>(a, in64, grid, s); break;
-        case 8:  dir == 0 ? sweep32_k<0, 8>(a, in64, grid, s) : sweep32_k<1, 8>(a, in64, grid, s); break;
-        default: dir == 0 ? sweep32_k<0, 16>(a, in64, grid, s) : sweep32_k<1, 16>(a, in64, grid, s); break;
-    }
+    launch_sweep32_from64(dir, a, nullptr, grid, s);
 }
 
-void launch_sweep32_from64(const sweep_args<float>& a, const double* in64, int grid, cudaStream_t s) {
+void launch_sweep32_from64(int dir, const sweep_args<float>& a, const double* in64, int grid, cudaStream_t s) {
     switch (a.k) {
-        case 1:  sweep32_k<0, 1>(a, in64, grid, s); break;
-        case 2:  sweep32_k<0, 2>(a, in64, grid, s); break;
-        case 4:  sweep32_k<0, 4>(a, in64, grid, s); break;
-        case 8:  sweep32_k<0, 8>(a, in64, grid, s); break;
-        default: sweep32_k<0, 16>(a, in64, grid, s); break;
+        case 1:  sweep32_dir<1>(dir, a, in64, grid, s); break;
+        case 2:  sweep32_dir<2>(dir, a, in64, grid, s); break;
+        case 4:  sweep32_dir<4>(dir, a, in64, grid, s); break;
+        case 8:  sweep32_dir<8>(dir, a, in64, grid, s); break;
+        default: sweep32_dir<16>(dir, a, in64, grid, s); break;
     }
 }
 
 int sweep_grid64(int num_sms) {
     int b0 = 0, b1 = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_sweep64<0>, kSweepThreads, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_sweep64<1>, kSweepThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_df64<0>, kSweepThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_df64<1>, kSweepThreads, 0);
     const int b = b0 < b1 ? b0 : b1;
     return (b > 0 ? b : 1) * num_sms;
 }
@@ -456,7 +657,6 @@ void launch_fill32(float* p, size_t n, float v, cudaStream_t s) {
 void launch_fill_sent64(double* p, size_t n, cudaStream_t s) {
     double v;
     const uint64_t bits = kSent64;
-    static_assert(sizeof(v) == sizeof(bits), "");
     __builtin_memcpy(&v, &bits, sizeof(v));
     launch_fill64(p, n, v, s);
 }

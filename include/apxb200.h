@@ -81,6 +81,8 @@ const char* apxb_version(void);
 
 /* ---- engine: one GPU, one stream, an error word and workspaces ---- */
 int apxb_engine_create(int device, apxb_engine** out);
+/* With factors or operators still alive the engine is only marked closed; the
+ * last of them to be destroyed releases it. */
 int apxb_engine_destroy(apxb_engine* e);
 int apxb_engine_sync(apxb_engine* e);
 /* The engine's CUDA stream (cudaStream_t), for callers that order their own work around it. */
