@@ -145,6 +145,9 @@ struct apxb_factor {
     uint32_t* ptr[2] = {nullptr, nullptr};
     uint32_t* idx[2] = {nullptr, nullptr};
     float* val[2] = {nullptr, nullptr};
+    uint32_t *seg_row[2] = {nullptr, nullptr}, *seg_lvl[2] = {nullptr, nullptr};
+    uint32_t *seg_ptr[2] = {nullptr, nullptr}, *seg_idx[2] = {nullptr, nullptr};
+    float* seg_val[2] = {nullptr, nullptr};
     // fp32 sweeps, k right-hand sides
     float *Yf = nullptr, *Zf = nullptr;
     size_t f32_cap = 0;                                // floats per buffer
@@ -362,6 +365,19 @@ int apxb_factor_create(apxb_engine* e, uint32_t n, const uint32_t* colptr, const
         APXB_CK(cudaMemcpyAsync(f->ptr[dir], pl.ptr.data(), 4 * pl.ptr.size(), cudaMemcpyHostToDevice, s));
         APXB_CK(cudaMemcpyAsync(f->idx[dir], pl.idx.data(), 4 * pl.idx.size(), cudaMemcpyHostToDevice, s));
         APXB_CK(cudaMemcpyAsync(f->val[dir], pl.val.data(), 4 * pl.val.size(), cudaMemcpyHostToDevice, s));
+        if (pl.seg_rows) {
+            if ((rc = f->dalloc(&f->seg_row[dir], pl.seg_row.size())) ||
+                (rc = f->dalloc(&f->seg_lvl[dir], pl.seg_lvl.size())) ||
+                (rc = f->dalloc(&f->seg_ptr[dir], pl.seg_ptr.size())) ||
+                (rc = f->dalloc(&f->seg_idx[dir], pl.seg_idx.size())) ||
+                (rc = f->dalloc(&f->seg_val[dir], pl.seg_val.size())))
+                return rc;
+            APXB_CK(cudaMemcpyAsync(f->seg_row[dir], pl.seg_row.data(), 4 * pl.seg_row.size(), cudaMemcpyHostToDevice, s));
+            APXB_CK(cudaMemcpyAsync(f->seg_lvl[dir], pl.seg_lvl.data(), 4 * pl.seg_lvl.size(), cudaMemcpyHostToDevice, s));
+            APXB_CK(cudaMemcpyAsync(f->seg_ptr[dir], pl.seg_ptr.data(), 4 * pl.seg_ptr.size(), cudaMemcpyHostToDevice, s));
+            APXB_CK(cudaMemcpyAsync(f->seg_idx[dir], pl.seg_idx.data(), 4 * pl.seg_idx.size(), cudaMemcpyHostToDevice, s));
+            APXB_CK(cudaMemcpyAsync(f->seg_val[dir], pl.seg_val.data(), 4 * pl.seg_val.size(), cudaMemcpyHostToDevice, s));
+        }
     }
     if ((rc = f->dalloc(&f->Y, n)) || (rc = f->dalloc(&f->Z, n)) || (rc = f->dalloc(&f->zp, n))) return rc;
     // Z[m] (the grounded entry of a Laplacian) is 0 for good; rows < m start armed.
@@ -439,6 +455,14 @@ void plan_args(const apxb_factor* f, int dir, apxb::sweep_args<T>& a) {
     a.ptr = f->ptr[dir];
     a.idx = f->idx[dir];
     a.val = f->val[dir];
+    a.seg_first = pl.seg_first;
+    a.seg_rows = pl.seg_rows;
+    a.seg_levels = pl.seg_levels;
+    a.seg_row = f->seg_row[dir];
+    a.seg_lvl = f->seg_lvl[dir];
+    a.seg_ptr = f->seg_ptr[dir];
+    a.seg_idx = f->seg_idx[dir];
+    a.seg_val = f->seg_val[dir];
 }
 
 apxb::sweep_args<double> sweep64_args(apxb_factor* f, int dir) {

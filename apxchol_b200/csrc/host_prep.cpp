@@ -26,12 +26,72 @@ bool keep_offdiag(float v, float s, double rel) {
 // Plan of one direction (see sweep_plan). level[r] = level of row r in this
 // direction; (ptr, idx, val) = the canonical arrays of the direction (forward:
 // CSR(L11), diagonal last; backward: CSC(L11), diagonal first).
+// APXB_SEG_LEVEL_ROWS overrides kSegLevelRows (0 disables the serial segment).
+uint32_t seg_level_rows_setting() {
+    const char* e = std::getenv("APXB_SEG_LEVEL_ROWS");
+    return e ? static_cast<uint32_t>(std::atoi(e)) : kSegLevelRows;
+}
+
+// Appends row r's entries re-laid (off-diagonals in the reference order, the
+// diagonal last) to (oi, ov).
+void relay_row(uint32_t r, bool forward, const std::vector<uint32_t>& ptr, const std::vector<uint32_t>& idx,
+               const std::vector<float>& val, std::vector<uint32_t>& oi, std::vector<float>& ov) {
+    const uint32_t b = ptr[r], en = ptr[r + 1];
+    const uint32_t d = forward ? en - 1 : b;
+    for (uint32_t p = b; p < en; ++p) {
+        if (p == d) continue;
+        oi.push_back(idx[p]); ov.push_back(val[p]);
+    }
+    oi.push_back(idx[d]); ov.push_back(val[d]);
+}
+
 void build_plan(uint32_t m, const std::vector<int32_t>& level, int32_t n_levels, const std::vector<uint32_t>& bits,
                 const std::vector<uint32_t>& ptr, const std::vector<uint32_t>& idx, const std::vector<float>& val,
-                bool forward, sweep_plan& plan) {
+                bool forward, bool contiguous, sweep_plan& plan) {
     std::vector<std::vector<uint32_t>> by_level(static_cast<size_t>(n_levels));
     for (uint32_t r = 0; r < m; ++r) by_level[level[r]].push_back(r);
     plan = sweep_plan{};
+    // Serial segment: the trailing run (forward order) of small levels.
+    int32_t seg_from = n_levels;   // in this direction's level numbering: forward [seg_from, n), backward [0, seg_to)
+    int32_t seg_to = 0;
+    const uint32_t seg_rows_max = seg_level_rows_setting();
+    if (contiguous && seg_rows_max > 0) {
+        uint32_t rows = 0;
+        int32_t nseg = 0;
+        for (int32_t k = 0; k < n_levels; ++k) {            // k-th level from the forward end
+            const int32_t l = forward ? n_levels - 1 - k : k;
+            const uint32_t c = static_cast<uint32_t>(by_level[l].size());
+            if (c > seg_rows_max || rows + c > kSegMaxRows) break;
+            rows += c;
+            ++nseg;
+        }
+        if (nseg >= static_cast<int32_t>(kSegMinLevels)) {
+            if (forward) seg_from = n_levels - nseg;
+            else seg_to = nseg;
+        }
+    }
+    auto in_seg = [&](int32_t l) { return forward ? l >= seg_from : l < seg_to; };
+    if (seg_from < n_levels || seg_to > 0) {
+        plan.seg_first = m;
+        plan.seg_ptr.push_back(0);
+        for (int32_t l = 0; l < n_levels; ++l) {
+            if (!in_seg(l)) continue;
+            const auto& rows = by_level[l];
+            const uint32_t thin = rows.empty() ? 0u : (bits[rows[0] >> 5] >> (rows[0] & 31)) & 1u;
+            plan.seg_lvl.push_back(static_cast<uint32_t>(plan.seg_row.size()) | (thin << 31));
+            for (uint32_t r : rows) {
+                plan.seg_row.push_back(r);
+                plan.seg_first = std::min(plan.seg_first, r);
+                relay_row(r, forward, ptr, idx, val, plan.seg_idx, plan.seg_val);
+                plan.seg_ptr.push_back(static_cast<uint32_t>(plan.seg_idx.size()));
+            }
+        }
+        plan.seg_levels = static_cast<uint32_t>(plan.seg_lvl.size());
+        plan.seg_lvl.push_back(static_cast<uint32_t>(plan.seg_row.size()));
+        plan.seg_rows = static_cast<uint32_t>(plan.seg_row.size());
+        for (int32_t l = 0; l < n_levels; ++l)
+            if (in_seg(l)) std::vector<uint32_t>().swap(by_level[l]);
+    }
     // items first: (level, G) groups cut into 32/G rows
     std::vector<uint32_t> item_rows;   // rows, item by item (count from info)
     item_rows.reserve(m);
@@ -83,6 +143,8 @@ void build_plan(uint32_t m, const std::vector<int32_t>& level, int32_t n_levels,
         }
     }
     plan.ptr[npos] = e;
+    plan.idx.resize(e);
+    plan.val.resize(e);
 }
 
 // Plan invariants the kernels rely on (checked at every setup): every row is
@@ -110,6 +172,22 @@ std::string check_plan(uint32_t m, const std::vector<int32_t>& level, const swee
         }
         if (l < prev) return "plan items out of level order";
         prev = l;
+    }
+    if (pl.seg_rows) {
+        if (pl.seg_first + pl.seg_rows != m) return "serial segment is not a suffix";
+        for (uint32_t i = 0; i < pl.seg_rows; ++i) {
+            const uint32_t r = pl.seg_row[i];
+            if (r < pl.seg_first || r >= m || seen[r]) return "bad segment row";
+            seen[r] = 1;
+            if (pl.seg_ptr[i + 1] <= pl.seg_ptr[i] || pl.seg_idx[pl.seg_ptr[i + 1] - 1] != r)
+                return "segment diagonal misplaced";
+        }
+        for (uint32_t l = 0; l < pl.seg_levels; ++l) {
+            const uint32_t lo = pl.seg_lvl[l] & 0x7fffffffu, hi = pl.seg_lvl[l + 1] & 0x7fffffffu;
+            if (hi < lo) return "bad segment level";
+            for (uint32_t i = lo; i < hi; ++i)
+                if (level[pl.seg_row[i]] != level[pl.seg_row[lo]]) return "segment level mixes levels";
+        }
     }
     for (uint32_t r = 0; r < m; ++r)
         if (!seen[r]) return "plan misses row " + std::to_string(r);
@@ -267,8 +345,9 @@ std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* r
     level_bits(fl, out.fwd_levels, out.fwd_thin_bits);
     level_bits(bl, out.bck_levels, out.bck_thin_bits);
     // Sweep plans (the kernels' layout), checked before anything is uploaded.
-    build_plan(m, fl, out.fwd_levels, out.fwd_thin_bits, out.csr_ptr, out.csr_idx, out.csr_val, true, out.fwd_plan);
-    build_plan(m, bl, out.bck_levels, out.bck_thin_bits, cp, ci, cv, false, out.bck_plan);
+    build_plan(m, fl, out.fwd_levels, out.fwd_thin_bits, out.csr_ptr, out.csr_idx, out.csr_val, true, done,
+               out.fwd_plan);
+    build_plan(m, bl, out.bck_levels, out.bck_thin_bits, cp, ci, cv, false, done, out.bck_plan);
     for (int dir = 0; dir < 2; ++dir) {
         const std::string bad = check_plan(m, dir == 0 ? fl : bl, dir == 0 ? out.fwd_plan : out.bck_plan);
         if (!bad.empty()) return "internal sweep plan error: " + bad;

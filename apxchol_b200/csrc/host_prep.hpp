@@ -40,6 +40,15 @@ constexpr double kDropRelDefault = 1e-4;    // kFactorDropRelDefault, factor_dro
 //    ascending), then the diagonal last, at [ptr[pos], ptr[pos + 1]).
 //  * `info[c]` = count | log2(G) << 8 | thin << 16 (thin: the level uses the
 //    4-way split sum; a level property, so uniform in an item).
+//  * The serial segment (round-as-level factors only): the run of small
+//    levels at the end of the elimination (the forward sweep's last levels,
+//    the backward sweep's first), at most kSegLevelRows rows each. One thread
+//    block solves it level by level through shared memory and __syncthreads,
+//    which is far cheaper per level than a cross-SM dependency hop. Its rows
+//    are the suffix [seg_first, m); `seg_row` lists them in processing order,
+//    `seg_lvl` holds each level's start in that list (seg_levels + 1 words,
+//    bit 31 = thin level), and their entries are re-laid like the items'
+//    (`seg_ptr` per listed row, diagonal last).
 struct sweep_plan {
     uint32_t n_items = 0;
     std::vector<uint32_t> info;
@@ -47,7 +56,16 @@ struct sweep_plan {
     std::vector<uint32_t> ptr;
     std::vector<uint32_t> idx;
     std::vector<float> val;
+    uint32_t seg_first = 0, seg_rows = 0, seg_levels = 0;
+    std::vector<uint32_t> seg_row, seg_lvl, seg_ptr, seg_idx;
+    std::vector<float> seg_val;
 };
+
+// The serial segment is off by default (APXB_SEG_LEVEL_ROWS=<rows> enables it):
+// on the factors measured so far the cross-SM dataflow hop beat it.
+constexpr uint32_t kSegLevelRows = 0;    // a level joins the serial segment when it has <= this many rows
+constexpr uint32_t kSegMaxRows = 4096;   // segment values stay in shared memory (fp64: 32 KB)
+constexpr uint32_t kSegMinLevels = 8;    // fewer small trailing levels than this: no segment
 
 constexpr uint32_t kNoRow = 0xffffffffu;
 

@@ -29,6 +29,13 @@ struct sweep_args {
     const uint32_t* ptr;              // per position: entry range in idx / val (diagonal last)
     const uint32_t* idx;
     const float* val;
+    // serial segment (see sweep_plan): rows [seg_first, seg_first + seg_rows)
+    uint32_t seg_first, seg_rows, seg_levels;
+    const uint32_t* seg_row;
+    const uint32_t* seg_lvl;
+    const uint32_t* seg_ptr;
+    const uint32_t* seg_idx;
+    const float* seg_val;
     const T* in;                      // right-hand side, row-major [row][k]
     const double* rhs_sub;            // nullable: device scalar(s) subtracted from every rhs
     T* out;                           // tracked solution [row][k]

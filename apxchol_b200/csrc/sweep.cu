@@ -4,8 +4,11 @@
 // omp_sptrsv::solve_levelset, include/apxchol/solver/sptrsv/omp.h:1094-1119).
 //
 // Design (B200):
-//  * One launch per sweep: a resident grid whose warps work off the
-//    direction's plan (host_prep.hpp, sweep_plan): work items of up to 32 rows
+//  * A sweep is a dataflow launch plus, for factors whose elimination ends in
+//    a long run of tiny rounds, a serial-segment launch (one block, shared
+//    memory, __syncthreads per level; forward: after the dataflow, backward:
+//    before it). The dataflow grid's warps work off the direction's plan
+//    (host_prep.hpp, sweep_plan): work items of up to 32 rows
 //    of one level and one lane-group width G, G lanes per row, with the rows'
 //    entries re-laid in processing order. A warp claims items from an atomic
 //    ticket in level order, so a row only waits on rows of earlier items; the
@@ -575,6 +578,166 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_df32(const sweep_args<floa
     leave(a.ctl);
 }
 
+
+// ---------------------------------------------------------------------------
+// Serial segment: one block solves the run of small trailing levels (forward:
+// after the dataflow launch; backward: before it) level by level, values in
+// shared memory, __syncthreads between levels. Each warp solves its rows (the
+// segment rows round-robin over the warps, in processing order) with all 32
+// lanes, and prefetches its next row while working on the current one.
+
+constexpr int kSegThreads = 512;
+constexpr uint64_t kBox = 0xFFF6000000000000ull;   // NaN box carrying a segment-local index
+
+__device__ __forceinline__ double box_index(uint32_t i) { return __longlong_as_double(static_cast<long long>(kBox | i)); }
+__device__ __forceinline__ bool is_box(double v) {
+    return (static_cast<unsigned long long>(__double_as_longlong(v)) & 0xFFFF000000000000ull) == kBox;
+}
+__device__ __forceinline__ uint32_t unbox(double v) {
+    return static_cast<uint32_t>(static_cast<unsigned long long>(__double_as_longlong(v)) & 0xffffffffull);
+}
+
+struct seg_slot {
+    uint32_t i, r, q, len;
+    double rhs, d;
+    double pv[kBatch];   // product (operand outside the segment, final) or the boxed segment index
+    float ww[kBatch];
+};
+
+__device__ __forceinline__ void seg_batch64(const sweep_args<double>& a, const seg_slot& s, uint32_t jb,
+                                            double (&pv)[kBatch], float (&ww)[kBatch]) {
+    const unsigned lane = threadIdx.x & 31u;
+    const uint32_t s0 = a.seg_first, s1 = a.seg_first + a.seg_rows;
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+        const uint32_t t = ((jb + k) << 5) + lane;
+        pv[k] = 0.0;
+        ww[k] = 0.0f;
+        if (t < s.len) {
+            const uint32_t j = __ldg(a.seg_idx + s.q + t);
+            const float w = __ldg(a.seg_val + s.q + t);
+            ww[k] = w;
+            pv[k] = (j >= s0 && j < s1) ? box_index(j - s0) : __dmul_rn(static_cast<double>(w), a.out[j]);
+        }
+    }
+}
+
+__device__ __forceinline__ void seg_fetch64(const sweep_args<double>& a, uint32_t i, seg_slot& s) {
+    s.i = i;
+    s.len = 0;
+    if (i >= a.seg_rows) return;
+    s.r = __ldg(a.seg_row + i);
+    s.q = __ldg(a.seg_ptr + i);
+    s.len = __ldg(a.seg_ptr + i + 1) - s.q - 1u;
+    seg_batch64(a, s, 0, s.pv, s.ww);
+    if ((threadIdx.x & 31u) == 0) {
+        s.rhs = a.in[s.r];
+        s.d = static_cast<double>(__ldg(a.seg_val + s.q + s.len));
+        if (a.reset) a.reset[s.r] = sent_of(0.0);
+    }
+}
+
+__device__ __forceinline__ void seg_solve64(const sweep_args<double>& a, seg_slot& s, bool thin, double* segv) {
+    const unsigned lane = threadIdx.x & 31u;
+    const uint32_t J = (s.len + 31u) >> 5;
+    const uint32_t gend = thin ? (s.len & ~3u) : 0u;
+    exact_state e;
+    for (uint32_t jb = 0; jb < J; jb += kBatch) {
+        if (jb > 0) seg_batch64(a, s, jb, s.pv, s.ww);
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+            double p = s.pv[k];
+            if (is_box(p)) p = __dmul_rn(static_cast<double>(s.ww[k]), segv[unbox(p)]);
+            exact_step<5>(thin, jb + k < J, lane, (jb + k) << 5, s.len, gend, p, e);
+        }
+    }
+    const double s1 = __shfl_sync(kFull, e.s, 1), s2 = __shfl_sync(kFull, e.s, 2), s3 = __shfl_sync(kFull, e.s, 3);
+    const double total = !thin ? e.s : (e.combined ? e.sum : dadd4(e.s, s1, s2, s3));
+    if (lane == 0) {
+        double rhs = s.rhs;
+        if (a.rhs_sub) rhs = __dsub_rn(rhs, *a.rhs_sub);
+        const double y = __ddiv_rn(__dsub_rn(rhs, total), s.d);
+        segv[s.r - a.seg_first] = y;
+        a.out[s.r] = y;
+        if (a.copy_out) a.copy_out[s.r] = y;
+    }
+}
+
+__global__ void __launch_bounds__(kSegThreads, 1) k_seg64(const sweep_args<double> a) {
+    if (a.skip && *a.skip) return;
+    if (a.err->code != 0) return;
+    extern __shared__ double segv[];
+    const unsigned warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    seg_slot cur, nxt;
+    seg_fetch64(a, warp, cur);
+    for (uint32_t l = 0; l < a.seg_levels; ++l) {
+        const uint32_t w0 = __ldg(a.seg_lvl + l), hi = __ldg(a.seg_lvl + l + 1) & 0x7fffffffu;
+        const bool thin = (w0 >> 31) != 0;
+        while (cur.i < hi) {
+            seg_fetch64(a, cur.i + nw, nxt);
+            seg_solve64(a, cur, thin, segv);
+            cur = nxt;
+        }
+        __syncthreads();
+    }
+}
+
+// fp32, K right-hand sides: lanes stride the row's entries, operands from
+// shared memory (inside the segment) or the output vector (final), fixed
+// butterfly.
+template <int K>
+__global__ void __launch_bounds__(kSegThreads, 1) k_seg32(const sweep_args<float> a, const double* in64) {
+    if (a.skip && *a.skip) return;
+    if (a.err->code != 0) return;
+    extern __shared__ float segf[];
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const uint32_t s0 = a.seg_first, s1 = a.seg_first + a.seg_rows;
+    uint32_t i = warp;
+    for (uint32_t l = 0; l < a.seg_levels; ++l) {
+        const uint32_t hi = __ldg(a.seg_lvl + l + 1) & 0x7fffffffu;
+        for (; i < hi; i += nw) {
+            const uint32_t r = __ldg(a.seg_row + i), q = __ldg(a.seg_ptr + i);
+            const uint32_t len = __ldg(a.seg_ptr + i + 1) - q - 1u;
+            float acc[K];
+#pragma unroll
+            for (int c = 0; c < K; ++c) acc[c] = 0.0f;
+            for (uint32_t t = lane; t < len; t += 32u) {
+                const uint32_t j = __ldg(a.seg_idx + q + t);
+                const float w = __ldg(a.seg_val + q + t);
+                const float* src = (j >= s0 && j < s1) ? segf + static_cast<size_t>(j - s0) * K
+                                                       : a.out + static_cast<size_t>(j) * K;
+#pragma unroll
+                for (int c = 0; c < K; ++c) acc[c] = __fmaf_rn(w, src[c], acc[c]);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                for (int c = 0; c < K; ++c) acc[c] += __shfl_xor_sync(kFull, acc[c], o);
+            if (lane == 0) {
+                const size_t base = static_cast<size_t>(r) * K;
+                const float d = __ldg(a.seg_val + q + len);
+#pragma unroll
+                for (int c = 0; c < K; ++c) {
+                    float rhs;
+                    if (in64) {
+                        double x = in64[base + c];
+                        if (a.rhs_sub) x -= a.rhs_sub[c];
+                        rhs = static_cast<float>(x);
+                    } else {
+                        rhs = a.in[base + c];
+                    }
+                    if (a.reset) a.reset[base + c] = sent_of(0.0f);
+                    const float y = __fdiv_rn(rhs - acc[c], d);
+                    segf[static_cast<size_t>(r - s0) * K + c] = y;
+                    a.out[base + c] = y;
+                    if (a.copy_out) a.copy_out[base + c] = y;
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void k_fill64(double* p, size_t n, double v) {
     for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<size_t>(gridDim.x) * blockDim.x)
@@ -599,19 +762,39 @@ int occ32() {
     return b0 < b1 ? b0 : b1;
 }
 
+template <class F>
+void set_smem(F* kernel, size_t bytes) {
+    if (bytes > 48 * 1024)
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+}
+
+template <int K>
+void seg32(const sweep_args<float>& a, const double* in64, cudaStream_t s) {
+    const size_t smem = static_cast<size_t>(a.seg_rows) * K * sizeof(float);
+    set_smem(k_seg32<K>, smem);
+    k_seg32<K><<<1, kSegThreads, smem, s>>>(a, in64);
+}
+
 template <int K>
 void sweep32_dir(int dir, const sweep_args<float>& a, const double* in64, int grid, cudaStream_t s) {
-    if (!a.n_items) return;
-    if (dir == 0) k_df32<0, K><<<grid, kSweepThreads, 0, s>>>(a, in64);
-    else          k_df32<1, K><<<grid, kSweepThreads, 0, s>>>(a, in64);
+    if (dir == 1 && a.seg_rows) seg32<K>(a, in64, s);
+    if (a.n_items) {
+        if (dir == 0) k_df32<0, K><<<grid, kSweepThreads, 0, s>>>(a, in64);
+        else          k_df32<1, K><<<grid, kSweepThreads, 0, s>>>(a, in64);
+    }
+    if (dir == 0 && a.seg_rows) seg32<K>(a, in64, s);
 }
 
 }  // namespace
 
 void launch_sweep64(int dir, const sweep_args<double>& a, int grid, cudaStream_t s) {
-    if (!a.n_items) return;
-    if (dir == 0) k_df64<0><<<grid, kSweepThreads, 0, s>>>(a);
-    else          k_df64<1><<<grid, kSweepThreads, 0, s>>>(a);
+    const size_t smem = static_cast<size_t>(a.seg_rows) * sizeof(double);
+    if (dir == 1 && a.seg_rows) { set_smem(k_seg64, smem); k_seg64<<<1, kSegThreads, smem, s>>>(a); }
+    if (a.n_items) {
+        if (dir == 0) k_df64<0><<<grid, kSweepThreads, 0, s>>>(a);
+        else          k_df64<1><<<grid, kSweepThreads, 0, s>>>(a);
+    }
+    if (dir == 0 && a.seg_rows) { set_smem(k_seg64, smem); k_seg64<<<1, kSegThreads, smem, s>>>(a); }
 }
 
 void launch_sweep32(int dir, const sweep_args<float>& a, int grid, cudaStream_t s) {

@@ -119,3 +119,21 @@ def test_apply_sddm_is_bit_exact_and_laplacian_close(eng):
         z, rz = D.apply(g["b"])
         zo = O.apply(g["b"], reset=(k == 0))
         assert np.linalg.norm(z - zo) <= 1e-12 * np.linalg.norm(zo), k
+
+
+@pytest.mark.parametrize("name", ["grid3d_48", "grid2d_256"])
+def test_serial_segment_path_is_bit_exact(eng, name, monkeypatch):
+    """The optional serial-segment launch (tiny trailing levels solved by one
+    block through shared memory) gives the same bytes as the dataflow path."""
+    A, F = problem(name)
+    O = oracle.Oracle(A, F)
+    monkeypatch.setenv("APXB_SEG_LEVEL_ROWS", "64")
+    D = native.DeviceFactor(eng, F)
+    D32 = native.DeviceFactor(eng, F, precision=native.PREC_FP32)
+    monkeypatch.delenv("APXB_SEG_LEVEL_ROWS")
+    D64_plain = native.DeviceFactor(eng, F, precision=native.PREC_FP32)
+    x = np.random.default_rng(6).standard_normal(F.m)
+    assert np.array_equal(_pair_dev(eng, D, x), O.pair(x))
+    z32 = _pair_dev(eng, D32, x)
+    want = O.pair(x)
+    assert np.linalg.norm(z32 - want) / np.linalg.norm(want) < FP32_SWEEP_RTOL
