@@ -1,0 +1,882 @@
+// Batched solve engine: many right-hand sides of one or several systems per
+// launch (the mixed-precision form).
+//
+//  * A batch holds S instances (each a factor + operator pair, block-diagonal
+//    in one combined permuted index space) and K right-hand-side slots per
+//    instance; vectors are row-interleaved [row][K], so every factor and
+//    operator entry is read once for all K columns.
+//  * Preconditioner: the fp32 sweeps with fp32 accumulation over a combined
+//    work plan (items of all instances, level by level: uneven instances share
+//    one launch). Everything else -- SpMV, residual update, dots, centring,
+//    the final true residual -- is fp64.
+//  * Each slot runs its own PCG (the reference cpu_solver's semantics,
+//    src/solve.cpp:478-654): per-slot scalars live on the device and are
+//    produced by one finalize kernel per reduction from per-tile partials
+//    summed in tile order (deterministic). A slot is "fresh" for one
+//    iteration after admission: that iteration's x/r update is skipped and
+//    its reductions initialise the slot, so a new right-hand side can join a
+//    running batch at any iteration boundary (continuous batching).
+//  * The iteration is a CUDA graph; a full solve runs it under a conditional
+//    WHILE node until every slot is done.
+#include <algorithm>
+
+#include "objects.hpp"
+
+namespace {
+
+constexpr uint32_t kTile = 1024;   // rows per reduction tile
+constexpr int kBT = 256;           // threads per block of the vector kernels
+
+enum fin_mode : int { kFinSpmv = 0, kFinXr = 1, kFinZsum = 2, kFinRz = 3, kFinResid = 4 };
+
+// Device pointers and settings of a batch.
+struct bp {
+    int K;
+    unsigned S, n_tot, n_tiles;
+    const unsigned* tile_inst; const unsigned* tile_lo; const unsigned* tile_hi;
+    const unsigned* inst_t0; const unsigned* inst_t1;
+    const unsigned* inst_off; const unsigned* inst_n; const int* inst_lap;
+    const int32_t* a_ptr; const int32_t* a_idx; const double* a_val;
+    const uint32_t* igperm;    // permuted position -> original (global) index
+    double *x, *r, *p, *Ap, *b;
+    float* rhs32;
+    const float* z;
+    // per slot [S*K]
+    double *rz, *pAp, *alpha, *beta, *rr, *rs, *bnorm, *rnorm, *prev, *mean, *shift, *xmean, *tres;
+    int *iters, *done, *status, *pmode, *center, *fresh;
+    unsigned long long* applies;
+    int* all_done;
+    double tol;
+    int max_iter, stag, center_k;
+    double* partials;          // [n_tiles][K][2]
+    apxb::dev_error* err;
+};
+
+// Block-level deterministic sum of NV values, result stored to partials[t][*].
+template <int NV>
+__device__ __forceinline__ void tile_store(double (&v)[NV], double* dst) {
+    __shared__ double red[NV * 32];
+    apxb::block_sum<NV>(v, red);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) dst[k] = v[k];
+    __syncthreads();
+}
+
+// x = 0, r = b = P B (fresh slots only); B in the caller's layout: instance i,
+// column c, original local index v at B[K * off_i + c * n_i + v]. Columns
+// >= nrhs[i] are zero (their slots finish at once).
+template <int K>
+__global__ void __launch_bounds__(kBT) k_b_admit(bp P, const double* B, const int* nrhs) {
+    for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
+        const unsigned i = P.tile_inst[t], off = P.inst_off[i], ni = P.inst_n[i];
+        for (unsigned pos = P.tile_lo[t] + threadIdx.x; pos < P.tile_hi[t]; pos += blockDim.x) {
+            const unsigned v = P.igperm[pos] - off;
+#pragma unroll
+            for (int c = 0; c < K; ++c) {
+                const unsigned sl = i * K + c;
+                if (!P.fresh[sl]) continue;
+                const double bv = c < nrhs[i] ? B[static_cast<size_t>(K) * off + static_cast<size_t>(c) * ni + v] : 0.0;
+                const size_t q = static_cast<size_t>(pos) * K + c;
+                P.b[q] = bv; P.r[q] = bv; P.x[q] = 0.0; P.p[q] = 0.0;
+            }
+        }
+    }
+}
+
+// Ap = A p with per-slot p.Ap partials (mode 0), or Y = A X (mode 1).
+template <int K>
+__global__ void __launch_bounds__(kBT) k_b_spmv(bp P, const double* X, double* Y, int mode) {
+    if (*P.all_done && mode == 0) return;
+    for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
+        double part[K];
+#pragma unroll
+        for (int c = 0; c < K; ++c) part[c] = 0.0;
+        for (unsigned row = P.tile_lo[t] + threadIdx.x; row < P.tile_hi[t]; row += blockDim.x) {
+            double acc[K];
+#pragma unroll
+            for (int c = 0; c < K; ++c) acc[c] = 0.0;
+            const int e = __ldg(P.a_ptr + row + 1);
+            for (int k = __ldg(P.a_ptr + row); k < e; ++k) {
+                const double w = __ldg(P.a_val + k);
+                const double* src = X + static_cast<size_t>(__ldg(P.a_idx + k)) * K;
+#pragma unroll
+                for (int c = 0; c < K; ++c) acc[c] = fma(w, src[c], acc[c]);
+            }
+            double* dst = Y + static_cast<size_t>(row) * K;
+#pragma unroll
+            for (int c = 0; c < K; ++c) {
+                dst[c] = acc[c];
+                if (mode == 0) part[c] = fma(X[static_cast<size_t>(row) * K + c], acc[c], part[c]);
+            }
+        }
+        if (mode == 0) tile_store<K>(part, P.partials + static_cast<size_t>(t) * K * 2);
+    }
+}
+
+// x += alpha p; r -= alpha Ap (not for fresh or done slots); r.r and sum(r) partials.
+template <int K>
+__global__ void __launch_bounds__(kBT) k_b_xr(bp P) {
+    if (*P.all_done) return;
+    for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
+        const unsigned i = P.tile_inst[t];
+        double a[K], v[2 * K];
+#pragma unroll
+        for (int c = 0; c < K; ++c) {
+            const unsigned sl = i * K + c;
+            a[c] = (P.fresh[sl] || P.done[sl]) ? 0.0 : P.alpha[sl];
+            v[c] = 0.0; v[K + c] = 0.0;
+        }
+        for (unsigned row = P.tile_lo[t] + threadIdx.x; row < P.tile_hi[t]; row += blockDim.x) {
+#pragma unroll
+            for (int c = 0; c < K; ++c) {
+                const size_t q = static_cast<size_t>(row) * K + c;
+                P.x[q] = fma(a[c], P.p[q], P.x[q]);
+                const double ri = fma(-a[c], P.Ap[q], P.r[q]);
+                P.r[q] = ri;
+                v[c] = fma(ri, ri, v[c]);
+                v[K + c] += ri;
+            }
+        }
+        double w[2 * K];
+#pragma unroll
+        for (int c = 0; c < 2 * K; ++c) w[c] = v[c];
+        tile_store<2 * K>(w, P.partials + static_cast<size_t>(t) * K * 2);
+    }
+}
+
+// fp32 preconditioner input: r - mean (the center-k input centring).
+template <int K>
+__global__ void __launch_bounds__(kBT) k_b_prep(bp P) {
+    if (*P.all_done) return;
+    for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
+        const unsigned i = P.tile_inst[t];
+        double mu[K];
+#pragma unroll
+        for (int c = 0; c < K; ++c) mu[c] = P.mean[i * K + c];
+        for (unsigned row = P.tile_lo[t] + threadIdx.x; row < P.tile_hi[t]; row += blockDim.x)
+#pragma unroll
+            for (int c = 0; c < K; ++c) {
+                const size_t q = static_cast<size_t>(row) * K + c;
+                P.rhs32[q] = static_cast<float>(P.r[q] - mu[c]);
+            }
+    }
+}
+
+// sum(z) partials (Laplacian instances; z = 0 at the grounded row).
+template <int K>
+__global__ void __launch_bounds__(kBT) k_b_zsum(bp P) {
+    if (*P.all_done) return;
+    for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
+        const unsigned i = P.tile_inst[t];
+        double v[K];
+#pragma unroll
+        for (int c = 0; c < K; ++c) v[c] = 0.0;
+        if (P.inst_lap[i])
+            for (unsigned row = P.tile_lo[t] + threadIdx.x; row < P.tile_hi[t]; row += blockDim.x)
+#pragma unroll
+                for (int c = 0; c < K; ++c) v[c] += static_cast<double>(P.z[static_cast<size_t>(row) * K + c]);
+        tile_store<K>(v, P.partials + static_cast<size_t>(t) * K * 2);
+    }
+}
+
+// r.(z - shift) partials.
+template <int K>
+__global__ void __launch_bounds__(kBT) k_b_rz(bp P) {
+    if (*P.all_done) return;
+    for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
+        const unsigned i = P.tile_inst[t];
+        double sh[K], v[K];
+#pragma unroll
+        for (int c = 0; c < K; ++c) { sh[c] = P.shift[i * K + c]; v[c] = 0.0; }
+        for (unsigned row = P.tile_lo[t] + threadIdx.x; row < P.tile_hi[t]; row += blockDim.x)
+#pragma unroll
+            for (int c = 0; c < K; ++c) {
+                const size_t q = static_cast<size_t>(row) * K + c;
+                v[c] = fma(P.r[q], static_cast<double>(P.z[q]) - sh[c], v[c]);
+            }
+        tile_store<K>(v, P.partials + static_cast<size_t>(t) * K * 2);
+    }
+}
+
+// p = (z - shift) + beta p; first application of a slot: p = z - shift.
+// Clears `fresh` (every slot has now been through one full iteration) and
+// sets the graph's WHILE condition.
+template <int K>
+__global__ void __launch_bounds__(kBT) k_b_up(bp P, unsigned long long handle, int use_cond) {
+    const bool stop = *P.all_done != 0 || P.err->code != 0;
+    if (use_cond && blockIdx.x == 0 && threadIdx.x == 0)
+        cudaGraphSetConditional(static_cast<cudaGraphConditionalHandle>(handle), stop ? 0u : 1u);
+    if (stop) return;
+    for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
+        const unsigned i = P.tile_inst[t];
+        double sh[K], be[K];
+        bool cp[K], live[K];
+#pragma unroll
+        for (int c = 0; c < K; ++c) {
+            const unsigned sl = i * K + c;
+            sh[c] = P.shift[sl]; be[c] = P.beta[sl]; cp[c] = P.pmode[sl] == 1; live[c] = !P.done[sl];
+        }
+        for (unsigned row = P.tile_lo[t] + threadIdx.x; row < P.tile_hi[t]; row += blockDim.x)
+#pragma unroll
+            for (int c = 0; c < K; ++c) {
+                if (!live[c]) continue;
+                const size_t q = static_cast<size_t>(row) * K + c;
+                const double zi = static_cast<double>(P.z[q]) - sh[c];
+                P.p[q] = cp[c] ? zi : fma(be[c], P.p[q], zi);
+            }
+    }
+}
+
+// Per-slot scalars from the tile partials (summed in tile order), then the
+// PCG state machine of the reduction that produced them.
+__global__ void __launch_bounds__(kBT) k_b_fin(bp P, int mode) {
+    __shared__ int any_live;
+    if (threadIdx.x == 0) any_live = 0;
+    __syncthreads();
+    const unsigned nslots = P.S * P.K;
+    if (!(*P.all_done) || mode == kFinResid) {
+        for (unsigned sl = threadIdx.x; sl < nslots; sl += blockDim.x) {
+            const unsigned i = sl / P.K, c = sl % P.K;
+            double s0 = 0.0, s1 = 0.0;
+            const int nv = (mode == kFinXr || mode == kFinResid) ? 2 : 1;
+            for (unsigned t = P.inst_t0[i]; t < P.inst_t1[i]; ++t) {
+                const double* src = P.partials + static_cast<size_t>(t) * P.K * 2;
+                if (nv == 2) { s0 += src[c]; s1 += src[P.K + c]; }
+                else s0 += src[c];
+            }
+            const double ni = static_cast<double>(P.inst_n[i]);
+            if (mode == kFinResid) {
+                P.tres[sl] = s1 > 0.0 ? sqrt(s0) / sqrt(s1) : 0.0;
+                continue;
+            }
+            if (P.done[sl] && !P.fresh[sl]) continue;
+            switch (mode) {
+                case kFinSpmv:
+                    P.pAp[sl] = s0;
+                    if (!P.fresh[sl]) {
+                        P.pmode[sl] = 0;
+                        if (s0 <= 0.0) { P.done[sl] = 1; P.status[sl] = 3; }
+                        else P.alpha[sl] = P.rz[sl] / s0;
+                    }
+                    break;
+                case kFinXr: {
+                    P.rr[sl] = s0;
+                    P.rs[sl] = s1;
+                    bool fin = false;
+                    if (P.fresh[sl]) {
+                        // initial residual r = b (src/solve.cpp:543-551)
+                        P.bnorm[sl] = sqrt(s0);
+                        P.iters[sl] = 0;
+                        P.prev[sl] = 1.0;
+                        P.pmode[sl] = 1;
+                        P.applies[sl] = 0;
+                        if (P.bnorm[sl] == 0.0) { P.done[sl] = 1; P.status[sl] = 0; P.rnorm[sl] = 0.0; fin = true; }
+                        else { P.rnorm[sl] = 1.0; P.status[sl] = 1; P.done[sl] = 0; }
+                    } else {
+                        const double rn = sqrt(s0) / P.bnorm[sl];
+                        P.rnorm[sl] = rn;
+                        const int it = ++P.iters[sl];
+                        int status = 1;
+                        if (rn < P.tol) { fin = true; status = 0; }
+                        else if (!isfinite(rn)) { fin = true; status = 4; }
+                        else if (P.stag > 0 && it % P.stag == 0) {
+                            if (rn > P.prev[sl] * 0.5) { fin = true; status = 2; }
+                            else P.prev[sl] = rn;
+                        }
+                        if (!fin && it >= P.max_iter) { fin = true; status = 1; }
+                        P.status[sl] = status;
+                        if (fin) P.done[sl] = 1;
+                    }
+                    if (!fin) {
+                        const unsigned long long ap = ++P.applies[sl];
+                        const int cen = P.inst_lap[i] && (ap % static_cast<unsigned long long>(P.center_k)) == 0;
+                        P.center[sl] = cen;
+                        P.mean[sl] = cen ? s1 / ni : 0.0;
+                        P.shift[sl] = 0.0;
+                    } else {
+                        P.mean[sl] = 0.0;
+                    }
+                    break;
+                }
+                case kFinZsum:
+                    P.shift[sl] = P.center[sl] ? s0 / ni : 0.0;
+                    break;
+                case kFinRz:
+                    P.beta[sl] = P.pmode[sl] == 1 ? 0.0 : s0 / P.rz[sl];
+                    P.rz[sl] = s0;
+                    P.fresh[sl] = 0;
+                    break;
+                default:
+                    break;
+            }
+        }
+    }
+    __syncthreads();
+    if (mode == kFinXr || mode == kFinSpmv) {
+        for (unsigned sl = threadIdx.x; sl < nslots; sl += blockDim.x)
+            if (!P.done[sl]) any_live = 1;
+        __syncthreads();
+        if (threadIdx.x == 0) *P.all_done = any_live ? 0 : 1;
+    }
+}
+
+// x out to the caller's layout, minus the slot's mean for Laplacian instances
+// (min-norm solution, src/solve.cpp:631-634); xmean from k_b_xsum.
+template <int K>
+__global__ void __launch_bounds__(kBT) k_b_xsum(bp P) {
+    for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
+        double v[K];
+#pragma unroll
+        for (int c = 0; c < K; ++c) v[c] = 0.0;
+        for (unsigned row = P.tile_lo[t] + threadIdx.x; row < P.tile_hi[t]; row += blockDim.x)
+#pragma unroll
+            for (int c = 0; c < K; ++c) v[c] += P.x[static_cast<size_t>(row) * K + c];
+        tile_store<K>(v, P.partials + static_cast<size_t>(t) * K * 2);
+    }
+}
+
+__global__ void __launch_bounds__(kBT) k_b_xmean(bp P) {
+    const unsigned nslots = P.S * P.K;
+    for (unsigned sl = threadIdx.x; sl < nslots; sl += blockDim.x) {
+        const unsigned i = sl / P.K, c = sl % P.K;
+        double s = 0.0;
+        for (unsigned t = P.inst_t0[i]; t < P.inst_t1[i]; ++t) s += P.partials[static_cast<size_t>(t) * P.K * 2 + c];
+        P.xmean[sl] = (P.inst_lap[i] && P.bnorm[sl] > 0.0) ? s / static_cast<double>(P.inst_n[i]) : 0.0;
+    }
+}
+
+template <int K>
+__global__ void __launch_bounds__(kBT) k_b_out(bp P, double* X) {
+    for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
+        const unsigned i = P.tile_inst[t], off = P.inst_off[i], ni = P.inst_n[i];
+        for (unsigned pos = P.tile_lo[t] + threadIdx.x; pos < P.tile_hi[t]; pos += blockDim.x) {
+            const unsigned v = P.igperm[pos] - off;
+#pragma unroll
+            for (int c = 0; c < K; ++c)
+                X[static_cast<size_t>(K) * off + static_cast<size_t>(c) * ni + v] =
+                    P.x[static_cast<size_t>(pos) * K + c] - P.xmean[i * K + c];
+        }
+    }
+}
+
+// ||b - A x||^2 and ||b||^2 partials with A x in Ap.
+template <int K>
+__global__ void __launch_bounds__(kBT) k_b_resid(bp P) {
+    for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
+        double v[2 * K];
+#pragma unroll
+        for (int c = 0; c < 2 * K; ++c) v[c] = 0.0;
+        for (unsigned row = P.tile_lo[t] + threadIdx.x; row < P.tile_hi[t]; row += blockDim.x)
+#pragma unroll
+            for (int c = 0; c < K; ++c) {
+                const size_t q = static_cast<size_t>(row) * K + c;
+                const double d = P.b[q] - P.Ap[q];
+                v[c] = fma(d, d, v[c]);
+                v[K + c] = fma(P.b[q], P.b[q], v[K + c]);
+            }
+        tile_store<2 * K>(v, P.partials + static_cast<size_t>(t) * K * 2);
+    }
+}
+
+__global__ void k_b_zero_rows(float* z, const uint32_t* rows, unsigned n, int K) {
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n * static_cast<unsigned>(K); i += gridDim.x * blockDim.x)
+        z[static_cast<size_t>(rows[i / K]) * K + (i % K)] = 0.0f;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Host side.
+
+struct apxb_batch {
+    apxb_engine* e = nullptr;
+    int S = 0, K = 0;
+    uint32_t n_tot = 0;
+    std::vector<uint32_t> off, n;
+    std::vector<int> lap;
+    std::vector<std::pair<void*, size_t>> owned;
+    // sweep plan per direction (borrowed from a single factor or combined)
+    uint32_t n_items[2] = {0, 0};
+    const uint32_t *info[2] = {nullptr, nullptr}, *ord[2] = {nullptr, nullptr}, *ptr[2] = {nullptr, nullptr};
+    const uint32_t* idx[2] = {nullptr, nullptr};
+    const float* val[2] = {nullptr, nullptr};
+    apxb::sweep_ctl* ctl = nullptr;
+    int grid32 = 0;
+    // operator (combined, permuted) and permutation
+    const int32_t *a_ptr = nullptr, *a_idx = nullptr;
+    const double* a_val = nullptr;
+    uint32_t* igperm = nullptr;
+    // tiles
+    uint32_t n_tiles = 0;
+    uint32_t *tile_inst = nullptr, *tile_lo = nullptr, *tile_hi = nullptr, *inst_t0 = nullptr, *inst_t1 = nullptr;
+    uint32_t *inst_off = nullptr, *inst_n = nullptr;
+    int* inst_lap = nullptr;
+    int* nrhs = nullptr;
+    // vectors and state
+    double *x = nullptr, *r = nullptr, *p = nullptr, *Ap = nullptr, *b = nullptr;
+    float *rhs32 = nullptr, *Yf = nullptr, *Zf = nullptr;
+    bool y_armed = false;
+    double* sd = nullptr;   // 13 double arrays of S*K
+    int* si = nullptr;      // 6 int arrays of S*K + all_done
+    unsigned long long* applies = nullptr;
+    double* partials = nullptr;
+    double* d_B = nullptr;  // staging of right-hand sides / solutions in the caller layout
+    // graphs (tol / max_iter are baked into them)
+    cudaGraphExec_t loop = nullptr;
+    cudaGraphExec_t one = nullptr;
+    bool loop_cond = false;
+    double graph_tol = -1.0;
+    int graph_max = -1;
+    // pinned host mirrors
+    double* h_sd = nullptr;
+    int* h_si = nullptr;
+
+    template <class T>
+    int dalloc(T** q, size_t count) {
+        const size_t bytes = count * sizeof(T);
+        const int rc = e->alloc(reinterpret_cast<void**>(q), bytes);
+        if (rc) return rc;
+        owned.emplace_back(*q, bytes);
+        return APXB_OK;
+    }
+    ~apxb_batch() {
+        if (loop) cudaGraphExecDestroy(loop);
+        if (one) cudaGraphExecDestroy(one);
+        for (auto& [q, bytes] : owned) e->release(q, bytes);
+        if (h_sd) cudaFreeHost(h_sd);
+        if (h_si) cudaFreeHost(h_si);
+    }
+    size_t slots() const { return static_cast<size_t>(S) * K; }
+    bp params(double tol, int max_iter) const {
+        bp P{};
+        P.K = K; P.S = S; P.n_tot = n_tot; P.n_tiles = n_tiles;
+        P.tile_inst = tile_inst; P.tile_lo = tile_lo; P.tile_hi = tile_hi; P.inst_t0 = inst_t0; P.inst_t1 = inst_t1;
+        P.inst_off = inst_off; P.inst_n = inst_n; P.inst_lap = inst_lap;
+        P.a_ptr = a_ptr; P.a_idx = a_idx; P.a_val = a_val; P.igperm = igperm;
+        P.x = x; P.r = r; P.p = p; P.Ap = Ap; P.b = b; P.rhs32 = rhs32; P.z = Zf;
+        const size_t ns = slots();
+        double* d = sd;
+        P.rz = d; P.pAp = d + ns; P.alpha = d + 2 * ns; P.beta = d + 3 * ns; P.rr = d + 4 * ns; P.rs = d + 5 * ns;
+        P.bnorm = d + 6 * ns; P.rnorm = d + 7 * ns; P.prev = d + 8 * ns; P.mean = d + 9 * ns; P.shift = d + 10 * ns;
+        P.xmean = d + 11 * ns; P.tres = d + 12 * ns;
+        int* s = si;
+        P.iters = s; P.done = s + ns; P.status = s + 2 * ns; P.pmode = s + 3 * ns; P.center = s + 4 * ns;
+        P.fresh = s + 5 * ns; P.all_done = s + 6 * ns;
+        P.applies = applies;
+        P.tol = tol; P.max_iter = max_iter; P.stag = 50; P.center_k = e->center_k;
+        P.partials = partials; P.err = e->d_err;
+        return P;
+    }
+};
+
+namespace {
+
+// Combined work plan of several factors (fp32 sweeps): the instances' items
+// merged level by level, rows and columns shifted to the combined index space.
+void combine_plans(const std::vector<const apxb_factor*>& fs, const std::vector<uint32_t>& off, int dir,
+                   apxb::sweep_plan& out) {
+    out = apxb::sweep_plan{};
+    // items of each instance are already in level order; merge by level using
+    // the level of each item's first row
+    struct src_item { uint32_t inst, item; int32_t level; };
+    std::vector<src_item> all;
+    for (uint32_t i = 0; i < fs.size(); ++i) {
+        const apxb::sweep_plan& pl = dir == 0 ? fs[i]->h.fwd_plan : fs[i]->h.bck_plan;
+        const std::vector<int32_t>& lev = dir == 0 ? fs[i]->h.fwd_level : fs[i]->h.bck_level;
+        for (uint32_t c = 0; c < pl.n_items; ++c)
+            all.push_back({i, c, lev[pl.ord[static_cast<size_t>(c) * 32]]});
+    }
+    std::stable_sort(all.begin(), all.end(), [](const src_item& a, const src_item& b) { return a.level < b.level; });
+    out.n_items = static_cast<uint32_t>(all.size());
+    out.info.resize(all.size());
+    out.ord.assign(all.size() * 32, apxb::kNoRow);
+    out.ptr.assign(all.size() * 32 + 1, 0);
+    uint32_t e = 0;
+    for (size_t c = 0; c < all.size(); ++c) {
+        const auto& sit = all[c];
+        const apxb::sweep_plan& pl = dir == 0 ? fs[sit.inst]->h.fwd_plan : fs[sit.inst]->h.bck_plan;
+        out.info[c] = pl.info[sit.item] & 0xffffu;   // count | lg (no exact-order flag in fp32)
+        for (uint32_t s = 0; s < 32; ++s) {
+            const size_t sp = static_cast<size_t>(sit.item) * 32 + s, dp = c * 32 + s;
+            out.ptr[dp] = e;
+            if (pl.ord[sp] == apxb::kNoRow) continue;
+            out.ord[dp] = pl.ord[sp] + off[sit.inst];
+            for (uint32_t q = pl.ptr[sp]; q < pl.ptr[sp + 1]; ++q) {
+                out.idx.push_back(pl.idx[q] + off[sit.inst]);
+                out.val.push_back(pl.val[q]);
+                ++e;
+            }
+        }
+    }
+    out.ptr[all.size() * 32] = e;
+}
+
+template <int K>
+int launch_iteration_k(apxb_batch* bt, const bp& P, cudaStream_t s, unsigned long long h, int use_cond) {
+    const int g = bt->e->vec_grid;
+    k_b_spmv<K><<<g, kBT, 0, s>>>(P, P.p, P.Ap, 0);
+    k_b_fin<<<1, kBT, 0, s>>>(P, kFinSpmv);
+    k_b_xr<K><<<g, kBT, 0, s>>>(P);
+    k_b_fin<<<1, kBT, 0, s>>>(P, kFinXr);
+    k_b_prep<K><<<g, kBT, 0, s>>>(P);
+    apxb::sweep_args<float> a{};
+    a.k = K; a.err = bt->e->d_err; a.budget_ns = bt->e->budget_ns; a.skip = P.all_done;
+    a.m = bt->n_tot;
+    for (int dir = 0; dir < 2; ++dir) {
+        a.n_items = bt->n_items[dir]; a.info = bt->info[dir]; a.ord = bt->ord[dir]; a.ptr = bt->ptr[dir];
+        a.idx = bt->idx[dir]; a.val = bt->val[dir]; a.ctl = bt->ctl + dir;
+        if (dir == 0) { a.in = bt->rhs32; a.out = bt->Yf; a.reset = bt->Zf; }
+        else { a.in = bt->Yf; a.out = bt->Zf; a.reset = bt->Yf; }
+        apxb::launch_sweep32(dir, a, bt->grid32, s);
+    }
+    k_b_zsum<K><<<g, kBT, 0, s>>>(P);
+    k_b_fin<<<1, kBT, 0, s>>>(P, kFinZsum);
+    k_b_rz<K><<<g, kBT, 0, s>>>(P);
+    k_b_fin<<<1, kBT, 0, s>>>(P, kFinRz);
+    k_b_up<K><<<g, kBT, 0, s>>>(P, h, use_cond);
+    const cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return fail(APXB_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(err));
+    return APXB_OK;
+}
+
+int launch_iteration(apxb_batch* bt, const bp& P, cudaStream_t s, unsigned long long h, int use_cond) {
+    switch (bt->K) {
+        case 1: return launch_iteration_k<1>(bt, P, s, h, use_cond);
+        case 2: return launch_iteration_k<2>(bt, P, s, h, use_cond);
+        case 4: return launch_iteration_k<4>(bt, P, s, h, use_cond);
+        case 8: return launch_iteration_k<8>(bt, P, s, h, use_cond);
+        default: return launch_iteration_k<16>(bt, P, s, h, use_cond);
+    }
+}
+
+template <int K>
+void launch_finish_k(apxb_batch* bt, const bp& P, double* X, bool resid, cudaStream_t s) {
+    const int g = bt->e->vec_grid;
+    k_b_xsum<K><<<g, kBT, 0, s>>>(P);
+    k_b_xmean<<<1, kBT, 0, s>>>(P);
+    k_b_out<K><<<g, kBT, 0, s>>>(P, X);
+    if (resid) {
+        k_b_spmv<K><<<g, kBT, 0, s>>>(P, P.x, P.Ap, 1);
+        k_b_resid<K><<<g, kBT, 0, s>>>(P);
+        k_b_fin<<<1, kBT, 0, s>>>(P, kFinResid);
+    }
+}
+
+void launch_finish(apxb_batch* bt, const bp& P, double* X, bool resid, cudaStream_t s) {
+    switch (bt->K) {
+        case 1: launch_finish_k<1>(bt, P, X, resid, s); break;
+        case 2: launch_finish_k<2>(bt, P, X, resid, s); break;
+        case 4: launch_finish_k<4>(bt, P, X, resid, s); break;
+        case 8: launch_finish_k<8>(bt, P, X, resid, s); break;
+        default: launch_finish_k<16>(bt, P, X, resid, s); break;
+    }
+}
+
+template <int K>
+void launch_admit_k(apxb_batch* bt, const bp& P, const double* B, cudaStream_t s) {
+    k_b_admit<K><<<bt->e->vec_grid, kBT, 0, s>>>(P, B, bt->nrhs);
+}
+
+void launch_admit(apxb_batch* bt, const bp& P, const double* B, cudaStream_t s) {
+    switch (bt->K) {
+        case 1: launch_admit_k<1>(bt, P, B, s); break;
+        case 2: launch_admit_k<2>(bt, P, B, s); break;
+        case 4: launch_admit_k<4>(bt, P, B, s); break;
+        case 8: launch_admit_k<8>(bt, P, B, s); break;
+        default: launch_admit_k<16>(bt, P, B, s); break;
+    }
+}
+
+int build_graphs(apxb_batch* bt, double tol, int max_iter) {
+    if (bt->loop) { cudaGraphExecDestroy(bt->loop); bt->loop = nullptr; }
+    if (bt->one) { cudaGraphExecDestroy(bt->one); bt->one = nullptr; }
+    cudaStream_t s = bt->e->stream;
+    const bp P = bt->params(tol, max_iter);
+    // one iteration (host-driven serving loop)
+    APXB_CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    int rc = launch_iteration(bt, P, s, 0, 0);
+    cudaGraph_t g1 = nullptr;
+    APXB_CK(cudaStreamEndCapture(s, &g1));
+    if (rc) { cudaGraphDestroy(g1); return rc; }
+    APXB_CK(cudaGraphInstantiate(&bt->one, g1, 0));
+    cudaGraphDestroy(g1);
+    // WHILE loop until every slot is done
+    cudaGraph_t g = nullptr;
+    APXB_CK(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle h;
+    cudaError_t err = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+    if (err == cudaSuccess) {
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        err = cudaGraphAddNode(&node, g, nullptr, 0, &cp);
+        if (err == cudaSuccess) {
+            err = cudaStreamBeginCaptureToGraph(s, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                cudaStreamCaptureModeThreadLocal);
+            if (err == cudaSuccess) {
+                rc = launch_iteration(bt, P, s, static_cast<unsigned long long>(h), 1);
+                cudaGraph_t captured = nullptr;
+                err = cudaStreamEndCapture(s, &captured);
+                if (rc) { cudaGraphDestroy(g); return rc; }
+            }
+        }
+        if (err == cudaSuccess) err = cudaGraphInstantiate(&bt->loop, g, 0);
+    }
+    cudaGraphDestroy(g);
+    bt->loop_cond = err == cudaSuccess;
+    if (!bt->loop_cond) { bt->loop = nullptr; cudaGetLastError(); }
+    return APXB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, apxb_operator* const* ops, int k,
+                      apxb_batch** out) {
+    if (!e || n_inst < 1 || !factors || !ops || !out) return fail(APXB_ERR_INVALID, "bad argument");
+    if (k != 1 && k != 2 && k != 4 && k != 8 && k != 16) return fail(APXB_ERR_INVALID, "k must be 1, 2, 4, 8 or 16");
+    *out = nullptr;
+    APXB_CK(cudaSetDevice(e->device));
+    std::unique_ptr<apxb_batch> bt(new (std::nothrow) apxb_batch);
+    if (!bt) return fail(APXB_ERR_INVALID, "host allocation failed");
+    bt->e = e; bt->S = n_inst; bt->K = k;
+    std::vector<const apxb_factor*> fs;
+    uint64_t nnz_a = 0;
+    for (int i = 0; i < n_inst; ++i) {
+        const apxb_factor* f = factors[i];
+        const apxb_operator* a = ops[i];
+        if (!f || !a || f->e != e || a->e != e) return fail(APXB_ERR_INVALID, "instance objects missing or on another engine");
+        if (a->n != f->h.n) return fail(APXB_ERR_INVALID, "instance operator / factor dimensions differ");
+        if (n_inst > 1 && (f->h.fwd_plan.seg_rows || f->h.bck_plan.seg_rows))
+            return fail(APXB_ERR_INVALID, "multi-instance batches need factors built without the serial segment");
+        bt->off.push_back(bt->n_tot);
+        bt->n.push_back(f->h.n);
+        bt->lap.push_back(f->h.sddm ? 0 : 1);
+        bt->n_tot += f->h.n;
+        nnz_a += a->nnz;
+        fs.push_back(f);
+    }
+    if (nnz_a >= 0x7fffffffull) return fail(APXB_ERR_INVALID, "combined operator exceeds the int32 range");
+    cudaStream_t s = e->stream;
+    const size_t nk = static_cast<size_t>(bt->n_tot) * k, ns = bt->slots();
+    int rc;
+    // ---- sweep plans ----
+    if (n_inst == 1) {
+        const apxb_factor* f = fs[0];
+        if (f->h.fwd_plan.seg_rows || f->h.bck_plan.seg_rows)
+            return fail(APXB_ERR_INVALID, "batches need a factor built without the serial segment");
+        for (int dir = 0; dir < 2; ++dir) {
+            const apxb::sweep_plan& pl = dir == 0 ? f->h.fwd_plan : f->h.bck_plan;
+            bt->n_items[dir] = pl.n_items;
+            bt->info[dir] = f->info[dir]; bt->ord[dir] = f->ord[dir]; bt->ptr[dir] = f->ptr[dir];
+            bt->idx[dir] = f->idx[dir]; bt->val[dir] = f->val[dir];
+        }
+    } else {
+        for (int dir = 0; dir < 2; ++dir) {
+            apxb::sweep_plan pl;
+            combine_plans(fs, bt->off, dir, pl);
+            uint32_t *info, *ord, *ptr, *idx;
+            float* val;
+            if ((rc = bt->dalloc(&info, pl.info.size())) || (rc = bt->dalloc(&ord, pl.ord.size())) ||
+                (rc = bt->dalloc(&ptr, pl.ptr.size())) || (rc = bt->dalloc(&idx, pl.idx.size())) ||
+                (rc = bt->dalloc(&val, pl.val.size())))
+                return rc;
+            APXB_CK(cudaMemcpyAsync(info, pl.info.data(), 4 * pl.info.size(), cudaMemcpyHostToDevice, s));
+            APXB_CK(cudaMemcpyAsync(ord, pl.ord.data(), 4 * pl.ord.size(), cudaMemcpyHostToDevice, s));
+            APXB_CK(cudaMemcpyAsync(ptr, pl.ptr.data(), 4 * pl.ptr.size(), cudaMemcpyHostToDevice, s));
+            APXB_CK(cudaMemcpyAsync(idx, pl.idx.data(), 4 * pl.idx.size(), cudaMemcpyHostToDevice, s));
+            APXB_CK(cudaMemcpyAsync(val, pl.val.data(), 4 * pl.val.size(), cudaMemcpyHostToDevice, s));
+            APXB_CK(cudaStreamSynchronize(s));
+            bt->n_items[dir] = pl.n_items;
+            bt->info[dir] = info; bt->ord[dir] = ord; bt->ptr[dir] = ptr; bt->idx[dir] = idx; bt->val[dir] = val;
+        }
+    }
+    if ((rc = bt->dalloc(&bt->ctl, 2))) return rc;
+    APXB_CK(cudaMemsetAsync(bt->ctl, 0, sizeof(apxb::sweep_ctl) * 2, s));
+    bt->grid32 = apxb::sweep_grid32(k, e->num_sms);
+    // ---- operator ----
+    if (n_inst == 1) {
+        bt->a_ptr = ops[0]->ptr; bt->a_idx = ops[0]->idx; bt->a_val = ops[0]->val;
+    } else {
+        int32_t *ap, *ai;
+        double* av;
+        if ((rc = bt->dalloc(&ap, bt->n_tot + 1)) || (rc = bt->dalloc(&ai, nnz_a)) || (rc = bt->dalloc(&av, nnz_a)))
+            return rc;
+        std::vector<int32_t> hp(bt->n_tot + 1, 0);
+        uint64_t base = 0;
+        for (int i = 0; i < n_inst; ++i) {
+            const apxb_operator* a = ops[i];
+            std::vector<int32_t> p(a->n + 1), ix(a->nnz);
+            APXB_CK(cudaMemcpy(p.data(), a->ptr, 4 * (static_cast<size_t>(a->n) + 1), cudaMemcpyDeviceToHost));
+            APXB_CK(cudaMemcpy(ix.data(), a->idx, 4 * a->nnz, cudaMemcpyDeviceToHost));
+            for (uint32_t r = 0; r <= a->n; ++r) hp[bt->off[i] + r] = static_cast<int32_t>(base + p[r]);
+            for (auto& c : ix) c += static_cast<int32_t>(bt->off[i]);
+            APXB_CK(cudaMemcpy(ai + base, ix.data(), 4 * a->nnz, cudaMemcpyHostToDevice));
+            APXB_CK(cudaMemcpy(av + base, a->val, 8 * a->nnz, cudaMemcpyDeviceToDevice));
+            base += a->nnz;
+        }
+        APXB_CK(cudaMemcpy(ap, hp.data(), 4 * hp.size(), cudaMemcpyHostToDevice));
+        bt->a_ptr = ap; bt->a_idx = ai; bt->a_val = av;
+    }
+    // ---- permutation (permuted position -> original global index), tiles ----
+    {
+        std::vector<uint32_t> ig(bt->n_tot);
+        std::vector<uint32_t> ti, tl, th, t0(n_inst), t1(n_inst);
+        for (int i = 0; i < n_inst; ++i) {
+            const auto& perm = fs[i]->h.perm;
+            for (uint32_t v = 0; v < bt->n[i]; ++v) ig[bt->off[i] + perm[v]] = bt->off[i] + v;
+            t0[i] = static_cast<uint32_t>(ti.size());
+            for (uint32_t lo = 0; lo < bt->n[i]; lo += kTile) {
+                ti.push_back(static_cast<uint32_t>(i));
+                tl.push_back(bt->off[i] + lo);
+                th.push_back(bt->off[i] + std::min(bt->n[i], lo + kTile));
+            }
+            t1[i] = static_cast<uint32_t>(ti.size());
+        }
+        bt->n_tiles = static_cast<uint32_t>(ti.size());
+        if ((rc = bt->dalloc(&bt->igperm, bt->n_tot)) || (rc = bt->dalloc(&bt->tile_inst, ti.size())) ||
+            (rc = bt->dalloc(&bt->tile_lo, ti.size())) || (rc = bt->dalloc(&bt->tile_hi, ti.size())) ||
+            (rc = bt->dalloc(&bt->inst_t0, n_inst)) || (rc = bt->dalloc(&bt->inst_t1, n_inst)) ||
+            (rc = bt->dalloc(&bt->inst_off, n_inst)) || (rc = bt->dalloc(&bt->inst_n, n_inst)) ||
+            (rc = bt->dalloc(&bt->inst_lap, n_inst)) || (rc = bt->dalloc(&bt->nrhs, n_inst)))
+            return rc;
+        APXB_CK(cudaMemcpy(bt->igperm, ig.data(), 4 * ig.size(), cudaMemcpyHostToDevice));
+        APXB_CK(cudaMemcpy(bt->tile_inst, ti.data(), 4 * ti.size(), cudaMemcpyHostToDevice));
+        APXB_CK(cudaMemcpy(bt->tile_lo, tl.data(), 4 * tl.size(), cudaMemcpyHostToDevice));
+        APXB_CK(cudaMemcpy(bt->tile_hi, th.data(), 4 * th.size(), cudaMemcpyHostToDevice));
+        APXB_CK(cudaMemcpy(bt->inst_t0, t0.data(), 4 * t0.size(), cudaMemcpyHostToDevice));
+        APXB_CK(cudaMemcpy(bt->inst_t1, t1.data(), 4 * t1.size(), cudaMemcpyHostToDevice));
+        APXB_CK(cudaMemcpy(bt->inst_off, bt->off.data(), 4 * bt->off.size(), cudaMemcpyHostToDevice));
+        APXB_CK(cudaMemcpy(bt->inst_n, bt->n.data(), 4 * bt->n.size(), cudaMemcpyHostToDevice));
+        APXB_CK(cudaMemcpy(bt->inst_lap, bt->lap.data(), 4 * bt->lap.size(), cudaMemcpyHostToDevice));
+    }
+    // ---- vectors, state ----
+    if ((rc = bt->dalloc(&bt->x, nk)) || (rc = bt->dalloc(&bt->r, nk)) || (rc = bt->dalloc(&bt->p, nk)) ||
+        (rc = bt->dalloc(&bt->Ap, nk)) || (rc = bt->dalloc(&bt->b, nk)) || (rc = bt->dalloc(&bt->rhs32, nk)) ||
+        (rc = bt->dalloc(&bt->Yf, nk)) || (rc = bt->dalloc(&bt->Zf, nk)) || (rc = bt->dalloc(&bt->sd, 13 * ns)) ||
+        (rc = bt->dalloc(&bt->si, 6 * ns + 1)) || (rc = bt->dalloc(&bt->applies, ns)) ||
+        (rc = bt->dalloc(&bt->partials, static_cast<size_t>(bt->n_tiles) * k * 2)) || (rc = bt->dalloc(&bt->d_B, nk)))
+        return rc;
+    APXB_CK(cudaMallocHost(&bt->h_sd, sizeof(double) * 13 * ns));
+    APXB_CK(cudaMallocHost(&bt->h_si, sizeof(int) * (6 * ns + 1)));
+    APXB_CK(cudaMemsetAsync(bt->sd, 0, sizeof(double) * 13 * ns, s));
+    APXB_CK(cudaMemsetAsync(bt->si, 0, sizeof(int) * (6 * ns + 1), s));
+    APXB_CK(cudaMemsetAsync(bt->applies, 0, sizeof(unsigned long long) * ns, s));
+    APXB_CK(cudaMemsetAsync(bt->p, 0, sizeof(double) * nk, s));
+    // Zf: markers on factor rows, 0 on each Laplacian instance's grounded row
+    apxb::launch_fill_sent32(bt->Yf, nk, s);
+    apxb::launch_fill_sent32(bt->Zf, nk, s);
+    {
+        std::vector<uint32_t> grounded;
+        for (int i = 0; i < n_inst; ++i)
+            if (bt->lap[i]) grounded.push_back(bt->off[i] + bt->n[i] - 1);
+        if (!grounded.empty()) {
+            uint32_t* gr;
+            if ((rc = bt->dalloc(&gr, grounded.size()))) return rc;
+            APXB_CK(cudaMemcpy(gr, grounded.data(), 4 * grounded.size(), cudaMemcpyHostToDevice));
+            k_b_zero_rows<<<1, 256, 0, s>>>(bt->Zf, gr, static_cast<unsigned>(grounded.size()), k);
+        }
+    }
+    bt->y_armed = true;
+    APXB_CK(cudaGetLastError());
+    APXB_CK(cudaStreamSynchronize(s));
+    e->children++;
+    *out = bt.release();
+    return APXB_OK;
+}
+
+int apxb_batch_destroy(apxb_batch* bt) {
+    if (!bt) return APXB_OK;
+    apxb_engine* e = bt->e;
+    cudaSetDevice(e->device);
+    cudaStreamSynchronize(e->stream);
+    delete bt;
+    apxb_detail::release_child(e);
+    return APXB_OK;
+}
+
+int apxb_batch_size(const apxb_batch* bt, int* n_inst, int* k, uint32_t* n_total) {
+    if (!bt) return fail(APXB_ERR_INVALID, "batch is NULL");
+    if (n_inst) *n_inst = bt->S;
+    if (k) *k = bt->K;
+    if (n_total) *n_total = bt->n_tot;
+    return APXB_OK;
+}
+
+int apxb_batch_solve(apxb_batch* bt, const double* B, double* X, const int* nrhs, double tol, int max_iter,
+                     int flags, apxb_pcg_result* res) {
+    if (!bt || !B || !X || !res) return fail(APXB_ERR_INVALID, "bad argument");
+    if (!(tol >= 0.0) || max_iter < 0) return fail(APXB_ERR_INVALID, "bad tol / max_iter");
+    apxb_engine* e = bt->e;
+    APXB_CK(cudaSetDevice(e->device));
+    cudaStream_t s = e->stream;
+    const size_t nk = static_cast<size_t>(bt->n_tot) * bt->K, ns = bt->slots();
+    const bool dev = flags & APXB_DEVICE_PTRS;
+    std::vector<int> nr(bt->S, bt->K);
+    if (nrhs)
+        for (int i = 0; i < bt->S; ++i) {
+            if (nrhs[i] < 0 || nrhs[i] > bt->K) return fail(APXB_ERR_INVALID, "nrhs out of range");
+            nr[i] = nrhs[i];
+        }
+    APXB_CK(cudaMemcpyAsync(bt->nrhs, nr.data(), sizeof(int) * nr.size(), cudaMemcpyHostToDevice, s));
+    const double* dB = B;
+    if (!dev) {
+        APXB_CK(cudaMemcpyAsync(bt->d_B, B, 8 * nk, cudaMemcpyHostToDevice, s));
+        dB = bt->d_B;
+    }
+    if (!bt->one || bt->graph_tol != tol || bt->graph_max != max_iter) {
+        const int rc = build_graphs(bt, tol, max_iter);
+        if (rc) return rc;
+        bt->graph_tol = tol;
+        bt->graph_max = max_iter;
+    }
+    const bp P = bt->params(tol, max_iter);
+    // every slot fresh, nothing done
+    std::vector<int> ones(ns, 1);
+    APXB_CK(cudaMemsetAsync(P.done, 0, sizeof(int) * ns, s));
+    APXB_CK(cudaMemcpyAsync(P.fresh, ones.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, s));
+    APXB_CK(cudaMemsetAsync(P.all_done, 0, sizeof(int), s));
+    // Only the forward output needs its markers now: the forward sweep re-arms
+    // every factor row of Zf itself, and Zf's grounded rows must stay 0.
+    if (!bt->y_armed) apxb::launch_fill_sent32(bt->Yf, nk, s);
+    bt->y_armed = true;
+    APXB_CK(cudaEventRecord(e->ev0, s));
+    launch_admit(bt, P, dB, s);
+    if (bt->loop_cond) {
+        APXB_CK(cudaGraphLaunch(bt->loop, s));
+    } else {
+        for (int it = 0; it <= max_iter + 1; it += 4) {
+            for (int j = 0; j < 4; ++j) APXB_CK(cudaGraphLaunch(bt->one, s));
+            int ad = 0;
+            APXB_CK(cudaMemcpyAsync(&ad, P.all_done, sizeof(int), cudaMemcpyDeviceToHost, s));
+            APXB_CK(cudaStreamSynchronize(s));
+            if (ad) break;
+        }
+    }
+    double* dX = dev ? X : bt->d_B;
+    launch_finish(bt, P, dX, (flags & APXB_TRUE_RESIDUAL) != 0, s);
+    APXB_CK(cudaEventRecord(e->ev1, s));
+    APXB_CK(cudaGetLastError());
+    if (!dev) APXB_CK(cudaMemcpyAsync(X, bt->d_B, 8 * nk, cudaMemcpyDeviceToHost, s));
+    APXB_CK(cudaMemcpyAsync(bt->h_sd, bt->sd, sizeof(double) * 13 * ns, cudaMemcpyDeviceToHost, s));
+    APXB_CK(cudaMemcpyAsync(bt->h_si, bt->si, sizeof(int) * 6 * ns, cudaMemcpyDeviceToHost, s));
+    const int rc = e->take_error();
+    if (rc) { bt->y_armed = false; cudaMemsetAsync(bt->ctl, 0, 2 * sizeof(apxb::sweep_ctl), s); return rc; }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e->ev0, e->ev1);
+    for (size_t sl = 0; sl < ns; ++sl) {
+        res[sl].iterations = bt->h_si[sl];
+        res[sl].status = bt->h_si[2 * ns + sl];
+        res[sl].residual = bt->h_sd[7 * ns + sl];
+        res[sl].true_residual = (flags & APXB_TRUE_RESIDUAL) ? bt->h_sd[12 * ns + sl] : -1.0;
+        res[sl].seconds = ms * 1e-3;
+    }
+    return APXB_OK;
+}
+
+}  // extern "C"

@@ -352,6 +352,8 @@ std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* r
         const std::string bad = check_plan(m, dir == 0 ? fl : bl, dir == 0 ? out.fwd_plan : out.bck_plan);
         if (!bad.empty()) return "internal sweep plan error: " + bad;
     }
+    out.fwd_level = std::move(fl);
+    out.bck_level = std::move(bl);
 
     // Permutation: must be a bijection of [0, n).
     out.perm.assign(perm, perm + n);

@@ -85,6 +85,7 @@ struct prepared_factor {
     std::vector<uint32_t> fwd_thin_bits, bck_thin_bits;
     int32_t fwd_levels = 0, bck_levels = 0;
     std::vector<uint32_t> perm;  // perm[original] = position
+    std::vector<int32_t> fwd_level, bck_level;   // level of every row per direction
     sweep_plan fwd_plan, bck_plan;
 };
 

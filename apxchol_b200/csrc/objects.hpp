@@ -1,0 +1,186 @@
+// Internal object definitions shared by the C ABI translation units
+// (capi.cu, batch.cu). Not part of the public interface.
+#pragma once
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "apxb200.h"
+#include "host_prep.hpp"
+#include "kernels.cuh"
+
+struct apxb_engine;
+namespace apxb_detail {
+int fail(int code, const std::string& msg);
+int center_k_from_env();
+// A factor, operator or batch on engine e was destroyed.
+void release_child(apxb_engine* e);
+}  // namespace apxb_detail
+using apxb_detail::fail;
+
+#define APXB_CK(call)                                                                            \
+    do {                                                                                         \
+        const cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                                   \
+            return fail(e_ == cudaErrorMemoryAllocation ? APXB_ERR_OOM : APXB_ERR_CUDA,          \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                    \
+    } while (0)
+
+
+struct apxb_engine {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    apxb::dev_error* d_err = nullptr;
+    apxb::dev_error* h_err = nullptr;     // pinned
+    unsigned long long budget_ns = 2000000000ull;
+    uint64_t mem_budget = 0, mem_used = 0;
+    double* d_partials = nullptr;         // [vec_grid * 4]
+    unsigned* d_counters = nullptr;       // [16]
+    double* d_scal = nullptr;             // [8]
+    double* h_scal = nullptr;             // pinned [8]
+    int vec_grid = 592;
+    int center_k = 10;
+    int sweep_grid = 0;                   // 0 = resident grid
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // staging for host-pointer entry points
+    double* d_stage_a = nullptr; double* d_stage_b = nullptr; size_t stage_n = 0;
+    double* h_stage_a = nullptr; double* h_stage_b = nullptr; size_t h_stage_n = 0;
+    // Factors and operators alive on this engine. apxb_engine_destroy with
+    // live children only marks the engine closing; the last child frees it.
+    int children = 0;
+    bool closing = false;
+
+    int alloc(void** p, size_t bytes) {
+        if (mem_budget && mem_used + bytes > mem_budget)
+            return fail(APXB_ERR_BUDGET, "device memory budget exhausted: " + std::to_string(mem_used) + " + " +
+                                             std::to_string(bytes) + " > " + std::to_string(mem_budget));
+        const cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+        if (e != cudaSuccess) {
+            *p = nullptr;
+            cudaGetLastError();
+            return fail(APXB_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        }
+        mem_used += bytes;
+        return APXB_OK;
+    }
+    void release(void* p, size_t bytes) {
+        if (p) {
+            cudaFree(p);
+            mem_used -= bytes;
+        }
+    }
+    // Reads and clears the device error word; returns its code (0 = none).
+    int take_error() {
+        if (cudaMemcpyAsync(h_err, d_err, sizeof(apxb::dev_error), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+            cudaStreamSynchronize(stream) != cudaSuccess)
+            return fail(APXB_ERR_CUDA, std::string("device fault: ") + cudaGetErrorString(cudaGetLastError()));
+        if (h_err->code == 0) return APXB_OK;
+        const int code = h_err->code;
+        const std::string msg = code == APXB_ERR_TIMEOUT
+            ? "a sweep wait exceeded its spin budget (kernel " + std::to_string(h_err->where) + ", row " +
+                  std::to_string(h_err->info) + ")"
+            : "device error " + std::to_string(code);
+        cudaMemsetAsync(d_err, 0, sizeof(apxb::dev_error), stream);
+        cudaStreamSynchronize(stream);
+        return fail(code, msg);
+    }
+    int ensure_stage(size_t n) {
+        if (stage_n < n) {
+            release(d_stage_a, stage_n * 8); release(d_stage_b, stage_n * 8);
+            d_stage_a = d_stage_b = nullptr; stage_n = 0;
+            int rc = alloc(reinterpret_cast<void**>(&d_stage_a), n * 8);
+            if (rc) return rc;
+            rc = alloc(reinterpret_cast<void**>(&d_stage_b), n * 8);
+            if (rc) return rc;
+            stage_n = n;
+        }
+        if (h_stage_n < n) {
+            if (h_stage_a) cudaFreeHost(h_stage_a);
+            if (h_stage_b) cudaFreeHost(h_stage_b);
+            h_stage_a = h_stage_b = nullptr; h_stage_n = 0;
+            APXB_CK(cudaMallocHost(&h_stage_a, n * 8));
+            APXB_CK(cudaMallocHost(&h_stage_b, n * 8));
+            h_stage_n = n;
+        }
+        return APXB_OK;
+    }
+};
+
+struct apxb_factor {
+    apxb_engine* e = nullptr;
+    apxb::prepared_factor h;
+    int precision = APXB_PREC_FP64;
+    uint64_t apply_count = 0;
+    uint64_t dev_bytes = 0;
+    std::vector<std::pair<void*, size_t>> owned;
+    uint32_t* perm = nullptr;
+    double *Y = nullptr, *Z = nullptr, *zp = nullptr;   // fp64 tracked buffers, permuted rhs
+    bool y_armed = false, z_armed = false;
+    apxb::sweep_ctl* ctl = nullptr;                    // [2]
+    int grid64 = 0;
+    // sweep plans (the kernels' layout), per direction
+    uint32_t* info[2] = {nullptr, nullptr};
+    uint32_t* ord[2] = {nullptr, nullptr};
+    uint32_t* ptr[2] = {nullptr, nullptr};
+    uint32_t* idx[2] = {nullptr, nullptr};
+    float* val[2] = {nullptr, nullptr};
+    uint32_t *seg_row[2] = {nullptr, nullptr}, *seg_lvl[2] = {nullptr, nullptr};
+    uint32_t *seg_ptr[2] = {nullptr, nullptr}, *seg_idx[2] = {nullptr, nullptr};
+    float* seg_val[2] = {nullptr, nullptr};
+    // fp32 sweeps, k right-hand sides
+    float *Yf = nullptr, *Zf = nullptr;
+    size_t f32_cap = 0;                                // floats per buffer
+    bool yf_armed = false, zf_armed = false;
+    int f32_k = 0;
+
+    template <class T>
+    int dalloc(T** p, size_t count) {
+        const size_t bytes = count * sizeof(T);
+        const int rc = e->alloc(reinterpret_cast<void**>(p), bytes);
+        if (rc) return rc;
+        owned.emplace_back(*p, bytes);
+        dev_bytes += bytes;
+        return APXB_OK;
+    }
+    ~apxb_factor() {
+        for (auto& [p, b] : owned) e->release(p, b);
+    }
+};
+
+struct apxb_operator {
+    apxb_engine* e = nullptr;
+    uint32_t n = 0;
+    uint64_t nnz = 0;
+    std::vector<std::pair<void*, size_t>> owned;
+    int32_t *ptr = nullptr, *idx = nullptr;
+    double* val = nullptr;
+    uint32_t* perm = nullptr;
+    // PCG workspace (permuted ordering) + original-ordering staging
+    double *x = nullptr, *r = nullptr, *p = nullptr, *Ap = nullptr, *b_orig = nullptr, *x_orig = nullptr;
+    apxb::pcg_state* st = nullptr;
+    apxb::pcg_state* h_st = nullptr;   // pinned
+    // cached loop graph for one factor
+    const apxb_factor* graph_factor = nullptr;
+    cudaGraphExec_t loop = nullptr;
+    bool loop_conditional = false;
+
+    template <class T>
+    int dalloc(T** q, size_t count) {
+        const size_t bytes = count * sizeof(T);
+        const int rc = e->alloc(reinterpret_cast<void**>(q), bytes);
+        if (rc) return rc;
+        owned.emplace_back(*q, bytes);
+        return APXB_OK;
+    }
+    ~apxb_operator() {
+        if (loop) cudaGraphExecDestroy(loop);
+        for (auto& [q, b] : owned) e->release(q, b);
+        if (h_st) cudaFreeHost(h_st);
+    }
+};
+

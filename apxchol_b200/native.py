@@ -16,6 +16,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libapxb200.so")
 HEADER = os.path.join(os.path.dirname(_HERE), "include", "apxb200.h")
 
+TRUE_RESIDUAL = 8
 OK = 0
 ERR_INVALID, ERR_CUDA, ERR_OOM, ERR_TIMEOUT, ERR_BAD_FACTOR, ERR_NONFINITE, ERR_BUDGET, ERR_BUSY = range(-1, -9, -1)
 PREC_FP64, PREC_FP32 = 0, 1
@@ -76,6 +77,10 @@ _SIGS = {
     "apxb_pcg": (ctypes.c_int, [c_p, c_p, c_p, c_p, c_p, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                 ctypes.POINTER(PcgResult)]),
     "apxb_test_stalled_sweep": (ctypes.c_int, [c_p, c_p, ctypes.c_uint64]),
+    "apxb_batch_create": (ctypes.c_int, [c_p, ctypes.c_int, c_p, c_p, ctypes.c_int, ctypes.POINTER(c_p)]),
+    "apxb_batch_destroy": (ctypes.c_int, [c_p]),
+    "apxb_batch_size": (ctypes.c_int, [c_p, c_p, c_p, c_p]),
+    "apxb_batch_solve": (ctypes.c_int, [c_p, c_p, c_p, c_p, ctypes.c_double, ctypes.c_int, ctypes.c_int, c_p]),
 }
 
 
@@ -296,3 +301,66 @@ def prepare_host(fac, drop_rel: float = -1.0):
                                                                 "csc_val", "fwd_thin", "bck_thin")]))
     out["m"], out["nnz"], out["levels"] = M, N, (int(lv[0]), int(lv[1]))
     return out
+
+
+class Batch:
+    """apxb_batch: S instances x k right-hand-side slots solved together
+    (fp32 preconditioner sweeps, fp64 everything else)."""
+
+    def __init__(self, eng: Engine, factors, operators, k: int):
+        self.eng, self.lib = eng, eng.lib
+        self.factors, self.operators = list(factors), list(operators)   # keep alive
+        S = len(self.factors)
+        fa = (c_p * S)(*[f.h for f in self.factors])
+        oa = (c_p * S)(*[o.h for o in self.operators])
+        h = c_p()
+        check(self.lib.apxb_batch_create(eng.h, S, fa, oa, k, ctypes.byref(h)))
+        self.h = h
+        self.S, self.k = S, k
+        self.sizes = [f.n for f in self.factors]
+        self.offsets = np.concatenate([[0], np.cumsum(self.sizes)]).astype(np.int64)
+        self.n_total = int(self.offsets[-1])
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.apxb_batch_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def pack(self, rhs):
+        """rhs[i] = array (n_i,) or (c_i, n_i) -> flat caller layout and nrhs."""
+        B = np.zeros(self.n_total * self.k)
+        nrhs = np.zeros(self.S, np.int32)
+        for i, bi in enumerate(rhs):
+            bi = np.atleast_2d(np.asarray(bi, np.float64))
+            c, ni = bi.shape
+            assert ni == self.sizes[i] and c <= self.k
+            base = self.k * int(self.offsets[i])
+            B[base: base + c * ni] = bi.ravel()
+            nrhs[i] = c
+        return B, nrhs
+
+    def unpack(self, X, nrhs):
+        out = []
+        for i in range(self.S):
+            base, ni = self.k * int(self.offsets[i]), self.sizes[i]
+            out.append(X[base: base + int(nrhs[i]) * ni].reshape(int(nrhs[i]), ni))
+        return out
+
+    def solve(self, rhs, tol=1e-8, max_iter=500, true_residual=True):
+        """rhs: list per instance of (c_i, n_i) arrays. Returns (list of x
+        arrays, list of per-instance result lists)."""
+        B, nrhs = self.pack(rhs)
+        X = np.empty_like(B)
+        res = (PcgResult * (self.S * self.k))()
+        flags = TRUE_RESIDUAL if true_residual else 0
+        check(self.lib.apxb_batch_solve(self.h, ptr(B), ptr(X), ptr(nrhs), tol, max_iter, flags, res))
+        results = [[res[i * self.k + c] for c in range(int(nrhs[i]))] for i in range(self.S)]
+        return self.unpack(X, nrhs), results
+
+    def solve_raw(self, B, X, nrhs, tol=1e-8, max_iter=500, flags=0):
+        """Caller-layout buffers (numpy host or torch device with DEVICE_PTRS)."""
+        res = (PcgResult * (self.S * self.k))()
+        check(self.lib.apxb_batch_solve(self.h, ptr(B), ptr(X), ptr(nrhs), tol, max_iter, flags, res))
+        return res

@@ -49,10 +49,12 @@ extern "C" {
 #define APXB_CENTER_SCHEDULE  0  /* Laplacian centring per the center-k counter (default) */
 #define APXB_CENTER_ALWAYS    2
 #define APXB_CENTER_NEVER     4
+#define APXB_TRUE_RESIDUAL    8  /* batch solve: recompute ||b - A x|| / ||b|| per slot in fp64 */
 
 typedef struct apxb_engine apxb_engine;
 typedef struct apxb_factor apxb_factor;
 typedef struct apxb_operator apxb_operator;
+typedef struct apxb_batch apxb_batch;
 
 typedef struct apxb_factor_info {
     uint32_t n;              /* operator dimension */
@@ -159,6 +161,25 @@ int apxb_operator_matvec(apxb_engine* e, apxb_operator* a, const double* x, doub
  * src/solve.cpp:478-654. want_true_residual: recompute ||b - A x||/||b||. */
 int apxb_pcg(apxb_engine* e, apxb_factor* f, apxb_operator* a, const double* b, double* x,
              double tol, int max_iter, int flags, int want_true_residual, apxb_pcg_result* res);
+
+/* ---- batched solves: mixed precision, many right-hand sides, uneven instances ----
+ * A batch binds S instances (factor + operator pairs of any sizes, solved as
+ * one block-diagonal system in a single set of launches) and k right-hand-side
+ * slots per instance (k = 1, 2, 4, 8 or 16). The preconditioner runs fp32
+ * sweeps with fp32 accumulation; SpMV, residuals, dots and centring are fp64.
+ * Each slot is an independent PCG with the semantics of apxb_pcg. No
+ * counterpart in the reference (its GPU PCG solves one right-hand side). */
+int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, apxb_operator* const* ops, int k,
+                      apxb_batch** out);
+int apxb_batch_destroy(apxb_batch* b);
+int apxb_batch_size(const apxb_batch* b, int* n_inst, int* k, uint32_t* n_total);
+/* B, X: for instance i (row offset off_i, size n_i, original ordering) and
+ * column c, entries at [k * off_i + c * n_i, ... + n_i). nrhs[i] (NULL = all
+ * k) columns of instance i are used; the others return x = 0. res receives
+ * one result per slot (instance-major). flags: APXB_DEVICE_PTRS,
+ * APXB_TRUE_RESIDUAL. */
+int apxb_batch_solve(apxb_batch* b, const double* B, double* X, const int* nrhs, double tol, int max_iter,
+                     int flags, apxb_pcg_result* res);
 
 /* ---- failure detection test hook ----
  * Runs one forward sweep whose first 32 rows are never solved (the work

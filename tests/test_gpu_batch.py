@@ -1,0 +1,77 @@
+"""Batched mixed-precision solves (gpu): many right-hand sides and uneven
+instances in one set of launches. fp32 preconditioner sweeps, fp64 outer
+PCG: every slot must reach the fp64-recomputed tolerance and agree with the
+reference's solution within the PCG tolerance; batched results must equal
+the same systems solved alone."""
+import numpy as np
+import pytest
+
+from apxchol_b200 import gen, native
+from tests.problems import problem
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-8
+TRUE_RES_FACTOR = 10.0
+
+
+@pytest.fixture(scope="module")
+def eng():
+    import torch
+    torch.cuda.init()
+    e = native.Engine(0)
+    yield e
+    e.close()
+
+
+def _objs(eng, name):
+    A, F = problem(name)
+    return A, F, native.DeviceFactor(eng, F, precision=native.PREC_FP32), native.DeviceOperator(eng, A, F.perm)
+
+
+@pytest.mark.parametrize("k", [1, 4, 16])
+def test_single_instance_multi_rhs(eng, k):
+    A, F, D, Op = _objs(eng, "grid3d_24")
+    bt = native.Batch(eng, [D], [Op], k)
+    B = np.stack([gen.rhs(A.n, 100 + c, False) for c in range(k)])
+    xs, res = bt.solve([B], tol=TOL)
+    O = oracle.Oracle(A, F, nt=8)
+    for c in range(k):
+        r = res[0][c]
+        assert r.status == 0 and r.true_residual < TRUE_RES_FACTOR * TOL, (c, r.status, r.true_residual)
+        xo, ito, _ = O.solve(B[c], TOL, 500)
+        assert np.linalg.norm(xs[0][c] - xo) <= 1e-6 * np.linalg.norm(xo)
+        assert abs(r.iterations - ito) <= 5, (r.iterations, ito)
+
+
+def test_uneven_instances_share_one_batch(eng):
+    names = ["grid2d_64", "grid3d_24", "regular_3000", "rmat_12"]
+    objs = [_objs(eng, nm) for nm in names]
+    bt = native.Batch(eng, [o[2] for o in objs], [o[3] for o in objs], 4)
+    rhs = []
+    for i, (A, F, D, Op) in enumerate(objs):
+        c = 1 + i % 4
+        rhs.append(np.stack([gen.rhs(A.n, 10 * i + j, not F.sddm) for j in range(c)]))
+    xs, res = bt.solve(rhs, tol=TOL)
+    for i, (A, F, D, Op) in enumerate(objs):
+        # each instance alone in its own batch gives the same bytes
+        alone = native.Batch(eng, [D], [Op], 4)
+        xa, ra = alone.solve([rhs[i]], tol=TOL)
+        assert np.array_equal(xs[i], xa[0]), names[i]
+        for c in range(rhs[i].shape[0]):
+            r = res[i][c]
+            assert r.status == 0 and r.true_residual < TRUE_RES_FACTOR * TOL, (names[i], c, r.true_residual)
+            assert r.iterations == ra[0][c].iterations
+            if not F.sddm:
+                assert abs(xs[i][c].mean()) < 1e-10 * np.abs(xs[i][c]).max()
+
+
+def test_batch_repeats_bitwise(eng):
+    A, F, D, Op = _objs(eng, "grid2d_256")
+    bt = native.Batch(eng, [D], [Op], 8)
+    B = np.stack([gen.rhs(A.n, 500 + c, True) for c in range(5)])
+    x1, r1 = bt.solve([B], tol=TOL)
+    x2, r2 = bt.solve([B], tol=TOL)
+    assert np.array_equal(x1[0], x2[0])
+    assert [r.iterations for r in r1[0]] == [r.iterations for r in r2[0]]
