@@ -24,7 +24,7 @@
 
 namespace {
 
-constexpr uint32_t kTile = 1024;   // rows per reduction tile
+constexpr uint32_t kTile = 2048;   // rows per reduction tile
 constexpr int kBT = 256;           // threads per block of the vector kernels
 
 enum fin_mode : int { kFinSpmv = 0, kFinXr = 1, kFinZsum = 2, kFinRz = 3, kFinResid = 4 };
@@ -37,7 +37,8 @@ struct bp {
     const unsigned* inst_t0; const unsigned* inst_t1;
     const unsigned* inst_off; const unsigned* inst_n; const int* inst_lap;
     const int32_t* a_ptr; const int32_t* a_idx; const double* a_val;
-    const uint32_t* igperm;    // permuted position -> original (global) index
+    const uint32_t* gperm;     // original (global) index -> permuted position
+    const uint32_t* inst_of;   // original (global) index -> instance
     double *x, *r, *p, *Ap, *b;
     float* rhs32;
     const float* z;
@@ -63,28 +64,75 @@ __device__ __forceinline__ void tile_store(double (&v)[NV], double* dst) {
     __syncthreads();
 }
 
+// Per-column deterministic block reduction of the flat [row][K] kernels: a
+// thread owns the column pair (c0, c0 + 1) (both column 0 when K == 1);
+// lanes with the same columns combine by a fixed butterfly, then thread
+// v * K + c adds the warps in order. dst[v * K + c] = total of value v, column c.
+template <int K, int NV>
+__device__ __forceinline__ void col_store(double (&a)[NV][2], double* dst) {
+    constexpr int H = K >= 2 ? K / 2 : 1;
+    __shared__ double red[kBT / 32][NV][K];
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        if (K == 1) a[v][0] += a[v][1];
+#pragma unroll
+        for (int e = 0; e < (K == 1 ? 1 : 2); ++e)
+#pragma unroll
+            for (int o = H; o < 32; o <<= 1) a[v][e] += __shfl_xor_sync(apxb::kFull, a[v][e], o);
+    }
+    if (lane < static_cast<unsigned>(H)) {
+        const int c0 = K == 1 ? 0 : 2 * static_cast<int>(lane);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            red[warp][v][c0] = a[v][0];
+            if (K > 1) red[warp][v][c0 + 1] = a[v][1];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < static_cast<unsigned>(K * NV)) {
+        const int v = threadIdx.x / K, c = threadIdx.x % K;
+        double s = 0.0;
+        for (int w = 0; w < kBT / 32; ++w) s += red[w][v][c];
+        dst[v * K + c] = s;
+    }
+    __syncthreads();
+}
+
+// Flat walk of a tile's [row][K] block in pairs: element q = 2 * (tid + j * kBT)
+// from the tile base; the thread's column pair is fixed (kBT * 2 % K == 0).
+#define FLAT_PAIRS(t, ...)                                                                    \
+    {                                                                                          \
+        const size_t base_ = static_cast<size_t>(P.tile_lo[t]) * K;                           \
+        const size_t end_ = static_cast<size_t>(P.tile_hi[t]) * K;                            \
+        for (size_t q = base_ + 2 * threadIdx.x; q < end_; q += 2 * kBT) {                   \
+            const bool two = q + 1 < end_;                                                     \
+            __VA_ARGS__                                                                        \
+        }                                                                                      \
+    }
+
 // x = 0, r = b = P B (fresh slots only); B in the caller's layout: instance i,
 // column c, original local index v at B[K * off_i + c * n_i + v]. Columns
-// >= nrhs[i] are zero (their slots finish at once).
+// >= nrhs[i] are zero (their slots finish at once). Walks the original order
+// (coalesced reads of B) and scatters each row's K values.
 template <int K>
 __global__ void __launch_bounds__(kBT) k_b_admit(bp P, const double* B, const int* nrhs) {
-    for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
-        const unsigned i = P.tile_inst[t], off = P.inst_off[i], ni = P.inst_n[i];
-        for (unsigned pos = P.tile_lo[t] + threadIdx.x; pos < P.tile_hi[t]; pos += blockDim.x) {
-            const unsigned v = P.igperm[pos] - off;
+    for (unsigned g = blockIdx.x * blockDim.x + threadIdx.x; g < P.n_tot; g += gridDim.x * blockDim.x) {
+        const unsigned i = P.inst_of[g], off = P.inst_off[i], ni = P.inst_n[i];
+        const unsigned v = g - off;
+        const size_t row = static_cast<size_t>(P.gperm[g]) * K;
 #pragma unroll
-            for (int c = 0; c < K; ++c) {
-                const unsigned sl = i * K + c;
-                if (!P.fresh[sl]) continue;
-                const double bv = c < nrhs[i] ? B[static_cast<size_t>(K) * off + static_cast<size_t>(c) * ni + v] : 0.0;
-                const size_t q = static_cast<size_t>(pos) * K + c;
-                P.b[q] = bv; P.r[q] = bv; P.x[q] = 0.0; P.p[q] = 0.0;
-            }
+        for (int c = 0; c < K; ++c) {
+            const unsigned sl = i * K + c;
+            if (!P.fresh[sl]) continue;
+            const double bv = c < nrhs[i] ? B[static_cast<size_t>(K) * off + static_cast<size_t>(c) * ni + v] : 0.0;
+            P.b[row + c] = bv; P.r[row + c] = bv; P.x[row + c] = 0.0; P.p[row + c] = 0.0;
         }
     }
 }
 
-// Ap = A p with per-slot p.Ap partials (mode 0), or Y = A X (mode 1).
+// Ap = A p with per-slot p.Ap partials (mode 0), or Y = A X (mode 1). One
+// thread per row, the K columns of every operand row read as 16-byte pairs.
 template <int K>
 __global__ void __launch_bounds__(kBT) k_b_spmv(bp P, const double* X, double* Y, int mode) {
     if (*P.all_done && mode == 0) return;
@@ -97,17 +145,36 @@ __global__ void __launch_bounds__(kBT) k_b_spmv(bp P, const double* X, double* Y
 #pragma unroll
             for (int c = 0; c < K; ++c) acc[c] = 0.0;
             const int e = __ldg(P.a_ptr + row + 1);
+#pragma unroll 2
             for (int k = __ldg(P.a_ptr + row); k < e; ++k) {
                 const double w = __ldg(P.a_val + k);
                 const double* src = X + static_cast<size_t>(__ldg(P.a_idx + k)) * K;
+                if constexpr (K == 1) {
+                    acc[0] = fma(w, src[0], acc[0]);
+                } else {
 #pragma unroll
-                for (int c = 0; c < K; ++c) acc[c] = fma(w, src[c], acc[c]);
+                    for (int c = 0; c < K; c += 2) {
+                        const double2 v = *reinterpret_cast<const double2*>(src + c);
+                        acc[c] = fma(w, v.x, acc[c]);
+                        acc[c + 1] = fma(w, v.y, acc[c + 1]);
+                    }
+                }
             }
             double* dst = Y + static_cast<size_t>(row) * K;
+            const double* xr = X + static_cast<size_t>(row) * K;
+            if constexpr (K == 1) {
+                dst[0] = acc[0];
+                if (mode == 0) part[0] = fma(xr[0], acc[0], part[0]);
+            } else {
 #pragma unroll
-            for (int c = 0; c < K; ++c) {
-                dst[c] = acc[c];
-                if (mode == 0) part[c] = fma(X[static_cast<size_t>(row) * K + c], acc[c], part[c]);
+                for (int c = 0; c < K; c += 2) {
+                    *reinterpret_cast<double2*>(dst + c) = make_double2(acc[c], acc[c + 1]);
+                    if (mode == 0) {
+                        const double2 xv = *reinterpret_cast<const double2*>(xr + c);
+                        part[c] = fma(xv.x, acc[c], part[c]);
+                        part[c + 1] = fma(xv.y, acc[c + 1], part[c + 1]);
+                    }
+                }
             }
         }
         if (mode == 0) tile_store<K>(part, P.partials + static_cast<size_t>(t) * K * 2);
@@ -118,30 +185,34 @@ __global__ void __launch_bounds__(kBT) k_b_spmv(bp P, const double* X, double* Y
 template <int K>
 __global__ void __launch_bounds__(kBT) k_b_xr(bp P) {
     if (*P.all_done) return;
+    const int c0 = K == 1 ? 0 : static_cast<int>((2 * threadIdx.x) % K), c1 = K == 1 ? 0 : c0 + 1;
     for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
         const unsigned i = P.tile_inst[t];
-        double a[K], v[2 * K];
-#pragma unroll
-        for (int c = 0; c < K; ++c) {
-            const unsigned sl = i * K + c;
-            a[c] = (P.fresh[sl] || P.done[sl]) ? 0.0 : P.alpha[sl];
-            v[c] = 0.0; v[K + c] = 0.0;
-        }
-        for (unsigned row = P.tile_lo[t] + threadIdx.x; row < P.tile_hi[t]; row += blockDim.x) {
-#pragma unroll
-            for (int c = 0; c < K; ++c) {
-                const size_t q = static_cast<size_t>(row) * K + c;
-                P.x[q] = fma(a[c], P.p[q], P.x[q]);
-                const double ri = fma(-a[c], P.Ap[q], P.r[q]);
-                P.r[q] = ri;
-                v[c] = fma(ri, ri, v[c]);
-                v[K + c] += ri;
+        const unsigned s0 = i * K + c0, s1 = i * K + c1;
+        const double a0 = (P.fresh[s0] || P.done[s0]) ? 0.0 : P.alpha[s0];
+        const double a1 = (P.fresh[s1] || P.done[s1]) ? 0.0 : P.alpha[s1];
+        double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+        FLAT_PAIRS(t, {
+            if (two) {
+                double2 x = *reinterpret_cast<const double2*>(P.x + q);
+                const double2 p = *reinterpret_cast<const double2*>(P.p + q);
+                double2 r = *reinterpret_cast<const double2*>(P.r + q);
+                const double2 ap = *reinterpret_cast<const double2*>(P.Ap + q);
+                x.x = fma(a0, p.x, x.x); x.y = fma(a1, p.y, x.y);
+                r.x = fma(-a0, ap.x, r.x); r.y = fma(-a1, ap.y, r.y);
+                *reinterpret_cast<double2*>(P.x + q) = x;
+                *reinterpret_cast<double2*>(P.r + q) = r;
+                acc[0][0] = fma(r.x, r.x, acc[0][0]); acc[0][1] = fma(r.y, r.y, acc[0][1]);
+                acc[1][0] += r.x; acc[1][1] += r.y;
+            } else {
+                P.x[q] = fma(a0, P.p[q], P.x[q]);
+                const double r = fma(-a0, P.Ap[q], P.r[q]);
+                P.r[q] = r;
+                acc[0][0] = fma(r, r, acc[0][0]);
+                acc[1][0] += r;
             }
-        }
-        double w[2 * K];
-#pragma unroll
-        for (int c = 0; c < 2 * K; ++c) w[c] = v[c];
-        tile_store<2 * K>(w, P.partials + static_cast<size_t>(t) * K * 2);
+        })
+        col_store<K, 2>(acc, P.partials + static_cast<size_t>(t) * K * 2);
     }
 }
 
@@ -149,17 +220,19 @@ __global__ void __launch_bounds__(kBT) k_b_xr(bp P) {
 template <int K>
 __global__ void __launch_bounds__(kBT) k_b_prep(bp P) {
     if (*P.all_done) return;
+    const int c0 = K == 1 ? 0 : static_cast<int>((2 * threadIdx.x) % K), c1 = K == 1 ? 0 : c0 + 1;
     for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
         const unsigned i = P.tile_inst[t];
-        double mu[K];
-#pragma unroll
-        for (int c = 0; c < K; ++c) mu[c] = P.mean[i * K + c];
-        for (unsigned row = P.tile_lo[t] + threadIdx.x; row < P.tile_hi[t]; row += blockDim.x)
-#pragma unroll
-            for (int c = 0; c < K; ++c) {
-                const size_t q = static_cast<size_t>(row) * K + c;
-                P.rhs32[q] = static_cast<float>(P.r[q] - mu[c]);
+        const double m0 = P.mean[i * K + c0], m1 = P.mean[i * K + c1];
+        FLAT_PAIRS(t, {
+            if (two) {
+                const double2 r = *reinterpret_cast<const double2*>(P.r + q);
+                *reinterpret_cast<float2*>(P.rhs32 + q) = make_float2(static_cast<float>(r.x - m0),
+                                                                       static_cast<float>(r.y - m1));
+            } else {
+                P.rhs32[q] = static_cast<float>(P.r[q] - m0);
             }
+        })
     }
 }
 
@@ -168,15 +241,18 @@ template <int K>
 __global__ void __launch_bounds__(kBT) k_b_zsum(bp P) {
     if (*P.all_done) return;
     for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
-        const unsigned i = P.tile_inst[t];
-        double v[K];
-#pragma unroll
-        for (int c = 0; c < K; ++c) v[c] = 0.0;
-        if (P.inst_lap[i])
-            for (unsigned row = P.tile_lo[t] + threadIdx.x; row < P.tile_hi[t]; row += blockDim.x)
-#pragma unroll
-                for (int c = 0; c < K; ++c) v[c] += static_cast<double>(P.z[static_cast<size_t>(row) * K + c]);
-        tile_store<K>(v, P.partials + static_cast<size_t>(t) * K * 2);
+        double acc[1][2] = {{0.0, 0.0}};
+        if (P.inst_lap[P.tile_inst[t]]) {
+            FLAT_PAIRS(t, {
+                if (two) {
+                    const float2 z = *reinterpret_cast<const float2*>(P.z + q);
+                    acc[0][0] += static_cast<double>(z.x); acc[0][1] += static_cast<double>(z.y);
+                } else {
+                    acc[0][0] += static_cast<double>(P.z[q]);
+                }
+            })
+        }
+        col_store<K, 1>(acc, P.partials + static_cast<size_t>(t) * K * 2);
     }
 }
 
@@ -184,67 +260,87 @@ __global__ void __launch_bounds__(kBT) k_b_zsum(bp P) {
 template <int K>
 __global__ void __launch_bounds__(kBT) k_b_rz(bp P) {
     if (*P.all_done) return;
+    const int c0 = K == 1 ? 0 : static_cast<int>((2 * threadIdx.x) % K), c1 = K == 1 ? 0 : c0 + 1;
     for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
         const unsigned i = P.tile_inst[t];
-        double sh[K], v[K];
-#pragma unroll
-        for (int c = 0; c < K; ++c) { sh[c] = P.shift[i * K + c]; v[c] = 0.0; }
-        for (unsigned row = P.tile_lo[t] + threadIdx.x; row < P.tile_hi[t]; row += blockDim.x)
-#pragma unroll
-            for (int c = 0; c < K; ++c) {
-                const size_t q = static_cast<size_t>(row) * K + c;
-                v[c] = fma(P.r[q], static_cast<double>(P.z[q]) - sh[c], v[c]);
+        const double h0 = P.shift[i * K + c0], h1 = P.shift[i * K + c1];
+        double acc[1][2] = {{0.0, 0.0}};
+        FLAT_PAIRS(t, {
+            if (two) {
+                const double2 r = *reinterpret_cast<const double2*>(P.r + q);
+                const float2 z = *reinterpret_cast<const float2*>(P.z + q);
+                acc[0][0] = fma(r.x, static_cast<double>(z.x) - h0, acc[0][0]);
+                acc[0][1] = fma(r.y, static_cast<double>(z.y) - h1, acc[0][1]);
+            } else {
+                acc[0][0] = fma(P.r[q], static_cast<double>(P.z[q]) - h0, acc[0][0]);
             }
-        tile_store<K>(v, P.partials + static_cast<size_t>(t) * K * 2);
+        })
+        col_store<K, 1>(acc, P.partials + static_cast<size_t>(t) * K * 2);
     }
 }
 
-// p = (z - shift) + beta p; first application of a slot: p = z - shift.
-// Clears `fresh` (every slot has now been through one full iteration) and
-// sets the graph's WHILE condition.
+// p = (z - shift) + beta p; first application of a slot: p = z - shift. Sets
+// the graph's WHILE condition.
 template <int K>
 __global__ void __launch_bounds__(kBT) k_b_up(bp P, unsigned long long handle, int use_cond) {
     const bool stop = *P.all_done != 0 || P.err->code != 0;
     if (use_cond && blockIdx.x == 0 && threadIdx.x == 0)
         cudaGraphSetConditional(static_cast<cudaGraphConditionalHandle>(handle), stop ? 0u : 1u);
     if (stop) return;
+    const int c0 = K == 1 ? 0 : static_cast<int>((2 * threadIdx.x) % K), c1 = K == 1 ? 0 : c0 + 1;
     for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
         const unsigned i = P.tile_inst[t];
-        double sh[K], be[K];
-        bool cp[K], live[K];
-#pragma unroll
-        for (int c = 0; c < K; ++c) {
-            const unsigned sl = i * K + c;
-            sh[c] = P.shift[sl]; be[c] = P.beta[sl]; cp[c] = P.pmode[sl] == 1; live[c] = !P.done[sl];
-        }
-        for (unsigned row = P.tile_lo[t] + threadIdx.x; row < P.tile_hi[t]; row += blockDim.x)
-#pragma unroll
-            for (int c = 0; c < K; ++c) {
-                if (!live[c]) continue;
-                const size_t q = static_cast<size_t>(row) * K + c;
-                const double zi = static_cast<double>(P.z[q]) - sh[c];
-                P.p[q] = cp[c] ? zi : fma(be[c], P.p[q], zi);
+        const unsigned s0 = i * K + c0, s1 = i * K + c1;
+        const double h0 = P.shift[s0], h1 = P.shift[s1], b0 = P.beta[s0], b1 = P.beta[s1];
+        const bool cp0 = P.pmode[s0] == 1, cp1 = P.pmode[s1] == 1, l0 = !P.done[s0], l1 = !P.done[s1];
+        FLAT_PAIRS(t, {
+            if (two) {
+                const float2 z = *reinterpret_cast<const float2*>(P.z + q);
+                double2 p = *reinterpret_cast<const double2*>(P.p + q);
+                const double z0 = static_cast<double>(z.x) - h0, z1 = static_cast<double>(z.y) - h1;
+                if (l0) p.x = cp0 ? z0 : fma(b0, p.x, z0);
+                if (l1) p.y = cp1 ? z1 : fma(b1, p.y, z1);
+                *reinterpret_cast<double2*>(P.p + q) = p;
+            } else if (l0) {
+                const double z0 = static_cast<double>(P.z[q]) - h0;
+                P.p[q] = cp0 ? z0 : fma(b0, P.p[q], z0);
             }
+        })
     }
 }
 
-// Per-slot scalars from the tile partials (summed in tile order), then the
-// PCG state machine of the reduction that produced them.
+// Per-slot scalars from the tile partials, then the PCG state machine of the
+// reduction that produced them. One warp per slot: lanes stride the
+// instance's tiles in order, then a fixed butterfly (deterministic).
+__device__ __forceinline__ void slot_sums(const bp& P, unsigned sl, int nv, double& s0, double& s1) {
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned i = sl / P.K, c = sl % P.K;
+    s0 = 0.0; s1 = 0.0;
+    for (unsigned t = P.inst_t0[i] + lane; t < P.inst_t1[i]; t += 32) {
+        const double* src = P.partials + static_cast<size_t>(t) * P.K * 2;
+        s0 += src[c];
+        if (nv == 2) s1 += src[P.K + c];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_xor_sync(apxb::kFull, s0, o);
+        s1 += __shfl_xor_sync(apxb::kFull, s1, o);
+    }
+}
+
 __global__ void __launch_bounds__(kBT) k_b_fin(bp P, int mode) {
     __shared__ int any_live;
     if (threadIdx.x == 0) any_live = 0;
     __syncthreads();
     const unsigned nslots = P.S * P.K;
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     if (!(*P.all_done) || mode == kFinResid) {
-        for (unsigned sl = threadIdx.x; sl < nslots; sl += blockDim.x) {
-            const unsigned i = sl / P.K, c = sl % P.K;
-            double s0 = 0.0, s1 = 0.0;
+        for (unsigned sl = warp; sl < nslots; sl += nw) {
             const int nv = (mode == kFinXr || mode == kFinResid) ? 2 : 1;
-            for (unsigned t = P.inst_t0[i]; t < P.inst_t1[i]; ++t) {
-                const double* src = P.partials + static_cast<size_t>(t) * P.K * 2;
-                if (nv == 2) { s0 += src[c]; s1 += src[P.K + c]; }
-                else s0 += src[c];
-            }
+            double s0, s1;
+            slot_sums(P, sl, nv, s0, s1);
+            if (lane != 0) continue;
+            const unsigned i = sl / P.K;
             const double ni = static_cast<double>(P.inst_n[i]);
             if (mode == kFinResid) {
                 P.tres[sl] = s1 > 0.0 ? sqrt(s0) / sqrt(s1) : 0.0;
@@ -338,25 +434,24 @@ __global__ void __launch_bounds__(kBT) k_b_xsum(bp P) {
 
 __global__ void __launch_bounds__(kBT) k_b_xmean(bp P) {
     const unsigned nslots = P.S * P.K;
-    for (unsigned sl = threadIdx.x; sl < nslots; sl += blockDim.x) {
-        const unsigned i = sl / P.K, c = sl % P.K;
-        double s = 0.0;
-        for (unsigned t = P.inst_t0[i]; t < P.inst_t1[i]; ++t) s += P.partials[static_cast<size_t>(t) * P.K * 2 + c];
-        P.xmean[sl] = (P.inst_lap[i] && P.bnorm[sl] > 0.0) ? s / static_cast<double>(P.inst_n[i]) : 0.0;
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (unsigned sl = warp; sl < nslots; sl += nw) {
+        double s, dummy;
+        slot_sums(P, sl, 1, s, dummy);
+        const unsigned i = sl / P.K;
+        if (lane == 0)
+            P.xmean[sl] = (P.inst_lap[i] && P.bnorm[sl] > 0.0) ? s / static_cast<double>(P.inst_n[i]) : 0.0;
     }
 }
 
 template <int K>
 __global__ void __launch_bounds__(kBT) k_b_out(bp P, double* X) {
-    for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
-        const unsigned i = P.tile_inst[t], off = P.inst_off[i], ni = P.inst_n[i];
-        for (unsigned pos = P.tile_lo[t] + threadIdx.x; pos < P.tile_hi[t]; pos += blockDim.x) {
-            const unsigned v = P.igperm[pos] - off;
+    for (unsigned g = blockIdx.x * blockDim.x + threadIdx.x; g < P.n_tot; g += gridDim.x * blockDim.x) {
+        const unsigned i = P.inst_of[g], off = P.inst_off[i], ni = P.inst_n[i];
+        const size_t row = static_cast<size_t>(P.gperm[g]) * K;
 #pragma unroll
-            for (int c = 0; c < K; ++c)
-                X[static_cast<size_t>(K) * off + static_cast<size_t>(c) * ni + v] =
-                    P.x[static_cast<size_t>(pos) * K + c] - P.xmean[i * K + c];
-        }
+        for (int c = 0; c < K; ++c)
+            X[static_cast<size_t>(K) * off + static_cast<size_t>(c) * ni + (g - off)] = P.x[row + c] - P.xmean[i * K + c];
     }
 }
 
@@ -406,7 +501,8 @@ struct apxb_batch {
     // operator (combined, permuted) and permutation
     const int32_t *a_ptr = nullptr, *a_idx = nullptr;
     const double* a_val = nullptr;
-    uint32_t* igperm = nullptr;
+    uint32_t* gperm = nullptr;
+    uint32_t* inst_of = nullptr;
     // tiles
     uint32_t n_tiles = 0;
     uint32_t *tile_inst = nullptr, *tile_lo = nullptr, *tile_hi = nullptr, *inst_t0 = nullptr, *inst_t1 = nullptr;
@@ -453,7 +549,7 @@ struct apxb_batch {
         P.K = K; P.S = S; P.n_tot = n_tot; P.n_tiles = n_tiles;
         P.tile_inst = tile_inst; P.tile_lo = tile_lo; P.tile_hi = tile_hi; P.inst_t0 = inst_t0; P.inst_t1 = inst_t1;
         P.inst_off = inst_off; P.inst_n = inst_n; P.inst_lap = inst_lap;
-        P.a_ptr = a_ptr; P.a_idx = a_idx; P.a_val = a_val; P.igperm = igperm;
+        P.a_ptr = a_ptr; P.a_idx = a_idx; P.a_val = a_val; P.gperm = gperm; P.inst_of = inst_of;
         P.x = x; P.r = r; P.p = p; P.Ap = Ap; P.b = b; P.rhs32 = rhs32; P.z = Zf;
         const size_t ns = slots();
         double* d = sd;
@@ -632,6 +728,12 @@ int build_graphs(apxb_batch* bt, double tol, int max_iter) {
     return APXB_OK;
 }
 
+// APXB_NO_GRAPH=1: launch every kernel directly (for per-kernel profiling).
+bool no_graph() {
+    const char* e = std::getenv("APXB_NO_GRAPH");
+    return e && *e && *e != '0';
+}
+
 }  // namespace
 
 extern "C" {
@@ -725,11 +827,11 @@ int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, a
     }
     // ---- permutation (permuted position -> original global index), tiles ----
     {
-        std::vector<uint32_t> ig(bt->n_tot);
+        std::vector<uint32_t> gp(bt->n_tot), io(bt->n_tot);
         std::vector<uint32_t> ti, tl, th, t0(n_inst), t1(n_inst);
         for (int i = 0; i < n_inst; ++i) {
             const auto& perm = fs[i]->h.perm;
-            for (uint32_t v = 0; v < bt->n[i]; ++v) ig[bt->off[i] + perm[v]] = bt->off[i] + v;
+            for (uint32_t v = 0; v < bt->n[i]; ++v) { gp[bt->off[i] + v] = bt->off[i] + perm[v]; io[bt->off[i] + v] = i; }
             t0[i] = static_cast<uint32_t>(ti.size());
             for (uint32_t lo = 0; lo < bt->n[i]; lo += kTile) {
                 ti.push_back(static_cast<uint32_t>(i));
@@ -739,13 +841,15 @@ int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, a
             t1[i] = static_cast<uint32_t>(ti.size());
         }
         bt->n_tiles = static_cast<uint32_t>(ti.size());
-        if ((rc = bt->dalloc(&bt->igperm, bt->n_tot)) || (rc = bt->dalloc(&bt->tile_inst, ti.size())) ||
+        if ((rc = bt->dalloc(&bt->gperm, bt->n_tot)) || (rc = bt->dalloc(&bt->inst_of, bt->n_tot)) ||
+            (rc = bt->dalloc(&bt->tile_inst, ti.size())) ||
             (rc = bt->dalloc(&bt->tile_lo, ti.size())) || (rc = bt->dalloc(&bt->tile_hi, ti.size())) ||
             (rc = bt->dalloc(&bt->inst_t0, n_inst)) || (rc = bt->dalloc(&bt->inst_t1, n_inst)) ||
             (rc = bt->dalloc(&bt->inst_off, n_inst)) || (rc = bt->dalloc(&bt->inst_n, n_inst)) ||
             (rc = bt->dalloc(&bt->inst_lap, n_inst)) || (rc = bt->dalloc(&bt->nrhs, n_inst)))
             return rc;
-        APXB_CK(cudaMemcpy(bt->igperm, ig.data(), 4 * ig.size(), cudaMemcpyHostToDevice));
+        APXB_CK(cudaMemcpy(bt->gperm, gp.data(), 4 * gp.size(), cudaMemcpyHostToDevice));
+        APXB_CK(cudaMemcpy(bt->inst_of, io.data(), 4 * io.size(), cudaMemcpyHostToDevice));
         APXB_CK(cudaMemcpy(bt->tile_inst, ti.data(), 4 * ti.size(), cudaMemcpyHostToDevice));
         APXB_CK(cudaMemcpy(bt->tile_lo, tl.data(), 4 * tl.size(), cudaMemcpyHostToDevice));
         APXB_CK(cudaMemcpy(bt->tile_hi, th.data(), 4 * th.size(), cudaMemcpyHostToDevice));
@@ -847,7 +951,18 @@ int apxb_batch_solve(apxb_batch* bt, const double* B, double* X, const int* nrhs
     bt->y_armed = true;
     APXB_CK(cudaEventRecord(e->ev0, s));
     launch_admit(bt, P, dB, s);
-    if (bt->loop_cond) {
+    if (no_graph()) {
+        for (int it = 0; it <= max_iter + 1; it += 4) {
+            for (int j = 0; j < 4; ++j) {
+                const int rc = launch_iteration(bt, P, s, 0, 0);
+                if (rc) return rc;
+            }
+            int ad = 0;
+            APXB_CK(cudaMemcpyAsync(&ad, P.all_done, sizeof(int), cudaMemcpyDeviceToHost, s));
+            APXB_CK(cudaStreamSynchronize(s));
+            if (ad) break;
+        }
+    } else if (bt->loop_cond) {
         APXB_CK(cudaGraphLaunch(bt->loop, s));
     } else {
         for (int it = 0; it <= max_iter + 1; it += 4) {
