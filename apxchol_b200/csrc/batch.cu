@@ -26,6 +26,7 @@ namespace {
 
 constexpr uint32_t kTile = 2048;   // rows per reduction tile
 constexpr int kBT = 256;           // threads per block of the vector kernels
+constexpr int kSd = 14;            // per-slot double arrays (bp::rz .. bp::tol)
 
 enum fin_mode : int { kFinSpmv = 0, kFinXr = 1, kFinZsum = 2, kFinRz = 3, kFinResid = 4 };
 
@@ -43,11 +44,10 @@ struct bp {
     float* rhs32;
     const float* z;
     // per slot [S*K]
-    double *rz, *pAp, *alpha, *beta, *rr, *rs, *bnorm, *rnorm, *prev, *mean, *shift, *xmean, *tres;
+    double *rz, *pAp, *alpha, *beta, *rr, *rs, *bnorm, *rnorm, *prev, *mean, *shift, *xmean, *tres, *tol;
     int *iters, *done, *status, *pmode, *center, *fresh;
     unsigned long long* applies;
     int* all_done;
-    double tol;
     int max_iter, stag, center_k;
     double* partials;          // [n_tiles][K][2]
     apxb::dev_error* err;
@@ -374,7 +374,7 @@ __global__ void __launch_bounds__(kBT) k_b_fin(bp P, int mode) {
                         P.rnorm[sl] = rn;
                         const int it = ++P.iters[sl];
                         int status = 1;
-                        if (rn < P.tol) { fin = true; status = 0; }
+                        if (rn < P.tol[sl]) { fin = true; status = 0; }
                         else if (!isfinite(rn)) { fin = true; status = 4; }
                         else if (P.stag > 0 && it % P.stag == 0) {
                             if (rn > P.prev[sl] * 0.5) { fin = true; status = 2; }
@@ -479,6 +479,28 @@ __global__ void k_b_zero_rows(float* z, const uint32_t* rows, unsigned n, int K)
         z[static_cast<size_t>(rows[i / K]) * K + (i % K)] = 0.0f;
 }
 
+// Continuous batching: x = 0, r = b = P b for one slot (b in original order).
+template <int K>
+__global__ void __launch_bounds__(kBT) k_b_admit_one(bp P, unsigned sl, const double* b) {
+    const unsigned i = sl / K, c = sl % K, off = P.inst_off[i], ni = P.inst_n[i];
+    for (unsigned v = blockIdx.x * blockDim.x + threadIdx.x; v < ni; v += gridDim.x * blockDim.x) {
+        const size_t q = static_cast<size_t>(P.gperm[off + v]) * K + c;
+        const double bv = b[v];
+        P.b[q] = bv; P.r[q] = bv; P.x[q] = 0.0; P.p[q] = 0.0;
+    }
+}
+
+// x of one slot in the original order minus the slot's mean (k_b_xsum +
+// k_b_xmean: the same sums a whole-batch solve takes, so a request's result
+// does not depend on the batch it ran in).
+template <int K>
+__global__ void __launch_bounds__(kBT) k_b_slot_out(bp P, unsigned sl, double* out) {
+    const unsigned i = sl / K, c = sl % K, off = P.inst_off[i], ni = P.inst_n[i];
+    const double mean = P.xmean[sl];
+    for (unsigned v = blockIdx.x * blockDim.x + threadIdx.x; v < ni; v += gridDim.x * blockDim.x)
+        out[v] = P.x[static_cast<size_t>(P.gperm[off + v]) * K + c] - mean;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -513,17 +535,17 @@ struct apxb_batch {
     double *x = nullptr, *r = nullptr, *p = nullptr, *Ap = nullptr, *b = nullptr;
     float *rhs32 = nullptr, *Yf = nullptr, *Zf = nullptr;
     bool y_armed = false;
-    double* sd = nullptr;   // 13 double arrays of S*K
+    double* sd = nullptr;   // kSd double arrays of S*K
     int* si = nullptr;      // 6 int arrays of S*K + all_done
     unsigned long long* applies = nullptr;
     double* partials = nullptr;
     double* d_B = nullptr;  // staging of right-hand sides / solutions in the caller layout
-    // graphs (tol / max_iter are baked into them)
+    // graphs (max_iter is baked into them; tolerances are per slot on the device)
     cudaGraphExec_t loop = nullptr;
     cudaGraphExec_t one = nullptr;
     bool loop_cond = false;
-    double graph_tol = -1.0;
     int graph_max = -1;
+    cudaEvent_t step_ev = nullptr;   // recorded after each apxb_batch_step
     // pinned host mirrors
     double* h_sd = nullptr;
     int* h_si = nullptr;
@@ -537,6 +559,7 @@ struct apxb_batch {
         return APXB_OK;
     }
     ~apxb_batch() {
+        if (step_ev) cudaEventDestroy(step_ev);
         if (loop) cudaGraphExecDestroy(loop);
         if (one) cudaGraphExecDestroy(one);
         for (auto& [q, bytes] : owned) e->release(q, bytes);
@@ -544,7 +567,7 @@ struct apxb_batch {
         if (h_si) cudaFreeHost(h_si);
     }
     size_t slots() const { return static_cast<size_t>(S) * K; }
-    bp params(double tol, int max_iter) const {
+    bp params(int max_iter) const {
         bp P{};
         P.K = K; P.S = S; P.n_tot = n_tot; P.n_tiles = n_tiles;
         P.tile_inst = tile_inst; P.tile_lo = tile_lo; P.tile_hi = tile_hi; P.inst_t0 = inst_t0; P.inst_t1 = inst_t1;
@@ -555,12 +578,12 @@ struct apxb_batch {
         double* d = sd;
         P.rz = d; P.pAp = d + ns; P.alpha = d + 2 * ns; P.beta = d + 3 * ns; P.rr = d + 4 * ns; P.rs = d + 5 * ns;
         P.bnorm = d + 6 * ns; P.rnorm = d + 7 * ns; P.prev = d + 8 * ns; P.mean = d + 9 * ns; P.shift = d + 10 * ns;
-        P.xmean = d + 11 * ns; P.tres = d + 12 * ns;
+        P.xmean = d + 11 * ns; P.tres = d + 12 * ns; P.tol = d + 13 * ns;
         int* s = si;
         P.iters = s; P.done = s + ns; P.status = s + 2 * ns; P.pmode = s + 3 * ns; P.center = s + 4 * ns;
         P.fresh = s + 5 * ns; P.all_done = s + 6 * ns;
         P.applies = applies;
-        P.tol = tol; P.max_iter = max_iter; P.stag = 50; P.center_k = e->center_k;
+        P.max_iter = max_iter; P.stag = 50; P.center_k = e->center_k;
         P.partials = partials; P.err = e->d_err;
         return P;
     }
@@ -684,11 +707,11 @@ void launch_admit(apxb_batch* bt, const bp& P, const double* B, cudaStream_t s) 
     }
 }
 
-int build_graphs(apxb_batch* bt, double tol, int max_iter) {
+int build_graphs(apxb_batch* bt, int max_iter) {
     if (bt->loop) { cudaGraphExecDestroy(bt->loop); bt->loop = nullptr; }
     if (bt->one) { cudaGraphExecDestroy(bt->one); bt->one = nullptr; }
     cudaStream_t s = bt->e->stream;
-    const bp P = bt->params(tol, max_iter);
+    const bp P = bt->params(max_iter);
     // one iteration (host-driven serving loop)
     APXB_CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     int rc = launch_iteration(bt, P, s, 0, 0);
@@ -732,6 +755,37 @@ int build_graphs(apxb_batch* bt, double tol, int max_iter) {
 bool no_graph() {
     const char* e = std::getenv("APXB_NO_GRAPH");
     return e && *e && *e != '0';
+}
+
+template <int K>
+void slot_io_k(apxb_batch* bt, const bp& P, unsigned sl, const double* in, double* out, cudaStream_t s) {
+    const int g = bt->e->vec_grid;
+    if (in) {
+        k_b_admit_one<K><<<g, kBT, 0, s>>>(P, sl, in);
+    } else {
+        k_b_xsum<K><<<g, kBT, 0, s>>>(P);
+        k_b_xmean<<<1, kBT, 0, s>>>(P);
+        k_b_slot_out<K><<<g, kBT, 0, s>>>(P, sl, out);
+    }
+}
+
+// in != NULL: load slot sl's right-hand side; else write its solution to out.
+void slot_io(apxb_batch* bt, const bp& P, unsigned sl, const double* in, double* out, cudaStream_t s) {
+    switch (bt->K) {
+        case 1: slot_io_k<1>(bt, P, sl, in, out, s); break;
+        case 2: slot_io_k<2>(bt, P, sl, in, out, s); break;
+        case 4: slot_io_k<4>(bt, P, sl, in, out, s); break;
+        case 8: slot_io_k<8>(bt, P, sl, in, out, s); break;
+        default: slot_io_k<16>(bt, P, sl, in, out, s); break;
+    }
+}
+
+int ensure_graphs(apxb_batch* bt, int max_iter) {
+    if (bt->one && bt->graph_max == max_iter) return APXB_OK;
+    const int rc = build_graphs(bt, max_iter);
+    if (rc) return rc;
+    bt->graph_max = max_iter;
+    return APXB_OK;
 }
 
 }  // namespace
@@ -862,14 +916,22 @@ int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, a
     // ---- vectors, state ----
     if ((rc = bt->dalloc(&bt->x, nk)) || (rc = bt->dalloc(&bt->r, nk)) || (rc = bt->dalloc(&bt->p, nk)) ||
         (rc = bt->dalloc(&bt->Ap, nk)) || (rc = bt->dalloc(&bt->b, nk)) || (rc = bt->dalloc(&bt->rhs32, nk)) ||
-        (rc = bt->dalloc(&bt->Yf, nk)) || (rc = bt->dalloc(&bt->Zf, nk)) || (rc = bt->dalloc(&bt->sd, 13 * ns)) ||
+        (rc = bt->dalloc(&bt->Yf, nk)) || (rc = bt->dalloc(&bt->Zf, nk)) || (rc = bt->dalloc(&bt->sd, kSd * ns)) ||
         (rc = bt->dalloc(&bt->si, 6 * ns + 1)) || (rc = bt->dalloc(&bt->applies, ns)) ||
         (rc = bt->dalloc(&bt->partials, static_cast<size_t>(bt->n_tiles) * k * 2)) || (rc = bt->dalloc(&bt->d_B, nk)))
         return rc;
-    APXB_CK(cudaMallocHost(&bt->h_sd, sizeof(double) * 13 * ns));
+    APXB_CK(cudaMallocHost(&bt->h_sd, sizeof(double) * kSd * ns));
     APXB_CK(cudaMallocHost(&bt->h_si, sizeof(int) * (6 * ns + 1)));
-    APXB_CK(cudaMemsetAsync(bt->sd, 0, sizeof(double) * 13 * ns, s));
+    std::fill(bt->h_sd, bt->h_sd + kSd * ns, 0.0);
+    std::fill(bt->h_si, bt->h_si + 6 * ns + 1, 0);
+    std::fill(bt->h_si + ns, bt->h_si + 2 * ns, 1);   // host mirror of the idle state below
+    APXB_CK(cudaMemsetAsync(bt->sd, 0, sizeof(double) * kSd * ns, s));
     APXB_CK(cudaMemsetAsync(bt->si, 0, sizeof(int) * (6 * ns + 1), s));
+    {   // every slot starts idle: done, and the batch all done
+        std::vector<int> idle(ns + 1, 1);
+        APXB_CK(cudaMemcpyAsync(bt->si + ns, idle.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, s));
+        APXB_CK(cudaMemcpyAsync(bt->si + 6 * ns, idle.data(), sizeof(int), cudaMemcpyHostToDevice, s));
+    }
     APXB_CK(cudaMemsetAsync(bt->applies, 0, sizeof(unsigned long long) * ns, s));
     APXB_CK(cudaMemsetAsync(bt->p, 0, sizeof(double) * nk, s));
     // Zf: markers on factor rows, 0 on each Laplacian instance's grounded row
@@ -933,15 +995,15 @@ int apxb_batch_solve(apxb_batch* bt, const double* B, double* X, const int* nrhs
         APXB_CK(cudaMemcpyAsync(bt->d_B, B, 8 * nk, cudaMemcpyHostToDevice, s));
         dB = bt->d_B;
     }
-    if (!bt->one || bt->graph_tol != tol || bt->graph_max != max_iter) {
-        const int rc = build_graphs(bt, tol, max_iter);
+    {
+        const int rc = ensure_graphs(bt, max_iter);
         if (rc) return rc;
-        bt->graph_tol = tol;
-        bt->graph_max = max_iter;
     }
-    const bp P = bt->params(tol, max_iter);
-    // every slot fresh, nothing done
+    const bp P = bt->params(max_iter);
+    // every slot fresh with the call's tolerance, nothing done
     std::vector<int> ones(ns, 1);
+    std::vector<double> tols(ns, tol);
+    APXB_CK(cudaMemcpyAsync(P.tol, tols.data(), sizeof(double) * ns, cudaMemcpyHostToDevice, s));
     APXB_CK(cudaMemsetAsync(P.done, 0, sizeof(int) * ns, s));
     APXB_CK(cudaMemcpyAsync(P.fresh, ones.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, s));
     APXB_CK(cudaMemsetAsync(P.all_done, 0, sizeof(int), s));
@@ -978,7 +1040,7 @@ int apxb_batch_solve(apxb_batch* bt, const double* B, double* X, const int* nrhs
     APXB_CK(cudaEventRecord(e->ev1, s));
     APXB_CK(cudaGetLastError());
     if (!dev) APXB_CK(cudaMemcpyAsync(X, bt->d_B, 8 * nk, cudaMemcpyDeviceToHost, s));
-    APXB_CK(cudaMemcpyAsync(bt->h_sd, bt->sd, sizeof(double) * 13 * ns, cudaMemcpyDeviceToHost, s));
+    APXB_CK(cudaMemcpyAsync(bt->h_sd, bt->sd, sizeof(double) * kSd * ns, cudaMemcpyDeviceToHost, s));
     APXB_CK(cudaMemcpyAsync(bt->h_si, bt->si, sizeof(int) * 6 * ns, cudaMemcpyDeviceToHost, s));
     const int rc = e->take_error();
     if (rc) { bt->y_armed = false; cudaMemsetAsync(bt->ctl, 0, 2 * sizeof(apxb::sweep_ctl), s); return rc; }
@@ -991,6 +1053,144 @@ int apxb_batch_solve(apxb_batch* bt, const double* B, double* X, const int* nrhs
         res[sl].true_residual = (flags & APXB_TRUE_RESIDUAL) ? bt->h_sd[12 * ns + sl] : -1.0;
         res[sl].seconds = ms * 1e-3;
     }
+    return APXB_OK;
+}
+
+// ---- continuous batching ----
+
+int apxb_batch_admit(apxb_batch* bt, int slot, const double* b, double tol, int max_iter, int flags) {
+    if (!bt || !b || slot < 0 || static_cast<size_t>(slot) >= bt->slots() || !(tol >= 0.0) || max_iter < 0)
+        return fail(APXB_ERR_INVALID, "bad argument");
+    apxb_engine* e = bt->e;
+    APXB_CK(cudaSetDevice(e->device));
+    cudaStream_t s = e->stream;
+    if (bt->step_ev) APXB_CK(cudaEventSynchronize(bt->step_ev));
+    const size_t ns = bt->slots();
+    if (bt->one && !bt->h_si[ns + slot]) return fail(APXB_ERR_BUSY, "slot is still iterating");
+    if (bt->graph_max != max_iter) {
+        // the graphs bake max_iter: only change it while no slot is live
+        for (size_t sl = 0; bt->one && sl < ns; ++sl)
+            if (!bt->h_si[ns + sl]) return fail(APXB_ERR_BUSY, "max_iter differs from that of the live slots");
+        const int rc = ensure_graphs(bt, max_iter);
+        if (rc) return rc;
+    }
+    const bp P = bt->params(bt->graph_max);
+    const double* db = b;
+    if (!(flags & APXB_DEVICE_PTRS)) {
+        APXB_CK(cudaMemcpyAsync(bt->d_B, b, 8 * static_cast<size_t>(bt->n[slot / bt->K]), cudaMemcpyHostToDevice, s));
+        db = bt->d_B;
+    }
+    const int one = 1, zero = 0;
+    APXB_CK(cudaMemcpyAsync(P.fresh + slot, &one, sizeof(int), cudaMemcpyHostToDevice, s));
+    APXB_CK(cudaMemcpyAsync(P.done + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, s));
+    APXB_CK(cudaMemcpyAsync(P.all_done, &zero, sizeof(int), cudaMemcpyHostToDevice, s));
+    APXB_CK(cudaMemcpyAsync(P.tol + slot, &tol, sizeof(double), cudaMemcpyHostToDevice, s));
+    if (!bt->y_armed) { apxb::launch_fill_sent32(bt->Yf, static_cast<size_t>(bt->n_tot) * bt->K, s); bt->y_armed = true; }
+    slot_io(bt, P, static_cast<unsigned>(slot), db, nullptr, s);
+    APXB_CK(cudaGetLastError());
+    // the host words above and the staging buffer are reused: finish the upload
+    APXB_CK(cudaStreamSynchronize(s));
+    bt->h_si[ns + slot] = 0;
+    return e->take_error();
+}
+
+int apxb_batch_step(apxb_batch* bt, int iterations) {
+    if (!bt || iterations < 1) return fail(APXB_ERR_INVALID, "bad argument");
+    if (!bt->one) return fail(APXB_ERR_INVALID, "nothing admitted");
+    apxb_engine* e = bt->e;
+    APXB_CK(cudaSetDevice(e->device));
+    cudaStream_t s = e->stream;
+    for (int k = 0; k < iterations; ++k) APXB_CK(cudaGraphLaunch(bt->one, s));
+    const size_t ns = bt->slots();
+    // slot states to the pinned mirrors, then an event the host can poll
+    APXB_CK(cudaMemcpyAsync(bt->h_si, bt->si, sizeof(int) * (6 * ns + 1), cudaMemcpyDeviceToHost, s));
+    APXB_CK(cudaMemcpyAsync(bt->h_sd, bt->sd, sizeof(double) * kSd * ns, cudaMemcpyDeviceToHost, s));
+    if (!bt->step_ev) APXB_CK(cudaEventCreateWithFlags(&bt->step_ev, cudaEventDisableTiming));
+    APXB_CK(cudaEventRecord(bt->step_ev, s));
+    return APXB_OK;
+}
+
+int apxb_batch_query(apxb_batch* bt, int* ready) {
+    if (!bt || !ready) return fail(APXB_ERR_INVALID, "bad argument");
+    *ready = 1;
+    if (!bt->step_ev) return APXB_OK;
+    const cudaError_t q = cudaEventQuery(bt->step_ev);
+    if (q == cudaErrorNotReady) { *ready = 0; return APXB_OK; }
+    if (q != cudaSuccess) return fail(APXB_ERR_CUDA, cudaGetErrorString(q));
+    const int rc = bt->e->take_error();   // a device error recorded by the steps
+    if (rc) {
+        bt->y_armed = false;
+        cudaMemsetAsync(bt->ctl, 0, 2 * sizeof(apxb::sweep_ctl), bt->e->stream);
+        return rc;
+    }
+    return APXB_OK;
+}
+
+int apxb_batch_slots(const apxb_batch* bt, int* done, int* iterations, int* status, double* residual) {
+    if (!bt) return fail(APXB_ERR_INVALID, "batch is NULL");
+    if (bt->step_ev) APXB_CK(cudaEventSynchronize(bt->step_ev));
+    const size_t ns = bt->slots();
+    for (size_t sl = 0; sl < ns; ++sl) {
+        if (done) done[sl] = bt->h_si[ns + sl] && !bt->h_si[5 * ns + sl];
+        if (iterations) iterations[sl] = bt->h_si[sl];
+        if (status) status[sl] = bt->h_si[2 * ns + sl];
+        if (residual) residual[sl] = bt->h_sd[7 * ns + sl];
+    }
+    return APXB_OK;
+}
+
+int apxb_batch_retire(apxb_batch* bt, int slot, double* x, int flags) {
+    if (!bt || !x || slot < 0 || static_cast<size_t>(slot) >= bt->slots()) return fail(APXB_ERR_INVALID, "bad argument");
+    apxb_engine* e = bt->e;
+    APXB_CK(cudaSetDevice(e->device));
+    cudaStream_t s = e->stream;
+    if (bt->step_ev) APXB_CK(cudaEventSynchronize(bt->step_ev));
+    if (!bt->h_si[bt->slots() + slot]) return fail(APXB_ERR_BUSY, "slot has not finished");
+    const bp P = bt->params(bt->graph_max);
+    double* dx = (flags & APXB_DEVICE_PTRS) ? x : bt->d_B;
+    slot_io(bt, P, static_cast<unsigned>(slot), nullptr, dx, s);
+    APXB_CK(cudaGetLastError());
+    if (!(flags & APXB_DEVICE_PTRS))
+        APXB_CK(cudaMemcpyAsync(x, bt->d_B, 8 * static_cast<size_t>(bt->n[slot / bt->K]), cudaMemcpyDeviceToHost, s));
+    APXB_CK(cudaStreamSynchronize(s));
+    return e->take_error();
+}
+
+// Times the batch's own forward and backward fp32 sweeps (k columns) on the
+// right-hand sides of its last iteration; seconds per sweep of each direction.
+int apxb_batch_sweep_timed(apxb_batch* bt, int reps, double* fwd_seconds, double* bck_seconds) {
+    if (!bt || reps < 1 || !fwd_seconds || !bck_seconds) return fail(APXB_ERR_INVALID, "bad argument");
+    apxb_engine* e = bt->e;
+    APXB_CK(cudaSetDevice(e->device));
+    cudaStream_t s = e->stream;
+    cudaEvent_t ev[3];
+    for (auto& v : ev) APXB_CK(cudaEventCreate(&v));
+    if (!bt->y_armed) { apxb::launch_fill_sent32(bt->Yf, static_cast<size_t>(bt->n_tot) * bt->K, s); bt->y_armed = true; }
+    apxb::sweep_args<float> a{};
+    a.k = bt->K; a.err = e->d_err; a.budget_ns = e->budget_ns; a.skip = nullptr; a.m = bt->n_tot;
+    double tf = 0.0, tb = 0.0;
+    int rc = APXB_OK;
+    for (int r = 0; r < reps && rc == APXB_OK; ++r) {
+        APXB_CK(cudaEventRecord(ev[0], s));
+        for (int dir = 0; dir < 2; ++dir) {
+            a.n_items = bt->n_items[dir]; a.info = bt->info[dir]; a.ord = bt->ord[dir]; a.ptr = bt->ptr[dir];
+            a.idx = bt->idx[dir]; a.val = bt->val[dir]; a.ctl = bt->ctl + dir;
+            if (dir == 0) { a.in = bt->rhs32; a.out = bt->Yf; a.reset = bt->Zf; }
+            else { a.in = bt->Yf; a.out = bt->Zf; a.reset = bt->Yf; }
+            apxb::launch_sweep32(dir, a, bt->grid32, s);
+            APXB_CK(cudaEventRecord(ev[dir + 1], s));
+        }
+        APXB_CK(cudaEventSynchronize(ev[2]));
+        float m0 = 0.0f, m1 = 0.0f;
+        cudaEventElapsedTime(&m0, ev[0], ev[1]);
+        cudaEventElapsedTime(&m1, ev[1], ev[2]);
+        tf += m0 * 1e-3; tb += m1 * 1e-3;
+        rc = e->take_error();
+    }
+    for (auto& v : ev) cudaEventDestroy(v);
+    if (rc) { bt->y_armed = false; cudaMemsetAsync(bt->ctl, 0, 2 * sizeof(apxb::sweep_ctl), s); return rc; }
+    *fwd_seconds = tf / reps;
+    *bck_seconds = tb / reps;
     return APXB_OK;
 }
 

@@ -1,0 +1,243 @@
+"""Solve server: resident factors, continuous batching, an HBM byte budget.
+
+Each resident matrix gets its own engine (CUDA stream), factor, operator and
+a batch of k right-hand-side slots (fp32 preconditioner sweeps, fp64 PCG;
+native.Batch). Requests (matrix id, right-hand side, tolerance) are admitted
+into free slots at iteration boundaries while the other slots keep
+iterating, and leave the moment they converge, so work of requests that
+arrive while others are running overlaps on the device -- across slots of one
+matrix and, through the per-matrix streams, across matrices.
+
+Matrices are admitted against a device-memory budget; when a new matrix does
+not fit, idle resident matrices are evicted least-recently-used first, and a
+matrix that still does not fit is refused (BudgetError).
+
+The reference has no serving layer; the per-request semantics are those of
+its cpu_solver::solve (src/solve.cpp:478-654) with the request's tolerance.
+"""
+from __future__ import annotations
+
+import collections
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import native
+
+
+class BudgetError(RuntimeError):
+    pass
+
+
+@dataclass
+class Request:
+    rid: int
+    mid: object
+    b: np.ndarray
+    tol: float
+    arrival: float                 # host clock (time.perf_counter) when it was submitted
+    start: float = 0.0             # when it entered a slot
+    finish: float = 0.0
+    x: np.ndarray | None = None
+    iterations: int = 0
+    status: int = -1
+    residual: float = float("nan")
+
+    @property
+    def latency(self) -> float:
+        return self.finish - self.arrival
+
+
+@dataclass
+class _Resident:
+    mid: object
+    eng: native.Engine
+    factor: native.DeviceFactor
+    op: native.DeviceOperator
+    batch: native.Batch
+    n: int
+    nbytes: int
+    queue: collections.deque = field(default_factory=collections.deque)
+    slots: list = field(default_factory=list)       # Request or None per slot
+    stepping: bool = False
+    last_used: float = 0.0
+
+    def busy(self) -> bool:
+        return bool(self.queue) or any(s is not None for s in self.slots)
+
+    def close(self):
+        self.batch.close(); self.op.close(); self.factor.close(); self.eng.close()
+
+
+def estimate_bytes(n: int, nnz_factor: int, nnz_a: int, k: int) -> int:
+    """Upper estimate of the device bytes of one resident matrix: the two
+    sweep plans (entries + 32-position items), the fp32 sweep vectors, the
+    permuted operator with its PCG vectors, and the batch's k-slot vectors."""
+    plan = 2 * (nnz_factor * 8 + n * 4 * 6)
+    operator = nnz_a * 12 + n * (4 + 8 * 7)
+    batch = n * k * (8 * 5 + 4 * 3) + n * 8
+    return int(1.25 * (plan + operator + batch)) + (4 << 20)
+
+
+class SolveServer:
+    """Continuous-batching solve server on one GPU.
+
+    register(mid, matrix, factor) makes a matrix known; submit(mid, b, tol)
+    queues a request (admitting the matrix under the budget if needed);
+    pump() advances every resident matrix once without blocking; drain()
+    pumps until every request is done; run_open_loop(arrivals) submits
+    requests at their arrival times while serving."""
+
+    def __init__(self, device: int = 0, budget_bytes: int = 60 * 10**9, k: int = 8, iters_per_step: int = 2,
+                 max_iter: int = 500):
+        self.device, self.budget, self.k = device, int(budget_bytes), k
+        self.iters_per_step, self.max_iter = iters_per_step, max_iter
+        self.resident: dict = {}
+        self.catalog: dict = {}          # mid -> (matrix, factor) that can be (re)admitted
+        self.completed: list = []
+        self.evictions = 0
+        self.admissions = 0
+        self._rid = 0
+
+    # ---- matrices ----
+    def register(self, mid, mat, fac):
+        """Make a matrix known to the server (admitted to the device on first use)."""
+        self.catalog[mid] = (mat, fac)
+
+    def estimate(self, mid) -> int:
+        mat, fac = self.catalog[mid]
+        return estimate_bytes(mat.n, fac.nnz, mat.nnz, self.k)
+
+    def used_bytes(self) -> int:
+        """Bytes reserved by resident matrices (each: the larger of its estimate and its measured use)."""
+        return sum(r.nbytes for r in self.resident.values())
+
+    def admit_matrix(self, mid):
+        if mid in self.resident:
+            return self.resident[mid]
+        mat, fac = self.catalog[mid]
+        need = self.estimate(mid)
+        while self.used_bytes() + need > self.budget:
+            idle = [r for r in self.resident.values() if not r.busy() and not r.stepping]
+            if not idle:
+                raise BudgetError(f"matrix {mid!r} needs {need} bytes; {self.used_bytes()} of {self.budget} in use "
+                                  "by busy matrices")
+            victim = min(idle, key=lambda r: r.last_used)
+            self.evict(victim.mid)
+        eng = native.Engine(self.device)
+        eng.set_memory_budget(self.budget - self.used_bytes())   # the engine refuses what would overrun the budget
+        f = op = None
+        try:
+            f = native.DeviceFactor(eng, fac, precision=native.PREC_FP32)
+            op = native.DeviceOperator(eng, mat, fac.perm)
+            bt = native.Batch(eng, [f], [op], self.k)
+        except native.ApxbError as ex:
+            for o in (op, f, eng):
+                if o is not None:
+                    o.close()
+            if ex.code == native.ERR_BUDGET:
+                raise BudgetError(str(ex)) from ex
+            raise
+        r = _Resident(mid=mid, eng=eng, factor=f, op=op, batch=bt, n=mat.n, nbytes=max(need, eng.memory_used()),
+                      slots=[None] * self.k, last_used=time.perf_counter())
+        self.resident[mid] = r
+        self.admissions += 1
+        return r
+
+    def evict(self, mid):
+        r = self.resident[mid]
+        if r.busy() or r.stepping:
+            raise RuntimeError("cannot evict a matrix with requests in flight")
+        del self.resident[mid]
+        r.close()
+        self.evictions += 1
+
+    # ---- requests ----
+    def submit(self, mid, b, tol: float = 1e-8, arrival: float | None = None) -> Request:
+        if mid not in self.catalog:
+            raise KeyError(f"unknown matrix {mid!r}")
+        self._rid += 1
+        req = Request(rid=self._rid, mid=mid, b=np.ascontiguousarray(b, np.float64), tol=tol,
+                      arrival=time.perf_counter() if arrival is None else arrival)
+        r = self.admit_matrix(mid)
+        r.queue.append(req)
+        return req
+
+    def _service(self, r: _Resident) -> bool:
+        """One pass over a resident matrix; returns whether anything happened."""
+        progressed = False
+        if r.stepping:
+            if not r.batch.ready():
+                return False
+            r.stepping = False
+            done, its, st, res = r.batch.slots()
+            for s, req in enumerate(r.slots):
+                if req is not None and done[s]:
+                    req.x = r.batch.retire(s)
+                    req.iterations, req.status, req.residual = int(its[s]), int(st[s]), float(res[s])
+                    req.finish = time.perf_counter()
+                    self.completed.append(req)
+                    r.slots[s] = None
+                    progressed = True
+        # admit waiting requests into free slots
+        for s in range(self.k):
+            if r.slots[s] is None and r.queue:
+                req = r.queue.popleft()
+                req.start = time.perf_counter()
+                r.batch.admit(s, req.b, req.tol, self.max_iter)
+                r.slots[s] = req
+                progressed = True
+        if any(x is not None for x in r.slots):
+            r.batch.step(self.iters_per_step)
+            r.stepping = True
+            r.last_used = time.perf_counter()
+            progressed = True
+        return progressed
+
+    def pump(self) -> bool:
+        """Service every resident matrix once."""
+        any_progress = False
+        for r in list(self.resident.values()):
+            any_progress |= self._service(r)
+        return any_progress
+
+    def idle(self) -> bool:
+        return not any(r.busy() or r.stepping for r in self.resident.values())
+
+    def drain(self, timeout: float = 600.0):
+        t0 = time.perf_counter()
+        while not self.idle():
+            if not self.pump():
+                time.sleep(20e-6)
+            if time.perf_counter() - t0 > timeout:
+                raise TimeoutError("server did not drain")
+
+    def run_open_loop(self, arrivals):
+        """arrivals: list of (t_offset_seconds, mid, b, tol) sorted by time.
+        Submits each at its time (open loop) while serving; returns the
+        completed requests of this run."""
+        start_n = len(self.completed)
+        t0 = time.perf_counter()
+        i = 0
+        while i < len(arrivals) or not self.idle():
+            now = time.perf_counter() - t0
+            while i < len(arrivals) and arrivals[i][0] <= now:
+                dt, mid, b, tol = arrivals[i]
+                self.submit(mid, b, tol, arrival=t0 + dt)
+                i += 1
+            if not self.pump():
+                time.sleep(20e-6)
+        return self.completed[start_n:]
+
+    def close(self):
+        for mid in list(self.resident):
+            self.resident.pop(mid).close()
+
+
+def latency_stats(reqs):
+    lat = np.array([q.latency for q in reqs]) * 1e3
+    if lat.size == 0:
+        return {"count": 0}
+    return {"count": int(lat.size), "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(lat.mean()), "max_ms": float(lat.max())}

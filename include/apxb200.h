@@ -181,6 +181,31 @@ int apxb_batch_size(const apxb_batch* b, int* n_inst, int* k, uint32_t* n_total)
 int apxb_batch_solve(apxb_batch* b, const double* B, double* X, const int* nrhs, double tol, int max_iter,
                      int flags, apxb_pcg_result* res);
 
+/* ---- continuous batching (the serving form; no counterpart in the reference) ----
+ * Slots are admitted and retired one at a time while the other slots keep
+ * iterating. Slot s belongs to instance s / k. A new batch has every slot idle.
+ *  admit:  load b (instance's n values, original ordering) into an idle slot
+ *          with its own tolerance; the slot starts at the next iteration.
+ *          max_iter can change only while no slot is live (else APXB_ERR_BUSY).
+ *  step:   enqueue `iterations` PCG iterations of every live slot and a copy
+ *          of the slot states; returns without waiting.
+ *  query:  *ready = 1 once the last step has finished (non-blocking).
+ *  slots:  states after the last step (waits for it): done (finished and not
+ *          re-admitted), iterations, status (as apxb_pcg_result.status) and
+ *          recurrence residual per slot; any pointer may be NULL.
+ *  retire: x of a finished slot (original ordering; Laplacian instances
+ *          centred); the slot stays idle until admitted again.
+ * A slot's arithmetic does not depend on the other slots, so a right-hand
+ * side gives the same bits alone and in any mix. */
+int apxb_batch_admit(apxb_batch* b, int slot, const double* rhs, double tol, int max_iter, int flags);
+int apxb_batch_step(apxb_batch* b, int iterations);
+int apxb_batch_query(apxb_batch* b, int* ready);
+int apxb_batch_slots(const apxb_batch* b, int* done, int* iterations, int* status, double* residual);
+int apxb_batch_retire(apxb_batch* b, int slot, double* x, int flags);
+/* Times the batch's forward and backward fp32 sweeps (all k columns) on the
+ * right-hand sides of its last iteration: seconds per sweep, mean of reps. */
+int apxb_batch_sweep_timed(apxb_batch* b, int reps, double* fwd_seconds, double* bck_seconds);
+
 /* ---- failure detection test hook ----
  * Runs one forward sweep whose first 32 rows are never solved (the work
  * counter starts past them), so every row that depends on them waits on a
