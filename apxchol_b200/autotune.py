@@ -1,0 +1,81 @@
+"""Autotuner of the batched mixed-precision form.
+
+For one matrix it times a whole batched solve (CUDA events, device-resident
+right-hand sides) for every right-hand-side block width k in {1, 2, 4, 8, 16}
+and every candidate sweep grid (the resident grid and one block per SM), and
+keeps the fastest solves/s. The sweeps' other knobs are fixed by the plan: the
+lanes per row follow the row length (1, 4, 8, 16 or 32), and the in-flight
+depth is the 3-stage item pipeline with 8 entries per lane.
+
+The reference has no autotuner; its GPU path solves one right-hand side at a
+time (cuda_pcg::solve, include/apxchol/solver/pcg_cuda.h:157-261).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import native
+
+KS = (1, 2, 4, 8, 16)
+
+
+@dataclass
+class Choice:
+    k: int
+    grid: int                     # 0 = the resident grid
+    solves_per_s: float
+    seconds_per_batch: float
+    iterations: int
+    table: list = field(default_factory=list)   # (k, grid, solves/s, iterations) of every candidate
+
+
+def _num_sms(device: int) -> int:
+    import torch
+    return torch.cuda.get_device_properties(device).multi_processor_count
+
+
+def time_batch(eng: native.Engine, bt: native.Batch, rhs, tol: float, max_iter: int, reps: int = 1):
+    """Device seconds of one batched solve of bt.k right-hand sides (rhs(j) -> array), best of reps."""
+    import torch
+    B = np.stack([rhs(j) for j in range(bt.k)])
+    Bf, nrhs = bt.pack([B])
+    dB = torch.from_numpy(Bf).cuda(eng.device)
+    dX = torch.empty_like(dB)
+    res = bt.solve_raw(dB, dX, nrhs, tol=tol, max_iter=max_iter, flags=native.DEVICE_PTRS)   # warm-up
+    best = float("inf")
+    for _ in range(reps):
+        res = bt.solve_raw(dB, dX, nrhs, tol=tol, max_iter=max_iter, flags=native.DEVICE_PTRS)
+        best = min(best, res[0].seconds)
+    its = max(res[c].iterations for c in range(bt.k))
+    return best, its
+
+
+def tune(eng: native.Engine, factor: native.DeviceFactor, op: native.DeviceOperator, rhs, tol: float = 1e-8,
+         max_iter: int = 500, ks=KS, grids=None, reps: int = 1, log=None) -> Choice:
+    """Pick k and the sweep grid for one matrix. rhs(j) gives the j-th right-hand side."""
+    if grids is None:
+        grids = (0, _num_sms(eng.device))
+    table = []
+    best = None
+    try:
+        for grid in grids:
+            eng.set_sweep_grid(grid)
+            for k in ks:
+                bt = native.Batch(eng, [factor], [op], k)
+                try:
+                    secs, its = time_batch(eng, bt, rhs, tol, max_iter, reps)
+                finally:
+                    bt.close()
+                sps = k / secs
+                table.append((k, grid, sps, its))
+                if log:
+                    log(f"[autotune] k={k:2d} grid={grid or 'resident'}: {secs * 1e3:8.2f} ms/batch, "
+                        f"{sps:8.1f} solves/s, {its} iterations")
+                if best is None or sps > best.solves_per_s:
+                    best = Choice(k=k, grid=grid, solves_per_s=sps, seconds_per_batch=secs, iterations=its)
+    finally:
+        eng.set_sweep_grid(0)
+    best.table = table
+    return best

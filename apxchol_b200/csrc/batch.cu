@@ -854,7 +854,7 @@ int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, a
     }
     if ((rc = bt->dalloc(&bt->ctl, 2))) return rc;
     APXB_CK(cudaMemsetAsync(bt->ctl, 0, sizeof(apxb::sweep_ctl) * 2, s));
-    bt->grid32 = apxb::sweep_grid32(k, e->num_sms);
+    bt->grid32 = e->sweep_grid > 0 ? e->sweep_grid : apxb::sweep_grid32(k, e->num_sms);
     // ---- operator ----
     if (n_inst == 1) {
         bt->a_ptr = ops[0]->ptr; bt->a_idx = ops[0]->idx; bt->a_val = ops[0]->val;

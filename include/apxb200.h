@@ -92,7 +92,8 @@ void* apxb_engine_stream(apxb_engine* e);
 /* Spin budget of every device wait, in nanoseconds (default 2e9). */
 int apxb_engine_set_spin_budget(apxb_engine* e, uint64_t ns);
 /* Blocks of the persistent sweep launches (0 = the resident grid). Any value
- * gives the same bytes; tests use it to show the result is schedule-free. */
+ * gives the same bytes; tests use it to show the result is schedule-free.
+ * Batches read it when they are created. */
 int apxb_engine_set_sweep_grid(apxb_engine* e, int blocks);
 /* Device-memory budget for factors and operators created on this engine (0 = unlimited). */
 int apxb_engine_set_memory_budget(apxb_engine* e, uint64_t bytes);

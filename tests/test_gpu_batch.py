@@ -75,3 +75,12 @@ def test_batch_repeats_bitwise(eng):
     x2, r2 = bt.solve([B], tol=TOL)
     assert np.array_equal(x1[0], x2[0])
     assert [r.iterations for r in r1[0]] == [r.iterations for r in r2[0]]
+
+
+def test_autotuner_picks_the_fastest_candidate(eng):
+    from apxchol_b200 import autotune
+    A, F, D, Op = _objs(eng, "grid3d_24")
+    ch = autotune.tune(eng, D, Op, lambda j: gen.rhs(A.n, 500 + j, False), ks=(1, 4), grids=(0, 64))
+    assert len(ch.table) == 4
+    assert ch.solves_per_s == max(t[2] for t in ch.table)
+    assert (ch.k, ch.grid) in [(t[0], t[1]) for t in ch.table]
