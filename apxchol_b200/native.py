@@ -70,6 +70,7 @@ _SIGS = {
     "apxb_sweep_pair_host": (ctypes.c_int, [c_p, c_p, c_p, c_p]),
     "apxb_sweep_pair_timed": (ctypes.c_int, [c_p, c_p, c_p, c_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "apxb_sweep_pair_multi": (ctypes.c_int, [c_p, c_p, ctypes.c_int, c_p, c_p]),
+    "apxb_sweep_pair_noalloc": (ctypes.c_int, [c_p, c_p, c_p, c_p]),
     "apxb_apply": (ctypes.c_int, [c_p, c_p, c_p, c_p, ctypes.c_int, c_p]),
     "apxb_operator_create": (ctypes.c_int, [c_p, ctypes.c_uint32, c_p, c_p, c_p, c_p, ctypes.POINTER(c_p)]),
     "apxb_operator_destroy": (ctypes.c_int, [c_p]),

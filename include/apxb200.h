@@ -135,6 +135,22 @@ int apxb_prepare_host(uint32_t n, const uint32_t* colptr, const uint32_t* rowidx
 int apxb_sweep(apxb_engine* e, apxb_factor* f, int dir, const double* d_in, double* d_out);
 /* Both sweeps: out = (L L^T)^-1 in. Device pointers (in and out may alias). */
 int apxb_sweep_pair(apxb_engine* e, apxb_factor* f, const double* d_in, double* d_out);
+/* apxb_sweep_pair without any device allocation in the call. No counterpart
+ * in the reference. For callers that cannot allocate device memory when they
+ * apply the preconditioner: hosts that reserve the GPU's memory for their own
+ * pool and forbid allocations outside it, and latency-bound loops that cannot
+ * take the device-wide synchronisation cudaMalloc / cudaFree may cause.
+ * Same result as apxb_sweep_pair, bit for bit. The intermediate vectors live in
+ * one fixed array of device memory owned by the library, 1 MiB + 256 B on every
+ * GPU that loads it, held until the process exits; so the factor's m must be
+ * at most 65,536 (larger: APXB_ERR_INVALID, with the limit in the message),
+ * and the factor must be fp64. The engine and the factor are created (and
+ * allocate) beforehand. The first call on a device looks up the array's
+ * device address on it: make that first call before any stream capture.
+ * Every call re-arms the array, but all calls on one device share it: calls
+ * whose work overlaps on the GPU (other engines' streams, other host threads)
+ * race and corrupt each other's results. */
+int apxb_sweep_pair_noalloc(apxb_engine* e, apxb_factor* f, const double* d_in, double* d_out);
 /* The same with host pointers (cuda_sptrsv::solve_LLt, cuda.h:464-473). */
 int apxb_sweep_pair_host(apxb_engine* e, apxb_factor* f, const double* in, double* out);
 /* reps back-to-back pairs on the engine stream, timed with CUDA events; *seconds = per pair. */
