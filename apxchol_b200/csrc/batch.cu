@@ -501,6 +501,17 @@ __global__ void __launch_bounds__(kBT) k_b_slot_out(bp P, unsigned sl, double* o
         out[v] = P.x[static_cast<size_t>(P.gperm[off + v]) * K + c] - mean;
 }
 
+// Slot state of an admission: fresh (its first iteration initialises it), not
+// done, its tolerance; the batch is live again.
+__global__ void k_b_mark_admit(bp P, unsigned sl, double tol) {
+    if (threadIdx.x == 0) {
+        P.fresh[sl] = 1;
+        P.done[sl] = 0;
+        P.tol[sl] = tol;
+        *P.all_done = 0;
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -545,7 +556,15 @@ struct apxb_batch {
     cudaGraphExec_t one = nullptr;
     bool loop_cond = false;
     int graph_max = -1;
-    cudaEvent_t step_ev = nullptr;   // recorded after each apxb_batch_step
+    // continuous batching: two state mirrors (steps alternate), per-slot
+    // admission flags and retirement events
+    int64_t steps_launched = 0;
+    cudaEvent_t step_ev[2] = {nullptr, nullptr};
+    double* m_sd[2] = {nullptr, nullptr};
+    int* m_si[2] = {nullptr, nullptr};
+    apxb::dev_error* m_err[2] = {nullptr, nullptr};
+    std::vector<char> slot_busy;
+    std::vector<cudaEvent_t> slot_ev;
     // pinned host mirrors
     double* h_sd = nullptr;
     int* h_si = nullptr;
@@ -559,7 +578,14 @@ struct apxb_batch {
         return APXB_OK;
     }
     ~apxb_batch() {
-        if (step_ev) cudaEventDestroy(step_ev);
+        for (int j = 0; j < 2; ++j) {
+            if (step_ev[j]) cudaEventDestroy(step_ev[j]);
+            if (m_sd[j]) cudaFreeHost(m_sd[j]);
+            if (m_si[j]) cudaFreeHost(m_si[j]);
+            if (m_err[j]) cudaFreeHost(m_err[j]);
+        }
+        for (auto ev : slot_ev)
+            if (ev) cudaEventDestroy(ev);
         if (loop) cudaGraphExecDestroy(loop);
         if (one) cudaGraphExecDestroy(one);
         for (auto& [q, bytes] : owned) e->release(q, bytes);
@@ -978,6 +1004,8 @@ int apxb_batch_solve(apxb_batch* bt, const double* B, double* X, const int* nrhs
                      int flags, apxb_pcg_result* res) {
     if (!bt || !B || !X || !res) return fail(APXB_ERR_INVALID, "bad argument");
     if (!(tol >= 0.0) || max_iter < 0) return fail(APXB_ERR_INVALID, "bad tol / max_iter");
+    for (char busy : bt->slot_busy)
+        if (busy) return fail(APXB_ERR_BUSY, "slots are admitted for continuous batching");
     apxb_engine* e = bt->e;
     APXB_CK(cudaSetDevice(e->device));
     cudaStream_t s = e->stream;
@@ -1057,84 +1085,128 @@ int apxb_batch_solve(apxb_batch* bt, const double* B, double* X, const int* nrhs
 }
 
 // ---- continuous batching ----
+// Everything is enqueued on the engine stream in order and nothing waits,
+// so the host can keep iterations queued while it admits and retires slots.
+
+namespace {
+
+// Staging of slot sl (instance i, column c) in the caller layout: K*off_i + c*n_i.
+double* slot_stage(apxb_batch* bt, unsigned sl) {
+    const unsigned i = sl / bt->K, c = sl % bt->K;
+    return bt->d_B + static_cast<size_t>(bt->K) * bt->off[i] + static_cast<size_t>(c) * bt->n[i];
+}
+
+int serving_init(apxb_batch* bt) {
+    if (bt->step_ev[0]) return APXB_OK;
+    const size_t ns = bt->slots();
+    for (int j = 0; j < 2; ++j) {
+        APXB_CK(cudaEventCreateWithFlags(&bt->step_ev[j], cudaEventDisableTiming));
+        APXB_CK(cudaMallocHost(&bt->m_sd[j], sizeof(double) * kSd * ns));
+        APXB_CK(cudaMallocHost(&bt->m_si[j], sizeof(int) * (6 * ns + 1)));
+        APXB_CK(cudaMallocHost(&bt->m_err[j], sizeof(apxb::dev_error)));
+    }
+    bt->slot_busy.assign(ns, 0);
+    bt->slot_ev.assign(ns, nullptr);
+    for (auto& ev : bt->slot_ev) APXB_CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    return APXB_OK;
+}
+
+}  // namespace
 
 int apxb_batch_admit(apxb_batch* bt, int slot, const double* b, double tol, int max_iter, int flags) {
     if (!bt || !b || slot < 0 || static_cast<size_t>(slot) >= bt->slots() || !(tol >= 0.0) || max_iter < 0)
         return fail(APXB_ERR_INVALID, "bad argument");
     apxb_engine* e = bt->e;
     APXB_CK(cudaSetDevice(e->device));
+    int rc = serving_init(bt);
+    if (rc) return rc;
+    if (bt->slot_busy[slot]) return fail(APXB_ERR_BUSY, "slot is admitted and not retired");
     cudaStream_t s = e->stream;
-    if (bt->step_ev) APXB_CK(cudaEventSynchronize(bt->step_ev));
-    const size_t ns = bt->slots();
-    if (bt->one && !bt->h_si[ns + slot]) return fail(APXB_ERR_BUSY, "slot is still iterating");
     if (bt->graph_max != max_iter) {
-        // the graphs bake max_iter: only change it while no slot is live
-        for (size_t sl = 0; bt->one && sl < ns; ++sl)
-            if (!bt->h_si[ns + sl]) return fail(APXB_ERR_BUSY, "max_iter differs from that of the live slots");
-        const int rc = ensure_graphs(bt, max_iter);
-        if (rc) return rc;
+        // the graphs bake max_iter: change it only while no slot is admitted
+        for (char busy : bt->slot_busy)
+            if (busy) return fail(APXB_ERR_BUSY, "max_iter differs from that of the admitted slots");
+        if ((rc = ensure_graphs(bt, max_iter))) return rc;
     }
     const bp P = bt->params(bt->graph_max);
+    const unsigned sl = static_cast<unsigned>(slot);
     const double* db = b;
     if (!(flags & APXB_DEVICE_PTRS)) {
-        APXB_CK(cudaMemcpyAsync(bt->d_B, b, 8 * static_cast<size_t>(bt->n[slot / bt->K]), cudaMemcpyHostToDevice, s));
-        db = bt->d_B;
+        double* st = slot_stage(bt, sl);
+        APXB_CK(cudaMemcpyAsync(st, b, 8 * static_cast<size_t>(bt->n[sl / bt->K]), cudaMemcpyHostToDevice, s));
+        db = st;
     }
-    const int one = 1, zero = 0;
-    APXB_CK(cudaMemcpyAsync(P.fresh + slot, &one, sizeof(int), cudaMemcpyHostToDevice, s));
-    APXB_CK(cudaMemcpyAsync(P.done + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, s));
-    APXB_CK(cudaMemcpyAsync(P.all_done, &zero, sizeof(int), cudaMemcpyHostToDevice, s));
-    APXB_CK(cudaMemcpyAsync(P.tol + slot, &tol, sizeof(double), cudaMemcpyHostToDevice, s));
     if (!bt->y_armed) { apxb::launch_fill_sent32(bt->Yf, static_cast<size_t>(bt->n_tot) * bt->K, s); bt->y_armed = true; }
-    slot_io(bt, P, static_cast<unsigned>(slot), db, nullptr, s);
+    slot_io(bt, P, sl, db, nullptr, s);
+    k_b_mark_admit<<<1, 32, 0, s>>>(P, sl, tol);
     APXB_CK(cudaGetLastError());
-    // the host words above and the staging buffer are reused: finish the upload
-    APXB_CK(cudaStreamSynchronize(s));
-    bt->h_si[ns + slot] = 0;
-    return e->take_error();
+    bt->slot_busy[slot] = 1;
+    return APXB_OK;
 }
 
-int apxb_batch_step(apxb_batch* bt, int iterations) {
-    if (!bt || iterations < 1) return fail(APXB_ERR_INVALID, "bad argument");
-    if (!bt->one) return fail(APXB_ERR_INVALID, "nothing admitted");
+int apxb_batch_step(apxb_batch* bt, int iterations, int64_t* step_id) {
+    if (!bt || iterations < 1 || !step_id) return fail(APXB_ERR_INVALID, "bad argument");
+    if (!bt->one || !bt->step_ev[0]) return fail(APXB_ERR_INVALID, "nothing admitted");
     apxb_engine* e = bt->e;
     APXB_CK(cudaSetDevice(e->device));
     cudaStream_t s = e->stream;
+    const int j = static_cast<int>(bt->steps_launched & 1);
+    // mirror j was last written by step id - 2, which the caller has consumed
+    APXB_CK(cudaEventSynchronize(bt->step_ev[j]));
     for (int k = 0; k < iterations; ++k) APXB_CK(cudaGraphLaunch(bt->one, s));
     const size_t ns = bt->slots();
-    // slot states to the pinned mirrors, then an event the host can poll
-    APXB_CK(cudaMemcpyAsync(bt->h_si, bt->si, sizeof(int) * (6 * ns + 1), cudaMemcpyDeviceToHost, s));
-    APXB_CK(cudaMemcpyAsync(bt->h_sd, bt->sd, sizeof(double) * kSd * ns, cudaMemcpyDeviceToHost, s));
-    if (!bt->step_ev) APXB_CK(cudaEventCreateWithFlags(&bt->step_ev, cudaEventDisableTiming));
-    APXB_CK(cudaEventRecord(bt->step_ev, s));
+    APXB_CK(cudaMemcpyAsync(bt->m_si[j], bt->si, sizeof(int) * (6 * ns + 1), cudaMemcpyDeviceToHost, s));
+    APXB_CK(cudaMemcpyAsync(bt->m_sd[j], bt->sd, sizeof(double) * kSd * ns, cudaMemcpyDeviceToHost, s));
+    APXB_CK(cudaMemcpyAsync(bt->m_err[j], e->d_err, sizeof(apxb::dev_error), cudaMemcpyDeviceToHost, s));
+    APXB_CK(cudaEventRecord(bt->step_ev[j], s));
+    *step_id = bt->steps_launched++;
     return APXB_OK;
 }
 
-int apxb_batch_query(apxb_batch* bt, int* ready) {
+namespace {
+
+int step_mirror(const apxb_batch* bt, int64_t step_id, int* j) {
+    if (step_id < 0 || step_id >= bt->steps_launched || step_id < bt->steps_launched - 2)
+        return fail(APXB_ERR_INVALID, "step id is not one of the last two steps");
+    *j = static_cast<int>(step_id & 1);
+    return APXB_OK;
+}
+
+}  // namespace
+
+int apxb_batch_query(apxb_batch* bt, int64_t step_id, int* ready) {
     if (!bt || !ready) return fail(APXB_ERR_INVALID, "bad argument");
-    *ready = 1;
-    if (!bt->step_ev) return APXB_OK;
-    const cudaError_t q = cudaEventQuery(bt->step_ev);
+    int j = 0;
+    int rc = step_mirror(bt, step_id, &j);
+    if (rc) return rc;
+    const cudaError_t q = cudaEventQuery(bt->step_ev[j]);
     if (q == cudaErrorNotReady) { *ready = 0; return APXB_OK; }
     if (q != cudaSuccess) return fail(APXB_ERR_CUDA, cudaGetErrorString(q));
-    const int rc = bt->e->take_error();   // a device error recorded by the steps
-    if (rc) {
+    *ready = 1;
+    if (bt->m_err[j]->code != 0) {   // a device error recorded during the step
+        bt->m_err[j]->code = 0;
+        rc = bt->e->take_error();
         bt->y_armed = false;
         cudaMemsetAsync(bt->ctl, 0, 2 * sizeof(apxb::sweep_ctl), bt->e->stream);
-        return rc;
+        return rc ? rc : fail(APXB_ERR_CUDA, "device error during a step");
     }
     return APXB_OK;
 }
 
-int apxb_batch_slots(const apxb_batch* bt, int* done, int* iterations, int* status, double* residual) {
+int apxb_batch_slots(const apxb_batch* bt, int64_t step_id, int* done, int* iterations, int* status,
+                     double* residual) {
     if (!bt) return fail(APXB_ERR_INVALID, "batch is NULL");
-    if (bt->step_ev) APXB_CK(cudaEventSynchronize(bt->step_ev));
+    int j = 0;
+    const int rc = step_mirror(bt, step_id, &j);
+    if (rc) return rc;
+    APXB_CK(cudaEventSynchronize(bt->step_ev[j]));
     const size_t ns = bt->slots();
+    const int* si = bt->m_si[j];
     for (size_t sl = 0; sl < ns; ++sl) {
-        if (done) done[sl] = bt->h_si[ns + sl] && !bt->h_si[5 * ns + sl];
-        if (iterations) iterations[sl] = bt->h_si[sl];
-        if (status) status[sl] = bt->h_si[2 * ns + sl];
-        if (residual) residual[sl] = bt->h_sd[7 * ns + sl];
+        if (done) done[sl] = si[ns + sl] && !si[5 * ns + sl];
+        if (iterations) iterations[sl] = si[sl];
+        if (status) status[sl] = si[2 * ns + sl];
+        if (residual) residual[sl] = bt->m_sd[j][7 * ns + sl];
     }
     return APXB_OK;
 }
@@ -1143,17 +1215,28 @@ int apxb_batch_retire(apxb_batch* bt, int slot, double* x, int flags) {
     if (!bt || !x || slot < 0 || static_cast<size_t>(slot) >= bt->slots()) return fail(APXB_ERR_INVALID, "bad argument");
     apxb_engine* e = bt->e;
     APXB_CK(cudaSetDevice(e->device));
+    if (bt->slot_busy.empty() || !bt->slot_busy[slot]) return fail(APXB_ERR_INVALID, "slot was not admitted");
     cudaStream_t s = e->stream;
-    if (bt->step_ev) APXB_CK(cudaEventSynchronize(bt->step_ev));
-    if (!bt->h_si[bt->slots() + slot]) return fail(APXB_ERR_BUSY, "slot has not finished");
     const bp P = bt->params(bt->graph_max);
-    double* dx = (flags & APXB_DEVICE_PTRS) ? x : bt->d_B;
-    slot_io(bt, P, static_cast<unsigned>(slot), nullptr, dx, s);
+    const unsigned sl = static_cast<unsigned>(slot);
+    double* dx = (flags & APXB_DEVICE_PTRS) ? x : slot_stage(bt, sl);
+    slot_io(bt, P, sl, nullptr, dx, s);
     APXB_CK(cudaGetLastError());
     if (!(flags & APXB_DEVICE_PTRS))
-        APXB_CK(cudaMemcpyAsync(x, bt->d_B, 8 * static_cast<size_t>(bt->n[slot / bt->K]), cudaMemcpyDeviceToHost, s));
-    APXB_CK(cudaStreamSynchronize(s));
-    return e->take_error();
+        APXB_CK(cudaMemcpyAsync(x, dx, 8 * static_cast<size_t>(bt->n[sl / bt->K]), cudaMemcpyDeviceToHost, s));
+    APXB_CK(cudaEventRecord(bt->slot_ev[slot], s));
+    bt->slot_busy[slot] = 0;
+    return APXB_OK;
+}
+
+int apxb_batch_retired(apxb_batch* bt, int slot, int* ready) {
+    if (!bt || !ready || slot < 0 || static_cast<size_t>(slot) >= bt->slots() || bt->slot_ev.empty())
+        return fail(APXB_ERR_INVALID, "bad argument");
+    const cudaError_t q = cudaEventQuery(bt->slot_ev[slot]);
+    if (q == cudaErrorNotReady) { *ready = 0; return APXB_OK; }
+    if (q != cudaSuccess) return fail(APXB_ERR_CUDA, cudaGetErrorString(q));
+    *ready = 1;
+    return APXB_OK;
 }
 
 // Times the batch's own forward and backward fp32 sweeps (k columns) on the

@@ -83,10 +83,11 @@ _SIGS = {
     "apxb_batch_size": (ctypes.c_int, [c_p, c_p, c_p, c_p]),
     "apxb_batch_solve": (ctypes.c_int, [c_p, c_p, c_p, c_p, ctypes.c_double, ctypes.c_int, ctypes.c_int, c_p]),
     "apxb_batch_admit": (ctypes.c_int, [c_p, ctypes.c_int, c_p, ctypes.c_double, ctypes.c_int, ctypes.c_int]),
-    "apxb_batch_step": (ctypes.c_int, [c_p, ctypes.c_int]),
-    "apxb_batch_query": (ctypes.c_int, [c_p, ctypes.POINTER(ctypes.c_int)]),
-    "apxb_batch_slots": (ctypes.c_int, [c_p, c_p, c_p, c_p, c_p]),
+    "apxb_batch_step": (ctypes.c_int, [c_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]),
+    "apxb_batch_query": (ctypes.c_int, [c_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int)]),
+    "apxb_batch_slots": (ctypes.c_int, [c_p, ctypes.c_int64, c_p, c_p, c_p, c_p]),
     "apxb_batch_retire": (ctypes.c_int, [c_p, ctypes.c_int, c_p, ctypes.c_int]),
+    "apxb_batch_retired": (ctypes.c_int, [c_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "apxb_batch_sweep_timed": (ctypes.c_int, [c_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                               ctypes.POINTER(ctypes.c_double)]),
 }
@@ -373,37 +374,47 @@ class Batch:
         check(self.lib.apxb_batch_solve(self.h, ptr(B), ptr(X), ptr(nrhs), tol, max_iter, flags, res))
         return res
 
-    # -- continuous batching --
+    # -- continuous batching (every call enqueues and returns) --
     def admit(self, slot: int, b, tol: float = 1e-8, max_iter: int = 500, device_ptrs: bool = False):
-        """Load a right-hand side (the slot's instance size, original ordering) into an idle slot."""
-        if not device_ptrs:
+        """Load a right-hand side (the slot's instance size, original ordering)
+        into an idle slot. Pinned host or device memory is read later in stream
+        order: keep it unchanged until the next step has finished."""
+        if not device_ptrs and isinstance(b, np.ndarray):
             b = np.ascontiguousarray(b, np.float64)
             assert b.shape == (self.sizes[slot // self.k],)
         check(self.lib.apxb_batch_admit(self.h, slot, ptr(b), tol, max_iter, DEVICE_PTRS if device_ptrs else 0))
 
-    def step(self, iterations: int = 1):
-        """Enqueue PCG iterations of every live slot (returns without waiting)."""
-        check(self.lib.apxb_batch_step(self.h, iterations))
+    def step(self, iterations: int = 1) -> int:
+        """Enqueue PCG iterations of every live slot; returns the step id."""
+        sid = ctypes.c_int64()
+        check(self.lib.apxb_batch_step(self.h, iterations, ctypes.byref(sid)))
+        return sid.value
 
-    def ready(self) -> bool:
+    def ready(self, step_id: int) -> bool:
         r = ctypes.c_int()
-        check(self.lib.apxb_batch_query(self.h, ctypes.byref(r)))
+        check(self.lib.apxb_batch_query(self.h, step_id, ctypes.byref(r)))
         return bool(r.value)
 
-    def slots(self):
-        """(done, iterations, status, residual) arrays after the last step."""
+    def slots(self, step_id: int):
+        """(done, iterations, status, residual) arrays after step step_id."""
         ns = self.S * self.k
         done, its, st = (np.zeros(ns, np.int32) for _ in range(3))
         res = np.zeros(ns)
-        check(self.lib.apxb_batch_slots(self.h, ptr(done), ptr(its), ptr(st), ptr(res)))
+        check(self.lib.apxb_batch_slots(self.h, step_id, ptr(done), ptr(its), ptr(st), ptr(res)))
         return done.astype(bool), its, st, res
 
     def retire(self, slot: int, x=None, device_ptrs: bool = False):
-        """Solution of a finished slot (original ordering)."""
+        """Enqueue the copy of a finished slot's solution into x (returned);
+        read it once retired(slot) is true."""
         if x is None:
             x = np.empty(self.sizes[slot // self.k])
         check(self.lib.apxb_batch_retire(self.h, slot, ptr(x), DEVICE_PTRS if device_ptrs else 0))
         return x
+
+    def retired(self, slot: int) -> bool:
+        r = ctypes.c_int()
+        check(self.lib.apxb_batch_retired(self.h, slot, ctypes.byref(r)))
+        return bool(r.value)
 
     def sweep_timed(self, reps: int = 10):
         """Seconds per forward and per backward fp32 sweep of this batch (CUDA events)."""

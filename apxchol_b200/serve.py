@@ -58,13 +58,19 @@ class _Resident:
     batch: native.Batch
     n: int
     nbytes: int
+    bbuf: list                     # pinned right-hand-side staging per slot
+    xbuf: list                     # pinned solution staging per slot
     queue: collections.deque = field(default_factory=collections.deque)
-    slots: list = field(default_factory=list)       # Request or None per slot
-    stepping: bool = False
+    slots: list = field(default_factory=list)          # live Request per slot, or None
+    first_step: list = field(default_factory=list)     # first step id whose states show the slot's request
+    inflight: collections.deque = field(default_factory=collections.deque)   # step ids not yet consumed
+    retiring: list = field(default_factory=list)       # (slot, Request) whose x copy is in flight
+    next_step: int = 0
     last_used: float = 0.0
 
     def busy(self) -> bool:
-        return bool(self.queue) or any(s is not None for s in self.slots)
+        return bool(self.queue) or bool(self.retiring) or bool(self.inflight) or \
+            any(s is not None for s in self.slots)
 
     def close(self):
         self.batch.close(); self.op.close(); self.factor.close(); self.eng.close()
@@ -90,9 +96,10 @@ class SolveServer:
     requests at their arrival times while serving."""
 
     def __init__(self, device: int = 0, budget_bytes: int = 60 * 10**9, k: int = 8, iters_per_step: int = 2,
-                 max_iter: int = 500):
+                 max_iter: int = 500, depth: int = 2):
         self.device, self.budget, self.k = device, int(budget_bytes), k
         self.iters_per_step, self.max_iter = iters_per_step, max_iter
+        self.depth = max(1, min(2, depth))      # steps kept queued per matrix (the batch keeps two state copies)
         self.resident: dict = {}
         self.catalog: dict = {}          # mid -> (matrix, factor) that can be (re)admitted
         self.completed: list = []
@@ -119,7 +126,7 @@ class SolveServer:
         mat, fac = self.catalog[mid]
         need = self.estimate(mid)
         while self.used_bytes() + need > self.budget:
-            idle = [r for r in self.resident.values() if not r.busy() and not r.stepping]
+            idle = [r for r in self.resident.values() if not r.busy()]
             if not idle:
                 raise BudgetError(f"matrix {mid!r} needs {need} bytes; {self.used_bytes()} of {self.budget} in use "
                                   "by busy matrices")
@@ -139,15 +146,19 @@ class SolveServer:
             if ex.code == native.ERR_BUDGET:
                 raise BudgetError(str(ex)) from ex
             raise
+        import torch   # pinned host staging (page-locked buffers make the copies asynchronous)
+        bbuf = [torch.empty(mat.n, dtype=torch.float64).pin_memory().numpy() for _ in range(self.k)]
+        xbuf = [torch.empty(mat.n, dtype=torch.float64).pin_memory().numpy() for _ in range(self.k)]
         r = _Resident(mid=mid, eng=eng, factor=f, op=op, batch=bt, n=mat.n, nbytes=max(need, eng.memory_used()),
-                      slots=[None] * self.k, last_used=time.perf_counter())
+                      bbuf=bbuf, xbuf=xbuf, slots=[None] * self.k, first_step=[0] * self.k,
+                      last_used=time.perf_counter())
         self.resident[mid] = r
         self.admissions += 1
         return r
 
     def evict(self, mid):
         r = self.resident[mid]
-        if r.busy() or r.stepping:
+        if r.busy():
             raise RuntimeError("cannot evict a matrix with requests in flight")
         del self.resident[mid]
         r.close()
@@ -164,33 +175,59 @@ class SolveServer:
         r.queue.append(req)
         return req
 
-    def _service(self, r: _Resident) -> bool:
-        """One pass over a resident matrix; returns whether anything happened."""
+    def _deliver(self, r: _Resident, wait: bool = False) -> bool:
+        """Hand over the solutions whose copies have landed."""
         progressed = False
-        if r.stepping:
-            if not r.batch.ready():
-                return False
-            r.stepping = False
-            done, its, st, res = r.batch.slots()
+        keep = []
+        for s, req in r.retiring:
+            if wait or r.batch.retired(s):
+                while not r.batch.retired(s):
+                    time.sleep(20e-6)
+                req.x = r.xbuf[s].copy()
+                req.finish = time.perf_counter()
+                self.completed.append(req)
+                progressed = True
+            else:
+                keep.append((s, req))
+        r.retiring = keep
+        return progressed
+
+    def _service(self, r: _Resident) -> bool:
+        """One non-blocking pass over a resident matrix; returns whether anything happened.
+
+        Steps stay queued on the device (up to `depth`) while the host reads the
+        states of the oldest finished step, retires the slots that finished
+        (their x copies are enqueued behind the queued steps) and admits
+        waiting requests into the freed slots (they join at the next step)."""
+        progressed = self._deliver(r)
+        if r.inflight and r.batch.ready(r.inflight[0]):
+            sid = r.inflight.popleft()
+            progressed = True
+            done, its, st, res = r.batch.slots(sid)
             for s, req in enumerate(r.slots):
-                if req is not None and done[s]:
-                    req.x = r.batch.retire(s)
-                    req.iterations, req.status, req.residual = int(its[s]), int(st[s]), float(res[s])
-                    req.finish = time.perf_counter()
-                    self.completed.append(req)
-                    r.slots[s] = None
-                    progressed = True
+                if req is None or sid < r.first_step[s] or not done[s]:
+                    continue
+                if any(q == s for q, _ in r.retiring):
+                    self._deliver(r, wait=True)           # the slot's previous solution is still in its buffer
+                req.iterations, req.status, req.residual = int(its[s]), int(st[s]), float(res[s])
+                r.batch.retire(s, r.xbuf[s])
+                r.retiring.append((s, req))
+                r.slots[s] = None
         # admit waiting requests into free slots
         for s in range(self.k):
             if r.slots[s] is None and r.queue:
                 req = r.queue.popleft()
                 req.start = time.perf_counter()
-                r.batch.admit(s, req.b, req.tol, self.max_iter)
+                np.copyto(r.bbuf[s], req.b)
+                r.batch.admit(s, r.bbuf[s], req.tol, self.max_iter)
                 r.slots[s] = req
+                r.first_step[s] = r.next_step
                 progressed = True
-        if any(x is not None for x in r.slots):
-            r.batch.step(self.iters_per_step)
-            r.stepping = True
+        # keep the device busy
+        while len(r.inflight) < self.depth and any(x is not None for x in r.slots):
+            sid = r.batch.step(self.iters_per_step)
+            r.next_step = sid + 1
+            r.inflight.append(sid)
             r.last_used = time.perf_counter()
             progressed = True
         return progressed
@@ -203,7 +240,7 @@ class SolveServer:
         return any_progress
 
     def idle(self) -> bool:
-        return not any(r.busy() or r.stepping for r in self.resident.values())
+        return not any(r.busy() for r in self.resident.values())
 
     def drain(self, timeout: float = 600.0):
         t0 = time.perf_counter()

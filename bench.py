@@ -1,19 +1,36 @@
-"""Solve-phase benchmark: PCG solves/s on the 3D 7-point 128^3 high-contrast
-SDDM grid (n = 2,097,152), tol 1e-8, FP64-verified.
+"""Solve-phase benchmark on the 3D 7-point 128^3 high-contrast SDDM grid
+(n = 2,097,152): PCG solves/s and p50/p99 ms at relres 1e-8 (FP64-verified),
+and the SpTRSV sweeps' HBM GB/s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--k K] [--grid G] [--no-serving] [--no-plain] [--no-cpu-baseline]
 
-Our arm: one step = one PCG solve of one N(0,1) right-hand side through the
-GPU-resident path (fp64 sweeps reproducing the reference arithmetic, fp64
-SpMV / vectors). `value` times K device-resident solves with CUDA events on
-the engine stream; `e2e` times the same solves through the public C ABI from
-pinned host memory (b uploaded and x downloaded inside the timed region).
-The roofline is the sweep kernel's: algorithmic bytes per sweep / measured
-sweep time against the measured HBM copy bandwidth. The CPU baseline is the
-reference's own cpu_solver (oracle/_ref) on the host cores, on a bounded
-sample of the same solves.
+Our arm. The headline is the batched mixed-precision form: one step is one
+batched PCG solve of k right-hand sides, with fp32 factor sweeps and fp64
+SpMV, residual, dots and centring. k and the sweep grid are picked by the
+autotuner (apxchol_b200/autotune.py) unless --k is given. Every step solves a
+fresh set of N(0,1) right-hand sides from a pool of distinct sets. The line
+reports:
+  * value      solves/s over K device-resident steps (CUDA events on the
+               engine stream).
+  * e2e        the same solves through the public C ABI (apxb_batch_solve)
+               from pinned host buffers: B uploaded and X downloaded inside the
+               timed region.
+  * plain_fp64 the plain single-RHS fp64 path (apxb_pcg; sweeps reproducing
+               the reference's arithmetic), its solves/s and the speed-up.
+  * serving    an open-loop Poisson request stream through SolveServer
+               (continuous batching) at 70% of the measured capacity, tolerance
+               drawn from {1e-6, 1e-8, 1e-10}: solves/s and p50/p99 latency
+               from arrival to result.
+  * roofline   the fp32 k-RHS sweep kernel: algorithmic bytes per sweep
+               (nnz_s*8 + 4(m+1) + 2*m*4*k) / measured sweep time, against the
+               measured HBM copy bandwidth. iter_frac: the factor + matrix bytes
+               of one PCG iteration (460 MB at 128^3) over the batch's time per
+               iteration.
+  * cpu_baseline  the reference's own cpu_solver (oracle/_ref) on the host cores.
+Inputs exceed L2 (factor + operator > 400 MB per iteration), so no flush is needed.
 
---impl reference: the reference's CPU solve phase alone (rank 0), each step one
+--impl reference: the reference's CPU solve phase (rank 0 only), each step one
 solve of the same system; prints the same JSON line with "impl": "reference".
 
 With torchrun (N > 1) every rank solves its own replica (no collective on the
@@ -35,38 +52,37 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "PCG solves/s (relres 1e-8, FP64-verified)"
-GRID_N = 128
+METRIC = "PCG solves/s and p50/p99 ms at relres 1e-8 (FP64); SpTRSV HBM GB/s"
 TOL = 1e-8
 MAX_ITER = 500
 FACTOR_SEED = 1
 FACTOR_THREADS = 8
+POOL = 4            # distinct right-hand-side sets cycled through the steps
 
 
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
-def build_problem():
+def build_problem(grid_n: int):
     from apxchol_b200 import gen, refsetup
     t0 = time.time()
-    A = gen.grid3d(GRID_N, seed=1)
+    A = gen.grid3d(grid_n, seed=1)
     t1 = time.time()
     F = refsetup.factorize(A, seed=FACTOR_SEED, threads=FACTOR_THREADS)
     t2 = time.time()
-    log(f"[bench] grid3d_{GRID_N}: n={A.n} nnz(A)={A.nnz} gen {t1 - t0:.1f}s; factor nnz={F.nnz} "
+    log(f"[bench] grid3d_{grid_n}: n={A.n} nnz(A)={A.nnz} gen {t1 - t0:.1f}s; factor nnz={F.nnz} "
         f"rounds={len(F.rounds)} factorize {t2 - t1:.1f}s")
     return A, F
 
 
-def workload_config(A, F, info=None):
-    cfg = {"workload": f"grid3d_{GRID_N} 7-point, weights 10^U[-3,3] (seed 1), boundary +1 (SDDM); "
-                       f"plain FP64 PCG, 1 RHS/solve",
+def workload_config(grid_n, A, F, form: str, extra=None):
+    cfg = {"workload": f"grid3d_{grid_n} 7-point, weights 10^U[-3,3] (seed 1), boundary +1 (SDDM); {form}",
            "n": int(A.n), "nnz_A": int(A.nnz), "nnz_factor": int(F.nnz), "tol": TOL, "max_iter": MAX_ITER,
            "factor": f"apxchol factorize seed {FACTOR_SEED}, {FACTOR_THREADS} threads, block_greedy/vec_pool",
-           "l2": "inputs larger than L2 (factor + operator > 400 MB per solve)"}
-    if info is not None:
-        cfg["nnz_stored"] = int(info.nnz_stored)
+           "l2": "inputs larger than L2 (factor + operator > 400 MB per iteration), no flush"}
+    if extra:
+        cfg.update(extra)
     return cfg
 
 
@@ -132,6 +148,26 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
+def max_over_ranks(values, world: int, device):
+    """Element-wise max of a list of floats over all ranks (identity at world 1)."""
+    if world <= 1:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
+def from_rank0(values, world: int, device):
+    """Rank 0's list of floats on every rank (identity at world 1)."""
+    if world <= 1:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    torch.distributed.broadcast(t, src=0)
+    return [float(v) for v in t.cpu()]
+
+
 def cpu_baseline(A, F, b, samples: int = 3):
     """The reference cpu_solver on this host (bounded sample of solves)."""
     import oracle
@@ -147,7 +183,7 @@ def cpu_baseline(A, F, b, samples: int = 3):
         its.append(it)
     med = statistics.median(times)
     return {"value": 1.0 / med, "unit": "solves/s", "cores": cores, "kind": "reference",
-            "sample": f"{samples} solves of the same 128^3 system (median {med * 1e3:.0f} ms, {its[0]} iterations), "
+            "sample": f"{samples} solves of the same system (median {med * 1e3:.0f} ms, {its[0]} iterations), "
                       f"reference cpu_solver OMP_NUM_THREADS={cores}",
             "iterations": int(its[0])}
 
@@ -157,11 +193,11 @@ def run_reference(args, rank, world):
         return 0
     import oracle
     from apxchol_b200 import gen
-    A, F = build_problem()
-    b = gen.rhs(A.n, 1000, False)
     if not oracle.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref missing"}))
         return 0
+    A, F = build_problem(args.grid)
+    b = gen.rhs(A.n, 1000, False)
     cores = os.cpu_count() or 1
     oracle.set_threads(cores)
     R = oracle.Ref(A, F)
@@ -178,7 +214,8 @@ def run_reference(args, rank, world):
     line = {"metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-            "config": workload_config(A, F), "impl": "reference",
+            "config": workload_config(args.grid, A, F, "reference cpu_solver, 1 RHS per solve"),
+            "impl": "reference",
             "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "reference",
                              "sample": f"{args.steps} solves, reference cpu_solver OMP_NUM_THREADS={cores}"},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -187,114 +224,204 @@ def run_reference(args, rank, world):
     return 0
 
 
+def serving_run(A, F, k, iters_per_step, rate, n_req, seed, log_fn):
+    """Open-loop Poisson requests through SolveServer; returns its summary."""
+    from apxchol_b200 import gen
+    from apxchol_b200.serve import SolveServer, latency_stats
+    srv = SolveServer(k=k, iters_per_step=iters_per_step)
+    try:
+        srv.register("g", A, F)
+        srv.admit_matrix("g")
+        pool = [gen.rhs(A.n, 7000 + j, False) for j in range(8)]
+        for j in range(k):                       # warm the graphs
+            srv.submit("g", pool[j % 8], TOL)
+        srv.drain()
+        srv.completed.clear()
+        rng = np.random.default_rng(seed)
+        t = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
+        tols = (1e-6, 1e-8, 1e-10)
+        arrivals = [(float(t[j]), "g", pool[j % 8], tols[int(rng.integers(3))]) for j in range(n_req)]
+        t0 = time.perf_counter()
+        done = srv.run_open_loop(arrivals)
+        wall = time.perf_counter() - t0
+        st = latency_stats(done)
+        bad = sum(1 for q in done if q.status != 0)
+        # fp64 check of a sample of results against the original A
+        worst = 0.0
+        for q in done[:: max(1, len(done) // 16)]:
+            worst = max(worst, float(np.linalg.norm(q.b - A.matvec(q.x)) / np.linalg.norm(q.b)) / q.tol)
+        out = {"rate_req_s": rate, "requests": len(done), "solves_s": len(done) / wall, "p50_ms": st["p50_ms"],
+               "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "k": k, "iters_per_step": iters_per_step,
+               "not_converged": bad, "max_true_relres_over_tol": worst}
+        log_fn(f"[bench] serving {rate:.0f} req/s: {out['solves_s']:.1f} solves/s, p50 {st['p50_ms']:.1f} ms, "
+               f"p99 {st['p99_ms']:.1f} ms, {bad} not converged, worst fp64 relres/tol {worst:.2f}")
+        return out
+    finally:
+        srv.close()
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
-    from apxchol_b200 import gen, native
+    from apxchol_b200 import autotune, gen, native
 
     torch.cuda.set_device(local_rank)
-    A, F = build_problem()
-    b = gen.rhs(A.n, 1000 + rank, False)
+    dev = torch.device("cuda", local_rank)
+    A, F = build_problem(args.grid)
+    n = A.n
     eng = native.Engine(local_rank)
     t0 = time.time()
-    D = native.DeviceFactor(eng, F, precision=native.PREC_FP64)
+    D32 = native.DeviceFactor(eng, F, precision=native.PREC_FP32)
     Op = native.DeviceOperator(eng, A, F.perm)
-    log(f"[bench] upload factor+operator {time.time() - t0:.1f}s; stored nnz {D.info.nnz_stored}; "
-        f"levels {D.info.fwd_levels}; device bytes {D.info.device_bytes / 1e6:.0f} MB")
+    log(f"[bench] upload fp32 factor + operator {time.time() - t0:.1f}s; stored nnz {D32.info.nnz_stored}; "
+        f"levels {D32.info.fwd_levels}")
     stream = torch.cuda.ExternalStream(eng.stream)
-    n = A.n
-    db = torch.from_numpy(b).cuda()
-    dx = torch.empty(n, dtype=torch.float64, device="cuda")
-    hb = torch.from_numpy(b).pin_memory()
-    hx = torch.empty(n, dtype=torch.float64).pin_memory()
+
+    def rhs(j):
+        return gen.rhs(n, 1000 + 100000 * rank + j, False)
+
+    # ---- pick k and the sweep grid ----
+    if args.k:
+        k, grid, tuned = args.k, args.sweep_grid, None
+    else:
+        ch = autotune.tune(eng, D32, Op, rhs, tol=TOL, max_iter=MAX_ITER, log=log if rank == 0 else None)
+        k, grid, tuned = ch.k, ch.grid, ch.table
+    k, grid = (int(v) for v in from_rank0([k, grid], world, dev))   # every replica runs rank 0's choice
+    eng.set_sweep_grid(grid)
+    bt = native.Batch(eng, [D32], [Op], k)
+    eng.set_sweep_grid(0)
+    sets = []
+    for p in range(POOL):
+        Bf, nrhs = bt.pack([np.stack([rhs(p * k + c) for c in range(k)])])
+        sets.append((Bf, torch.from_numpy(Bf).to(dev)))
+    dX = torch.empty_like(sets[0][1])
     torch.cuda.synchronize()
 
-    def solve_dev():
-        _, r = native.pcg(eng, D, Op, db, dx, tol=TOL, max_iter=MAX_ITER, device_ptrs=True, true_residual=False)
-        return r
+    def step_dev(i, flags=native.DEVICE_PTRS):
+        return bt.solve_raw(sets[i % POOL][1], dX, nrhs, tol=TOL, max_iter=MAX_ITER, flags=flags)
 
-    def solve_host():
-        # host pointers (pinned): the library copies b in and x out inside the call
-        r = native.PcgResult()
-        native.check(eng.lib.apxb_pcg(eng.h, D.h, Op.h, hb.data_ptr(), hx.data_ptr(), TOL, MAX_ITER, 0, 0,
-                                      native.ctypes.byref(r)))
-        return r
-
-    for _ in range(max(args.warmup, 3)):
-        r = solve_dev()
-    _, rv = native.pcg(eng, D, Op, db, dx, tol=TOL, max_iter=MAX_ITER, device_ptrs=True, true_residual=True)
-    iters = rv.iterations
-    x_host = dx.cpu().numpy()
-    tres = float(np.linalg.norm(b - A.matvec(x_host)) / np.linalg.norm(b))
-    log(f"[bench] rank {rank}: {iters} iterations, recurrence relres {rv.residual:.2e}, "
-        f"fp64 true relres {tres:.2e} (device {rv.true_residual:.2e}), status {rv.status}")
+    for i in range(args.warmup):
+        step_dev(i)
+    # FP64 verification of every slot of one step, on the device and on the host
+    res = step_dev(0, native.DEVICE_PTRS | native.TRUE_RESIDUAL)
+    its = [res[c].iterations for c in range(k)]
+    dev_tres = max(res[c].true_residual for c in range(k))
+    X0 = dX.cpu().numpy()
+    host_tres = 0.0
+    for c in range(k):
+        bcol, xcol = sets[0][0][c * n:(c + 1) * n], X0[c * n:(c + 1) * n]
+        host_tres = max(host_tres, float(np.linalg.norm(bcol - A.matvec(xcol)) / np.linalg.norm(bcol)))
+    log(f"[bench] rank {rank}: k={k} grid={grid or 'resident'}: iterations {min(its)}-{max(its)}, "
+        f"fp64 true relres max {host_tres:.2e} (device {dev_tres:.2e})")
 
     def barrier():
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
-    # ---- value: device-resident solves ----
+    # ---- value: device-resident batched solves ----
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    iters_timed = []
     with ClockSampler(local_rank) as clk:
         barrier()
         ev0.record(stream)
-        its = []
-        for _ in range(args.steps):
-            its.append(solve_dev().iterations)
+        for i in range(args.steps):
+            r = step_dev(i + 1)
+            iters_timed.append(max(r[c].iterations for c in range(k)))
         ev1.record(stream)
         barrier()
     dev_s = ev0.elapsed_time(ev1) * 1e-3
-    # ---- e2e: host buffers through the C ABI ----
-    for _ in range(2):
-        solve_host()
+    # ---- e2e: pinned host buffers through the C ABI ----
+    hB = [torch.from_numpy(s[0]).pin_memory() for s in sets]
+    hX = torch.empty(n * k, dtype=torch.float64).pin_memory()
+
+    def step_host(i):
+        res_h = (native.PcgResult * (k))()
+        native.check(eng.lib.apxb_batch_solve(bt.h, hB[i % POOL].data_ptr(), hX.data_ptr(), native.ptr(nrhs),
+                                              TOL, MAX_ITER, 0, res_h))
+        return res_h
+
+    step_host(0)
     barrier()
     ev0.record(stream)
-    for _ in range(args.steps):
-        solve_host()
+    for i in range(args.steps):
+        step_host(i + 1)
     ev1.record(stream)
     barrier()
     e2e_s = ev0.elapsed_time(ev1) * 1e-3
-    # ---- roofline: the sweep kernels ----
-    dm = torch.from_numpy(np.random.default_rng(5).standard_normal(D.m)).cuda()
-    dz = torch.empty_like(dm)
-    torch.cuda.synchronize()
-    D.sweep_pair_timed(dm, dz, 3)
-    pair_s = D.sweep_pair_timed(dm, dz, 20)
-    m, nnz_s = D.info.m, D.info.nnz_stored
-    sweep_bytes = nnz_s * 8 + 4 * (m + 1) + 2 * m * 8
-    sweep_s = pair_s / 2
+    # ---- roofline: the batch's own fp32 k-RHS sweeps ----
+    fwd_s, bck_s = bt.sweep_timed(10)
+    m, nnz_s = D32.info.m, D32.info.nnz_stored
+    sweep_bytes = nnz_s * 8 + 4 * (m + 1) + 2 * m * 4 * k
+    sweep_s = (fwd_s + bck_s) / 2
     peak, peak_kind = measured_peak_hbm()
     achieved = sweep_bytes / sweep_s / 1e9
-    # per-iteration algorithmic bytes (factor + matrix), and all traffic
-    b_factor = 2 * (nnz_s * 8 + 4 * (m + 1))
-    b_matrix = A.nnz * 12 + 4 * (n + 1)
-    if world > 1:
-        t = torch.tensor([dev_s, e2e_s], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        dev_s, e2e_s = float(t[0]), float(t[1])
+    b_iter = 2 * (nnz_s * 8 + 4 * (m + 1)) + A.nnz * 12 + 4 * (n + 1)
+    iter_s = dev_s / max(1, sum(iters_timed))
+    iter_gbs = b_iter / iter_s / 1e9
+    dev_s, e2e_s = max_over_ranks([dev_s, e2e_s], world, dev)
+    bt.close()
+
+    # ---- plain fp64 single-RHS path ----
+    plain = None
+    if not args.no_plain:
+        D64 = native.DeviceFactor(eng, F, precision=native.PREC_FP64)
+        db = torch.from_numpy(rhs(0)).to(dev)
+        dx = torch.empty_like(db)
+        for _ in range(3):
+            native.pcg(eng, D64, Op, db, dx, tol=TOL, max_iter=MAX_ITER, device_ptrs=True, true_residual=False)
+        ns = max(3, min(args.steps, 8))
+        secs, pits = [], 0
+        for j in range(ns):
+            _, r = native.pcg(eng, D64, Op, sets[j % POOL][1][:n], dx, tol=TOL, max_iter=MAX_ITER, device_ptrs=True,
+                              true_residual=False)
+            secs.append(r.seconds)
+            pits = r.iterations
+        dm = torch.from_numpy(np.random.default_rng(5).standard_normal(m)).to(dev)
+        dz = torch.empty_like(dm)
+        D64.sweep_pair_timed(dm, dz, 3)
+        pair64 = D64.sweep_pair_timed(dm, dz, 10)
+        b64 = nnz_s * 8 + 4 * (m + 1) + 2 * m * 8
+        plain = {"solves_s": ns / sum(secs), "ms_per_solve": sum(secs) / ns * 1e3, "iterations": pits,
+                 "sweep_us": pair64 / 2 * 1e6, "sweep_gbs": b64 / (pair64 / 2) / 1e9}
+        D64.close()
+        log(f"[bench] plain fp64: {plain['solves_s']:.1f} solves/s ({plain['ms_per_solve']:.1f} ms, {pits} it), "
+            f"fp64 sweep {plain['sweep_us']:.0f} us = {plain['sweep_gbs']:.0f} GB/s")
+
+    value = world * args.steps * k / dev_s
+    serving = None
+    if not args.no_serving and rank == 0:
+        serving = serving_run(A, F, k, args.iters_per_step, 0.7 * value / world, args.serve_requests, 11, log)
+
     if rank != 0:
+        eng.close()
         return 0
-    launches_per_solve = 1 + 5 + 7 * iters + 2
+    mean_its = sum(iters_timed) / max(1, len(iters_timed))
+    launches_per_step = 1 + 12 * (mean_its + 1) + 3
     line = {
-        "metric": METRIC, "value": world * args.steps / dev_s, "unit": "solves/s", "n_gpus": world,
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_s / args.steps * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 sweeps / f64 outer",
         "data": "synthetic (seeded generator, reference factorization)",
-        "config": workload_config(A, F, D.info) | {"parallelism": f"replicas x{world}"},
-        "iterations": iters, "true_relres": tres,
-        "e2e": {"value": world * args.steps / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": 8 * n,
-                "d2h_bytes_per_step": 8 * n + 48},
+        "config": workload_config(args.grid, A, F, f"batched mixed precision, {k} RHS per step",
+                                  {"k": k, "sweep_grid": grid or "resident", "rhs_sets": POOL,
+                                   "parallelism": f"replicas x{world}"}),
+        "iterations": [min(iters_timed), max(iters_timed)], "true_relres_max": host_tres,
+        "e2e": {"value": world * args.steps * k / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": 8 * n * k,
+                "d2h_bytes_per_step": 8 * n * k + 24 * k},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": "k_sweep64 (forward/backward, fp64)",
-                     "bytes_per_launch": sweep_bytes, "sweep_us": sweep_s * 1e6, "peak_kind": peak_kind,
-                     "iter_bytes": b_factor + b_matrix,
-                     "iter_gbs": (b_factor + b_matrix) / (dev_s / args.steps / max(iters, 1)) / 1e9},
-        "gpu_launches": launches_per_solve * args.steps,
+                     "traffic": None, "kernel": f"k_df32<DIR,{k}> (fp32 sweep, {k} RHS)",
+                     "bytes_per_launch": sweep_bytes, "fwd_us": fwd_s * 1e6, "bck_us": bck_s * 1e6,
+                     "peak_kind": peak_kind, "iter_bytes": b_iter, "iter_gbs": iter_gbs, "iter_frac": iter_gbs / peak},
+        "plain_fp64": plain,
+        "speedup_vs_plain_fp64": (value / world) / plain["solves_s"] if plain else None,
+        "serving": serving,
+        "autotune": [{"k": t[0], "grid": t[1] or "resident", "solves_s": t[2]} for t in tuned] if tuned else None,
+        "gpu_launches": int(round(launches_per_step * args.steps)),
         "clocks": clk.summary(),
     }
     if not args.no_cpu_baseline:
         try:
-            line["cpu_baseline"] = cpu_baseline(A, F, b)
+            line["cpu_baseline"] = cpu_baseline(A, F, rhs(0))
         except Exception as ex:   # the baseline is context only
             line["cpu_baseline"] = {"error": str(ex)}
     print(json.dumps(line), flush=True)
@@ -308,6 +435,13 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--grid", type=int, default=128, help="grid side (the workload is 128)")
+    ap.add_argument("--k", type=int, default=0, help="right-hand sides per step (0 = autotune)")
+    ap.add_argument("--sweep-grid", type=int, default=0, help="sweep blocks with --k (0 = resident)")
+    ap.add_argument("--iters-per-step", type=int, default=2, help="serving: iterations per server step")
+    ap.add_argument("--serve-requests", type=int, default=1000)
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

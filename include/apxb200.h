@@ -200,25 +200,37 @@ int apxb_batch_solve(apxb_batch* b, const double* B, double* X, const int* nrhs,
 
 /* ---- continuous batching (the serving form; no counterpart in the reference) ----
  * Slots are admitted and retired one at a time while the other slots keep
- * iterating. Slot s belongs to instance s / k. A new batch has every slot idle.
- *  admit:  load b (instance's n values, original ordering) into an idle slot
- *          with its own tolerance; the slot starts at the next iteration.
- *          max_iter can change only while no slot is live (else APXB_ERR_BUSY).
- *  step:   enqueue `iterations` PCG iterations of every live slot and a copy
- *          of the slot states; returns without waiting.
- *  query:  *ready = 1 once the last step has finished (non-blocking).
- *  slots:  states after the last step (waits for it): done (finished and not
- *          re-admitted), iterations, status (as apxb_pcg_result.status) and
- *          recurrence residual per slot; any pointer may be NULL.
- *  retire: x of a finished slot (original ordering; Laplacian instances
- *          centred); the slot stays idle until admitted again.
- * A slot's arithmetic does not depend on the other slots, so a right-hand
- * side gives the same bits alone and in any mix. */
+ * iterating. Slot s belongs to instance s / k; a new batch has every slot idle.
+ * Every call below only enqueues work on the engine stream, in call order, and
+ * returns without waiting, so the host can keep iterations queued while it
+ * admits and retires slots.
+ *  admit:   load rhs (the instance's n values, original ordering) into an idle
+ *           slot, with its own tolerance; the slot joins at the next iteration
+ *           enqueued after the call. Pageable host memory is staged before the
+ *           call returns; pinned host or device memory is read later, in stream
+ *           order, and must stay unchanged until then. max_iter can change
+ *           only while no slot is admitted (else APXB_ERR_BUSY).
+ *  step:    enqueue `iterations` iterations of every live slot, then a copy of
+ *           the slot states; *step_id names the step.
+ *  query:   *ready = 1 once step step_id has finished (non-blocking).
+ *  slots:   the slot states after step step_id (waits for it): done (finished
+ *           and not re-admitted since), iterations, status (as
+ *           apxb_pcg_result.status) and recurrence residual; any pointer may be
+ *           NULL. The states of a step stay readable until two later steps are
+ *           enqueued (the library keeps two copies).
+ *  retire:  enqueue the copy of a finished slot's x (original ordering;
+ *           Laplacian instances centred) to x; the slot is idle at once and can
+ *           be admitted again (the new right-hand side is ordered after the copy).
+ *  retired: *ready = 1 once the last retire of that slot has written x.
+ * A slot's arithmetic does not depend on the other slots, so a right-hand side
+ * gives the same bits alone and in any mix. apxb_batch_solve refuses while
+ * slots are admitted. */
 int apxb_batch_admit(apxb_batch* b, int slot, const double* rhs, double tol, int max_iter, int flags);
-int apxb_batch_step(apxb_batch* b, int iterations);
-int apxb_batch_query(apxb_batch* b, int* ready);
-int apxb_batch_slots(const apxb_batch* b, int* done, int* iterations, int* status, double* residual);
+int apxb_batch_step(apxb_batch* b, int iterations, int64_t* step_id);
+int apxb_batch_query(apxb_batch* b, int64_t step_id, int* ready);
+int apxb_batch_slots(const apxb_batch* b, int64_t step_id, int* done, int* iterations, int* status, double* residual);
 int apxb_batch_retire(apxb_batch* b, int slot, double* x, int flags);
+int apxb_batch_retired(apxb_batch* b, int slot, int* ready);
 /* Times the batch's forward and backward fp32 sweeps (all k columns) on the
  * right-hand sides of its last iteration: seconds per sweep, mean of reps. */
 int apxb_batch_sweep_timed(apxb_batch* b, int reps, double* fwd_seconds, double* bck_seconds);

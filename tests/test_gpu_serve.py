@@ -111,7 +111,7 @@ def test_budget_admission_and_eviction():
         srv.close()
 
 
-def test_slot_primitives_reject_misuse():
+def test_slot_primitives():
     A, F = problem("grid2d_64")
     eng = native.Engine(0)
     try:
@@ -123,17 +123,23 @@ def test_slot_primitives_reject_misuse():
         b = gen.rhs(A.n, 7, True)
         bt.admit(0, b, 1e-8)
         with pytest.raises(native.ApxbError) as ex:
-            bt.admit(0, b, 1e-8)             # slot 0 is live
+            bt.admit(0, b, 1e-8)             # slot 0 is admitted
         assert ex.value.code == native.ERR_BUSY
-        with pytest.raises(native.ApxbError):
-            bt.retire(0)                     # not finished
+        with pytest.raises(native.ApxbError) as ex:
+            bt.solve([b[None, :]], tol=1e-8)   # a whole-batch solve waits for the slots
+        assert ex.value.code == native.ERR_BUSY
+        sids = []
         for _ in range(200):
-            bt.step(5)
-            done, its, st, res = bt.slots()
+            sids.append(bt.step(5))
+            done, its, st, res = bt.slots(sids[-1])
             if done[0]:
                 break
         assert done[0] and st[0] == 0 and done[1]      # slot 1 was never admitted: idle
+        if len(sids) >= 3:
+            with pytest.raises(native.ApxbError):
+                bt.slots(sids[-3])           # only the last two steps' states are kept
         x = bt.retire(0)
+        assert bt.retired(0)
         xs, _ = bt.solve([b[None, :]], tol=1e-8)
         assert np.array_equal(x, xs[0][0])
         bt.close(); Op.close(); D.close()
