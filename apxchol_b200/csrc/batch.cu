@@ -524,11 +524,13 @@ struct apxb_batch {
     std::vector<uint32_t> off, n;
     std::vector<int> lap;
     std::vector<std::pair<void*, size_t>> owned;
-    // sweep plan per direction (borrowed from a single factor or combined)
+    // batch sweep plan per direction (column lanes for this k; chunked claims)
     uint32_t n_items[2] = {0, 0};
     const uint32_t *info[2] = {nullptr, nullptr}, *ord[2] = {nullptr, nullptr}, *ptr[2] = {nullptr, nullptr};
     const uint32_t* idx[2] = {nullptr, nullptr};
     const float* val[2] = {nullptr, nullptr};
+    const uint32_t* chunk[2] = {nullptr, nullptr};
+    uint32_t n_chunks[2] = {0, 0};
     apxb::sweep_ctl* ctl = nullptr;
     int grid32 = 0;
     // operator (combined, permuted) and permutation
@@ -593,6 +595,14 @@ struct apxb_batch {
         if (h_si) cudaFreeHost(h_si);
     }
     size_t slots() const { return static_cast<size_t>(S) * K; }
+    // plan, buffers and counters of one sweep direction
+    void sweep_dir(int dir, apxb::sweep_args<float>& a) const {
+        a.n_items = n_items[dir]; a.info = info[dir]; a.ord = ord[dir]; a.ptr = ptr[dir];
+        a.idx = idx[dir]; a.val = val[dir]; a.ctl = ctl + dir;
+        a.chunk = chunk[dir]; a.n_chunks = n_chunks[dir];
+        if (dir == 0) { a.in = rhs32; a.out = Yf; a.reset = Zf; }
+        else { a.in = Yf; a.out = Zf; a.reset = Yf; }
+    }
     bp params(int max_iter) const {
         bp P{};
         P.K = K; P.S = S; P.n_tot = n_tot; P.n_tiles = n_tiles;
@@ -617,44 +627,49 @@ struct apxb_batch {
 
 namespace {
 
-// Combined work plan of several factors (fp32 sweeps): the instances' items
-// merged level by level, rows and columns shifted to the combined index space.
-void combine_plans(const std::vector<const apxb_factor*>& fs, const std::vector<uint32_t>& off, int dir,
-                   apxb::sweep_plan& out) {
-    out = apxb::sweep_plan{};
-    // items of each instance are already in level order; merge by level using
-    // the level of each item's first row
+// Batch plan of each direction (host_prep.hpp, build_batch_plan) for the
+// batch's column lanes; several instances: their items merged level by level,
+// rows and columns shifted to the combined index space, then re-chunked.
+void batch_plan(const std::vector<const apxb_factor*>& fs, const std::vector<uint32_t>& off, int dir,
+                uint32_t col_lanes, apxb::sweep_plan& out) {
+    if (fs.size() == 1) {
+        apxb::build_batch_plan(fs[0]->h, dir, col_lanes, out);
+        return;
+    }
+    std::vector<apxb::sweep_plan> pl(fs.size());
     struct src_item { uint32_t inst, item; int32_t level; };
     std::vector<src_item> all;
     for (uint32_t i = 0; i < fs.size(); ++i) {
-        const apxb::sweep_plan& pl = dir == 0 ? fs[i]->h.fwd_plan : fs[i]->h.bck_plan;
-        const std::vector<int32_t>& lev = dir == 0 ? fs[i]->h.fwd_level : fs[i]->h.bck_level;
-        for (uint32_t c = 0; c < pl.n_items; ++c)
-            all.push_back({i, c, lev[pl.ord[static_cast<size_t>(c) * 32]]});
+        apxb::build_batch_plan(fs[i]->h, dir, col_lanes, pl[i]);
+        for (uint32_t c = 0; c < pl[i].n_items; ++c) all.push_back({i, c, pl[i].item_level[c]});
     }
     std::stable_sort(all.begin(), all.end(), [](const src_item& a, const src_item& b) { return a.level < b.level; });
+    out = apxb::sweep_plan{};
     out.n_items = static_cast<uint32_t>(all.size());
     out.info.resize(all.size());
+    out.item_level.resize(all.size());
     out.ord.assign(all.size() * 32, apxb::kNoRow);
     out.ptr.assign(all.size() * 32 + 1, 0);
     uint32_t e = 0;
     for (size_t c = 0; c < all.size(); ++c) {
         const auto& sit = all[c];
-        const apxb::sweep_plan& pl = dir == 0 ? fs[sit.inst]->h.fwd_plan : fs[sit.inst]->h.bck_plan;
-        out.info[c] = pl.info[sit.item] & 0xffffu;   // count | lg (no exact-order flag in fp32)
+        const apxb::sweep_plan& p = pl[sit.inst];
+        out.info[c] = p.info[sit.item];
+        out.item_level[c] = sit.level;
         for (uint32_t s = 0; s < 32; ++s) {
             const size_t sp = static_cast<size_t>(sit.item) * 32 + s, dp = c * 32 + s;
             out.ptr[dp] = e;
-            if (pl.ord[sp] == apxb::kNoRow) continue;
-            out.ord[dp] = pl.ord[sp] + off[sit.inst];
-            for (uint32_t q = pl.ptr[sp]; q < pl.ptr[sp + 1]; ++q) {
-                out.idx.push_back(pl.idx[q] + off[sit.inst]);
-                out.val.push_back(pl.val[q]);
+            if (p.ord[sp] == apxb::kNoRow) continue;
+            out.ord[dp] = p.ord[sp] + off[sit.inst];
+            for (uint32_t q = p.ptr[sp]; q < p.ptr[sp + 1]; ++q) {
+                out.idx.push_back(p.idx[q] + off[sit.inst]);
+                out.val.push_back(p.val[q]);
                 ++e;
             }
         }
     }
     out.ptr[all.size() * 32] = e;
+    apxb::chunk_plan(out);
 }
 
 template <int K>
@@ -669,11 +684,8 @@ int launch_iteration_k(apxb_batch* bt, const bp& P, cudaStream_t s, unsigned lon
     a.k = K; a.err = bt->e->d_err; a.budget_ns = bt->e->budget_ns; a.skip = P.all_done;
     a.m = bt->n_tot;
     for (int dir = 0; dir < 2; ++dir) {
-        a.n_items = bt->n_items[dir]; a.info = bt->info[dir]; a.ord = bt->ord[dir]; a.ptr = bt->ptr[dir];
-        a.idx = bt->idx[dir]; a.val = bt->val[dir]; a.ctl = bt->ctl + dir;
-        if (dir == 0) { a.in = bt->rhs32; a.out = bt->Yf; a.reset = bt->Zf; }
-        else { a.in = bt->Yf; a.out = bt->Zf; a.reset = bt->Yf; }
-        apxb::launch_sweep32(dir, a, bt->grid32, s);
+        bt->sweep_dir(dir, a);
+        apxb::launch_sweep32_batch(dir, a, bt->grid32, s);
     }
     k_b_zsum<K><<<g, kBT, 0, s>>>(P);
     k_b_fin<<<1, kBT, 0, s>>>(P, kFinZsum);
@@ -834,8 +846,6 @@ int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, a
         const apxb_operator* a = ops[i];
         if (!f || !a || f->e != e || a->e != e) return fail(APXB_ERR_INVALID, "instance objects missing or on another engine");
         if (a->n != f->h.n) return fail(APXB_ERR_INVALID, "instance operator / factor dimensions differ");
-        if (n_inst > 1 && (f->h.fwd_plan.seg_rows || f->h.bck_plan.seg_rows))
-            return fail(APXB_ERR_INVALID, "multi-instance batches need factors built without the serial segment");
         bt->off.push_back(bt->n_tot);
         bt->n.push_back(f->h.n);
         bt->lap.push_back(f->h.sddm ? 0 : 1);
@@ -847,40 +857,39 @@ int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, a
     cudaStream_t s = e->stream;
     const size_t nk = static_cast<size_t>(bt->n_tot) * k, ns = bt->slots();
     int rc;
-    // ---- sweep plans ----
-    if (n_inst == 1) {
-        const apxb_factor* f = fs[0];
-        if (f->h.fwd_plan.seg_rows || f->h.bck_plan.seg_rows)
-            return fail(APXB_ERR_INVALID, "batches need a factor built without the serial segment");
-        for (int dir = 0; dir < 2; ++dir) {
-            const apxb::sweep_plan& pl = dir == 0 ? f->h.fwd_plan : f->h.bck_plan;
-            bt->n_items[dir] = pl.n_items;
-            bt->info[dir] = f->info[dir]; bt->ord[dir] = f->ord[dir]; bt->ptr[dir] = f->ptr[dir];
-            bt->idx[dir] = f->idx[dir]; bt->val[dir] = f->val[dir];
-        }
-    } else {
+    // ---- sweep plans (batch plans for this k) ----
+    {
+        const uint32_t col_lanes = k >= 8 ? static_cast<uint32_t>(k / 4) : 1u;
         for (int dir = 0; dir < 2; ++dir) {
             apxb::sweep_plan pl;
-            combine_plans(fs, bt->off, dir, pl);
-            uint32_t *info, *ord, *ptr, *idx;
+            batch_plan(fs, bt->off, dir, col_lanes, pl);
+            if (n_inst == 1) {
+                const std::string bad = apxb::check_batch_plan(fs[0]->h.m, dir == 0 ? fs[0]->h.fwd_level
+                                                                                    : fs[0]->h.bck_level,
+                                                               pl, col_lanes);
+                if (!bad.empty()) return fail(APXB_ERR_INVALID, "internal batch plan error: " + bad);
+            }
+            uint32_t *info, *ord, *ptr, *idx, *chunk;
             float* val;
             if ((rc = bt->dalloc(&info, pl.info.size())) || (rc = bt->dalloc(&ord, pl.ord.size())) ||
                 (rc = bt->dalloc(&ptr, pl.ptr.size())) || (rc = bt->dalloc(&idx, pl.idx.size())) ||
-                (rc = bt->dalloc(&val, pl.val.size())))
+                (rc = bt->dalloc(&val, pl.val.size())) || (rc = bt->dalloc(&chunk, pl.chunk.size())))
                 return rc;
             APXB_CK(cudaMemcpyAsync(info, pl.info.data(), 4 * pl.info.size(), cudaMemcpyHostToDevice, s));
             APXB_CK(cudaMemcpyAsync(ord, pl.ord.data(), 4 * pl.ord.size(), cudaMemcpyHostToDevice, s));
             APXB_CK(cudaMemcpyAsync(ptr, pl.ptr.data(), 4 * pl.ptr.size(), cudaMemcpyHostToDevice, s));
             APXB_CK(cudaMemcpyAsync(idx, pl.idx.data(), 4 * pl.idx.size(), cudaMemcpyHostToDevice, s));
             APXB_CK(cudaMemcpyAsync(val, pl.val.data(), 4 * pl.val.size(), cudaMemcpyHostToDevice, s));
+            APXB_CK(cudaMemcpyAsync(chunk, pl.chunk.data(), 4 * pl.chunk.size(), cudaMemcpyHostToDevice, s));
             APXB_CK(cudaStreamSynchronize(s));
             bt->n_items[dir] = pl.n_items;
             bt->info[dir] = info; bt->ord[dir] = ord; bt->ptr[dir] = ptr; bt->idx[dir] = idx; bt->val[dir] = val;
+            bt->chunk[dir] = chunk; bt->n_chunks[dir] = static_cast<uint32_t>(pl.chunk.size() - 1);
         }
     }
     if ((rc = bt->dalloc(&bt->ctl, 2))) return rc;
     APXB_CK(cudaMemsetAsync(bt->ctl, 0, sizeof(apxb::sweep_ctl) * 2, s));
-    bt->grid32 = e->sweep_grid > 0 ? e->sweep_grid : apxb::sweep_grid32(k, e->num_sms);
+    bt->grid32 = e->sweep_grid > 0 ? e->sweep_grid : apxb::sweep_grid32_batch(k, e->num_sms);
     // ---- operator ----
     if (n_inst == 1) {
         bt->a_ptr = ops[0]->ptr; bt->a_idx = ops[0]->idx; bt->a_val = ops[0]->val;
@@ -1256,11 +1265,8 @@ int apxb_batch_sweep_timed(apxb_batch* bt, int reps, double* fwd_seconds, double
     for (int r = 0; r < reps && rc == APXB_OK; ++r) {
         APXB_CK(cudaEventRecord(ev[0], s));
         for (int dir = 0; dir < 2; ++dir) {
-            a.n_items = bt->n_items[dir]; a.info = bt->info[dir]; a.ord = bt->ord[dir]; a.ptr = bt->ptr[dir];
-            a.idx = bt->idx[dir]; a.val = bt->val[dir]; a.ctl = bt->ctl + dir;
-            if (dir == 0) { a.in = bt->rhs32; a.out = bt->Yf; a.reset = bt->Zf; }
-            else { a.in = bt->Yf; a.out = bt->Zf; a.reset = bt->Yf; }
-            apxb::launch_sweep32(dir, a, bt->grid32, s);
+            bt->sweep_dir(dir, a);
+            apxb::launch_sweep32_batch(dir, a, bt->grid32, s);
             APXB_CK(cudaEventRecord(ev[dir + 1], s));
         }
         APXB_CK(cudaEventSynchronize(ev[2]));

@@ -204,6 +204,128 @@ void level_bits(const std::vector<int32_t>& level, int32_t n_levels, std::vector
 
 }  // namespace
 
+void build_batch_plan(const prepared_factor& h, int dir, uint32_t col_lanes, sweep_plan& plan) {
+    const bool forward = dir == 0;
+    const uint32_t m = h.m;
+    const std::vector<int32_t>& level = forward ? h.fwd_level : h.bck_level;
+    const int32_t n_levels = forward ? h.fwd_levels : h.bck_levels;
+    const std::vector<uint32_t>& ptr = forward ? h.csr_ptr : h.csc_ptr;
+    const std::vector<uint32_t>& idx = forward ? h.csr_idx : h.csc_idx;
+    const std::vector<float>& val = forward ? h.csr_val : h.csc_val;
+    auto width = [&](uint32_t r) {
+        const uint32_t len = ptr[r + 1] - ptr[r] - 1;
+        uint32_t ge = 1;
+        while (ge * col_lanes < 32 && ge * 8 < len) ge *= 2;
+        return ge * col_lanes;
+    };
+    std::vector<std::vector<uint32_t>> by_level(static_cast<size_t>(n_levels));
+    for (uint32_t r = 0; r < m; ++r) by_level[level[r]].push_back(r);
+    plan = sweep_plan{};
+    std::vector<uint32_t> item_rows;
+    item_rows.reserve(m);
+    for (int32_t l = 0; l < n_levels; ++l) {
+        auto& rows = by_level[l];
+        for (uint32_t g = 32; g >= col_lanes && g >= 1; g /= 2) {
+            const uint32_t cap = 32 / g;
+            uint32_t lg = 0;
+            while ((1u << lg) < g) ++lg;
+            uint32_t in_item = 0;
+            for (uint32_t r : rows) {
+                if (width(r) != g) continue;
+                item_rows.push_back(r);
+                if (++in_item == cap) {
+                    plan.info.push_back(in_item | (lg << 8));
+                    plan.item_level.push_back(l);
+                    in_item = 0;
+                }
+            }
+            if (in_item) { plan.info.push_back(in_item | (lg << 8)); plan.item_level.push_back(l); }
+            if (g == 1) break;
+        }
+        std::vector<uint32_t>().swap(rows);
+    }
+    plan.n_items = static_cast<uint32_t>(plan.info.size());
+    const size_t npos = static_cast<size_t>(plan.n_items) * 32;
+    plan.ord.assign(npos, kNoRow);
+    plan.ptr.assign(npos + 1, 0);
+    plan.idx.resize(idx.size());
+    plan.val.resize(val.size());
+    size_t k = 0;
+    uint32_t e = 0;
+    std::vector<std::pair<int32_t, uint32_t>> order;   // (dependency level, position in the row)
+    for (uint32_t c = 0; c < plan.n_items; ++c) {
+        const uint32_t cnt = plan.info[c] & 0xffu;
+        for (uint32_t sl = 0; sl < 32; ++sl) {
+            const size_t pos = static_cast<size_t>(c) * 32 + sl;
+            plan.ptr[pos] = e;
+            if (sl >= cnt) continue;
+            const uint32_t r = item_rows[k++];
+            plan.ord[pos] = r;
+            const uint32_t b = ptr[r], en = ptr[r + 1];
+            const uint32_t d = forward ? en - 1 : b;
+            order.clear();
+            for (uint32_t p = b; p < en; ++p)
+                if (p != d) order.emplace_back(level[idx[p]], p);
+            std::sort(order.begin(), order.end(), [&](const auto& x, const auto& y) {
+                return x.first != y.first ? x.first < y.first : idx[x.second] < idx[y.second];
+            });
+            for (const auto& o : order) { plan.idx[e] = idx[o.second]; plan.val[e] = val[o.second]; ++e; }
+            plan.idx[e] = idx[d]; plan.val[e] = val[d]; ++e;
+        }
+    }
+    plan.ptr[npos] = e;
+    plan.idx.resize(e);
+    plan.val.resize(e);
+    chunk_plan(plan);
+}
+
+void chunk_plan(sweep_plan& p) {
+    p.chunk.clear();
+    uint32_t c = 0;
+    while (c < p.n_items) {
+        uint32_t e = c;
+        while (e < p.n_items && p.item_level[e] == p.item_level[c]) ++e;
+        const uint32_t per = std::max(1u, std::min(8u, (e - c) / 4096u));
+        for (uint32_t s = c; s < e; s += per) p.chunk.push_back(s);
+        c = e;
+    }
+    p.chunk.push_back(p.n_items);
+}
+
+std::string check_batch_plan(uint32_t m, const std::vector<int32_t>& level, const sweep_plan& pl, uint32_t col_lanes) {
+    std::vector<uint8_t> seen(m, 0);
+    int32_t prev = -1;
+    if (pl.item_level.size() != pl.n_items || pl.info.size() != pl.n_items) return "bad batch plan sizes";
+    for (uint32_t c = 0; c < pl.n_items; ++c) {
+        const uint32_t cnt = pl.info[c] & 0xffu, lg = (pl.info[c] >> 8) & 0xffu;
+        if (cnt == 0 || lg > 5 || (1u << lg) < col_lanes || cnt > (32u >> lg)) return "bad batch plan item";
+        for (uint32_t s = 0; s < 32; ++s) {
+            const size_t pos = static_cast<size_t>(c) * 32 + s;
+            const uint32_t r = pl.ord[pos];
+            if (s >= cnt) {
+                if (r != kNoRow || pl.ptr[pos + 1] != pl.ptr[pos]) return "non-empty padding slot";
+                continue;
+            }
+            if (r >= m || seen[r]) return "batch plan lists a row twice or out of range";
+            seen[r] = 1;
+            if (pl.ptr[pos + 1] <= pl.ptr[pos] || pl.idx[pl.ptr[pos + 1] - 1] != r) return "slot diagonal misplaced";
+            if (level[r] != pl.item_level[c]) return "batch plan item level mismatch";
+            for (uint32_t q = pl.ptr[pos]; q + 1 < pl.ptr[pos + 1]; ++q)
+                if (pl.idx[q] >= m || level[pl.idx[q]] >= level[r]) return "batch plan dependency not older";
+        }
+        if (pl.item_level[c] < prev) return "batch plan items out of level order";
+        prev = pl.item_level[c];
+    }
+    for (uint32_t r = 0; r < m; ++r)
+        if (!seen[r]) return "batch plan misses row " + std::to_string(r);
+    if (pl.chunk.empty() || pl.chunk.front() != 0 || pl.chunk.back() != pl.n_items) return "bad chunk table";
+    for (size_t i = 0; i + 1 < pl.chunk.size(); ++i) {
+        const uint32_t lo = pl.chunk[i], hi = pl.chunk[i + 1];
+        if (hi <= lo || hi - lo > 8 || pl.item_level[hi - 1] != pl.item_level[lo]) return "bad chunk";
+    }
+    return {};
+}
+
 std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* rowidx, const float* vals,
                            const uint32_t* perm, bool sddm, const uint64_t* rounds, uint32_t n_rounds,
                            double drop_rel, prepared_factor& out) {

@@ -51,6 +51,8 @@ constexpr double kDropRelDefault = 1e-4;    // kFactorDropRelDefault, factor_dro
 //    (`seg_ptr` per listed row, diagonal last).
 struct sweep_plan {
     uint32_t n_items = 0;
+    std::vector<int32_t> item_level;   // level of each item (host side; batch plans)
+    std::vector<uint32_t> chunk;       // claim units of batch plans: chunk c = items [chunk[c], chunk[c+1])
     std::vector<uint32_t> info;
     std::vector<uint32_t> ord;
     std::vector<uint32_t> ptr;
@@ -96,6 +98,27 @@ inline uint32_t group_width(uint32_t len) {
     while (g < 32 && g * 8 < len) g *= 2;
     return g;
 }
+
+// Work plan of the batched fp32 sweep with k right-hand sides per row (the
+// column-lane kernels). Same item layout as sweep_plan, except:
+//  * a row gets G = C * ge lanes: C column lanes, each holding min(k, 4) of the
+//    k columns (C = k / min(k, 4)), times ge entry lanes (the smallest power
+//    of two with 8 * ge >= off-diagonals, C * ge <= 32), so every lane keeps
+//    up to 8 entries of 16-byte gathers in flight;
+//  * a row's off-diagonals are ordered by the level of the row they depend on,
+//    oldest first (ties by column), then the diagonal: consumed in order, a
+//    row then waits only at its end, on its newest dependencies;
+//  * item_level holds each item's level; chunk (see chunk_plan) the claim units.
+// The fp32 sweep need not follow the reference's sum order (it has a
+// tolerance); this order is fixed, so results stay deterministic.
+void build_batch_plan(const prepared_factor& h, int dir, uint32_t col_lanes, sweep_plan& out);
+// Claim units over a plan's items (in level order): consecutive items of one
+// level, max(1, min(8, items of the level / 4096)) per unit, so large levels
+// take one work-counter claim per several items while every warp stays busy.
+void chunk_plan(sweep_plan& p);
+// Invariants of a batch plan (rows once each, items in level order within one
+// level, G >= col_lanes, diagonal last, chunks cover the items).
+std::string check_batch_plan(uint32_t m, const std::vector<int32_t>& level, const sweep_plan& p, uint32_t col_lanes);
 
 // Returns an empty string on success, else the reason the factor was rejected.
 std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* rowidx, const float* vals,

@@ -46,6 +46,9 @@ struct sweep_args {
     const int* skip;                  // nullable: the launch is a no-op when *skip != 0
     unsigned long long budget_ns;     // spin budget of every wait
     int k;                            // right-hand sides per row (fp32 multi-RHS sweep)
+    // batch plans (host_prep.hpp, build_batch_plan): claim units over the items
+    const uint32_t* chunk;            // chunk c = items [chunk[c], chunk[c + 1])
+    uint32_t n_chunks;
 };
 
 // fp64 sweep reproducing the reference CPU arithmetic (exact sum order).
@@ -54,9 +57,13 @@ void launch_sweep64(int dir, const sweep_args<double>& a, int grid, cudaStream_t
 void launch_sweep32(int dir, const sweep_args<float>& a, int grid, cudaStream_t s);
 // The same with the right-hand side read from fp64 (minus rhs_sub[s] when given).
 void launch_sweep32_from64(int dir, const sweep_args<float>& a, const double* in64, int grid, cudaStream_t s);
+// Batched fp32 sweep over a batch plan (column lanes, chunked claims), k in
+// {1, 2, 4, 8, 16}: a.k, a.chunk and a.n_chunks must be set.
+void launch_sweep32_batch(int dir, const sweep_args<float>& a, int grid, cudaStream_t s);
 // Resident grid (blocks) of the persistent sweeps.
 int sweep_grid64(int num_sms);
 int sweep_grid32(int k, int num_sms);
+int sweep_grid32_batch(int k, int num_sms);
 constexpr int kSweepThreads = 256;
 
 void launch_fill64(double* p, size_t n, double v, cudaStream_t s);

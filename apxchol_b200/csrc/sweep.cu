@@ -218,7 +218,6 @@ __device__ __forceinline__ void load_data64(const sweep_args<double>& a, const s
     if (v.valid && v.u == 0) {
         s.rhs = a.in[v.row];
         s.d = static_cast<double>(__ldg(a.val + v.q + v.len));
-        if (a.reset) a.reset[v.row] = sent_of(0.0);
     }
 }
 
@@ -355,6 +354,10 @@ __device__ __forceinline__ bool run64(const sweep_args<double>& a, stage_data64&
         const double y = __ddiv_rn(__dsub_rn(rhs, total), s.d);
         st_relaxed(a.out + v.row, y);
         if (a.copy_out) a.copy_out[v.row] = y;
+        // re-arm after the right-hand side was consumed: the backward sweep
+        // reads it from the buffer it re-arms (a store issued right behind the
+        // load of the same address would wait for that load)
+        if (a.reset) a.reset[v.row] = sent_of(0.0);
     }
     return true;
 }
@@ -477,12 +480,6 @@ __device__ __forceinline__ void load_data32(const sweep_args<float>& a, const do
             for (int r = 0; r < K; ++r) s.rhs[r] = a.in[base + r];
         }
         s.d = __ldg(a.val + v.q + v.len);
-        if (a.reset) {
-            float sent[K];
-#pragma unroll
-            for (int r = 0; r < K; ++r) sent[r] = sent_of(0.0f);
-            st_row<K>(a.reset + base, sent);
-        }
     }
 }
 
@@ -546,6 +543,12 @@ __device__ __forceinline__ bool run32(const sweep_args<float>& a, stage_data32<K
 #pragma unroll
             for (int r = 0; r < K; ++r) a.copy_out[static_cast<size_t>(v.row) * K + r] = y[r];
         }
+        if (a.reset) {   // re-arm after the right-hand side was consumed (see run64)
+            float sent[K];
+#pragma unroll
+            for (int r = 0; r < K; ++r) sent[r] = sent_of(0.0f);
+            st_row<K>(a.reset + static_cast<size_t>(v.row) * K, sent);
+        }
     }
     return true;
 }
@@ -578,6 +581,193 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_df32(const sweep_args<floa
     leave(a.ctl);
 }
 
+
+// ---------------------------------------------------------------------------
+// Batched fp32 sweep over a batch plan (host_prep.hpp, build_batch_plan).
+// A row's G lanes are C column lanes x ge entry lanes: lane u of the group
+// handles columns [KC * (u % C), KC * (u % C) + KC) and entries t = u / C,
+// u / C + ge, ... of the row (oldest dependency first), 8 at a time, so each
+// gather is one 16-byte load (k >= 4) and a lane keeps 8 of them in flight.
+// Partial sums are combined by a fixed butterfly over the entry lanes. Work is
+// claimed in chunks (consecutive items of one level) from the ticket counter;
+// the next chunk is claimed when the current one starts, so the atomic's
+// latency is hidden behind a chunk of work.
+
+template <int K>
+struct wide_cfg {
+    static constexpr int KC = K < 4 ? K : 4;   // columns per lane
+    static constexpr int C = K / KC;           // column lanes per row
+    static constexpr int LC = C == 4 ? 2 : (C == 2 ? 1 : 0);
+    static constexpr int B = 8;                // entries in flight per lane
+};
+
+template <int K>
+struct stage_wide {
+    lane_view v;
+    unsigned cl, ue, glg;        // column lane, entry lane, log2(entry lanes)
+    float rhs[wide_cfg<K>::KC];
+    float d;
+    uint32_t jj[wide_cfg<K>::B];
+    float ww[wide_cfg<K>::B];
+};
+
+template <int K>
+__device__ __forceinline__ void load_wide(const sweep_args<float>& a, const stage_desc& ds, stage_wide<K>& s) {
+    using W = wide_cfg<K>;
+    s.v = view_of(ds);
+    const lane_view& v = s.v;
+    s.cl = v.u & static_cast<unsigned>(W::C - 1);
+    s.ue = v.u >> W::LC;
+    s.glg = v.lg - W::LC;
+    s.d = 1.0f;
+#pragma unroll
+    for (int r = 0; r < W::KC; ++r) s.rhs[r] = 0.0f;
+    if (v.c >= a.n_items) return;
+#pragma unroll
+    for (int k = 0; k < W::B; ++k) {
+        const uint32_t t = (static_cast<uint32_t>(k) << s.glg) + s.ue;
+        if (t < v.len) { s.jj[k] = __ldg(a.idx + v.q + t); s.ww[k] = __ldg(a.val + v.q + t); }
+    }
+    if (v.valid && s.ue == 0) {
+        const size_t base = static_cast<size_t>(v.row) * K + s.cl * W::KC;
+#pragma unroll
+        for (int r = 0; r < W::KC; ++r) s.rhs[r] = a.in[base + r];
+        s.d = __ldg(a.val + v.q + v.len);
+    }
+}
+
+template <int DIR, int K>
+__device__ __forceinline__ bool run_wide(const sweep_args<float>& a, stage_wide<K>& s) {
+    using W = wide_cfg<K>;
+    constexpr int B = W::B, KC = W::KC;
+    const lane_view& v = s.v;
+    const int where = DIR == 0 ? kFwdSweep32 : kBckSweep32;
+    const uint32_t ge = 1u << s.glg;
+    const uint32_t J = (v.len + ge - 1u) >> s.glg;
+    const uint32_t Jmax = __reduce_max_sync(kFull, J);
+    const size_t col = static_cast<size_t>(s.cl) * KC;
+    float acc[KC];
+#pragma unroll
+    for (int r = 0; r < KC; ++r) acc[r] = 0.0f;
+    idle_clock clk;
+    for (uint32_t jb = 0; jb < Jmax; jb += B) {
+        if (jb > 0) {
+#pragma unroll
+            for (int k = 0; k < B; ++k) {
+                const uint32_t t = ((jb + k) << s.glg) + s.ue;
+                if (t < v.len) { s.jj[k] = __ldg(a.idx + v.q + t); s.ww[k] = __ldg(a.val + v.q + t); }
+            }
+        }
+        const uint32_t t0 = (jb << s.glg) + s.ue;
+        const uint32_t nk = t0 < v.len ? min(static_cast<uint32_t>(B), ((v.len - t0 - 1u) >> s.glg) + 1u) : 0u;
+        float yv[B][KC];
+#pragma unroll
+        for (int k = 0; k < B; ++k)
+            if (static_cast<uint32_t>(k) < nk) ld_row<KC>(a.out + static_cast<size_t>(s.jj[k]) * K + col, yv[k]);
+        uint32_t kpos = 0;
+        for (;;) {
+            const uint32_t before = kpos;
+#pragma unroll
+            for (int k = 0; k < B; ++k) {
+                if (kpos == static_cast<uint32_t>(k) && kpos < nk && row_ready<KC>(yv[k])) {
+#pragma unroll
+                    for (int r = 0; r < KC; ++r) acc[r] = __fmaf_rn(s.ww[k], yv[k][r], acc[r]);
+                    ++kpos;
+                }
+            }
+            if (__all_sync(kFull, kpos >= nk)) break;
+            if (__any_sync(kFull, kpos != before)) clk.spins = 0;
+            else if (clk.idle(a.err, a.budget_ns, where, v.row)) return false;
+            // re-poll only the entry this lane is blocked on and the ones after it
+#pragma unroll
+            for (int k = 0; k < B; ++k)
+                if (static_cast<uint32_t>(k) >= kpos && static_cast<uint32_t>(k) < nk && !row_ready<KC>(yv[k]))
+                    ld_row<KC>(a.out + static_cast<size_t>(s.jj[k]) * K + col, yv[k]);
+        }
+    }
+    // fixed butterfly over the entry lanes (same column lane)
+    for (unsigned o = v.G >> 1; o >= static_cast<unsigned>(W::C); o >>= 1)
+#pragma unroll
+        for (int r = 0; r < KC; ++r) acc[r] += __shfl_xor_sync(kFull, acc[r], static_cast<int>(o), static_cast<int>(v.G));
+    if (v.valid && s.ue == 0) {
+        float y[KC];
+#pragma unroll
+        for (int r = 0; r < KC; ++r) y[r] = __fdiv_rn(s.rhs[r] - acc[r], s.d);
+        st_row<KC>(a.out + static_cast<size_t>(v.row) * K + col, y);
+        // re-arm the row in the buffer the other direction writes next; done
+        // here, after the row's right-hand side has been consumed, since the
+        // backward sweep reads its right-hand side from that same buffer
+        if (a.reset) {
+            float sent[KC];
+#pragma unroll
+            for (int r = 0; r < KC; ++r) sent[r] = sent_of(0.0f);
+            st_row<KC>(a.reset + static_cast<size_t>(v.row) * K + col, sent);
+        }
+    }
+    return true;
+}
+
+// Warp-uniform chunked claim: the items of the current chunk, then those of
+// the pending chunk, whose ticket was taken when the current one began and
+// whose bounds are loaded when the current chunk hands out its last item.
+// A contended same-address atomic takes about (claimers x 0.7 ns), so the
+// ticket is only read a chunk later.
+struct chunk_claim {
+    unsigned cur = 0, end = 0;
+    unsigned pend = 0;            // ticket of the next chunk
+    unsigned plo = 0, phi = 0;    // its bounds (valid when loaded)
+    bool loaded = false;
+    __device__ __forceinline__ void load_pending(const sweep_args<float>& a) {
+        if (!loaded && pend < a.n_chunks) {
+            plo = __ldg(a.chunk + pend);
+            phi = __ldg(a.chunk + pend + 1);
+            loaded = true;
+        }
+    }
+    __device__ __forceinline__ unsigned next(const sweep_args<float>& a) {
+        if (cur >= end) {
+            if (pend >= a.n_chunks) return a.n_items;
+            load_pending(a);
+            cur = plo;
+            end = phi;
+            loaded = false;
+            unsigned t = 0;
+            if ((threadIdx.x & 31u) == 0) t = atomicAdd(&a.ctl->ticket, 1u);
+            pend = __shfl_sync(kFull, t, 0);
+            return cur++;
+        }
+        const unsigned c = cur++;
+        if (cur >= end) load_pending(a);
+        return c;
+    }
+};
+
+template <int DIR, int K>
+__global__ void __launch_bounds__(kSweepThreads, 2) k_dw32(const sweep_args<float> a) {
+    if (a.skip && *a.skip) return;
+    const unsigned lane = threadIdx.x & 31u;
+    chunk_claim cc;
+    {
+        unsigned t = 0;
+        if (lane == 0) t = atomicAdd(&a.ctl->ticket, 1u);
+        cc.pend = __shfl_sync(kFull, t, 0);
+    }
+    stage_desc dD;
+    load_desc(a, cc.next(a), dD);
+    stage_wide<K> sL;
+    load_wide<K>(a, dD, sL);
+    load_desc(a, cc.next(a), dD);
+    int bad = 0;   // the error word, read one item late so the load is never waited on
+    while (sL.v.c < a.n_items) {
+        stage_wide<K> sR = sL;
+        load_wide<K>(a, dD, sL);
+        load_desc(a, cc.next(a), dD);
+        if (__shfl_sync(kFull, bad, 0)) break;
+        if (lane == 0) bad = ld_relaxed_int(&a.err->code);
+        if (!run_wide<DIR, K>(a, sR)) break;
+    }
+    leave(a.ctl);
+}
 
 // ---------------------------------------------------------------------------
 // Serial segment: one block solves the run of small trailing levels (forward:
@@ -633,7 +823,6 @@ __device__ __forceinline__ void seg_fetch64(const sweep_args<double>& a, uint32_
     if ((threadIdx.x & 31u) == 0) {
         s.rhs = a.in[s.r];
         s.d = static_cast<double>(__ldg(a.seg_val + s.q + s.len));
-        if (a.reset) a.reset[s.r] = sent_of(0.0);
     }
 }
 
@@ -660,6 +849,7 @@ __device__ __forceinline__ void seg_solve64(const sweep_args<double>& a, seg_slo
         segv[s.r - a.seg_first] = y;
         a.out[s.r] = y;
         if (a.copy_out) a.copy_out[s.r] = y;
+        if (a.reset) a.reset[s.r] = sent_of(0.0);
     }
 }
 
@@ -726,11 +916,11 @@ __global__ void __launch_bounds__(kSegThreads, 1) k_seg32(const sweep_args<float
                     } else {
                         rhs = a.in[base + c];
                     }
-                    if (a.reset) a.reset[base + c] = sent_of(0.0f);
                     const float y = __fdiv_rn(rhs - acc[c], d);
                     segf[static_cast<size_t>(r - s0) * K + c] = y;
                     a.out[base + c] = y;
                     if (a.copy_out) a.copy_out[base + c] = y;
+                    if (a.reset) a.reset[base + c] = sent_of(0.0f);
                 }
             }
         }
@@ -816,6 +1006,42 @@ int sweep_grid64(int num_sms) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_df64<0>, kSweepThreads, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_df64<1>, kSweepThreads, 0);
     const int b = b0 < b1 ? b0 : b1;
+    return (b > 0 ? b : 1) * num_sms;
+}
+
+template <int K>
+void sweep32_batch_dir(int dir, const sweep_args<float>& a, int grid, cudaStream_t s) {
+    if (!a.n_items) return;
+    if (dir == 0) k_dw32<0, K><<<grid, kSweepThreads, 0, s>>>(a);
+    else          k_dw32<1, K><<<grid, kSweepThreads, 0, s>>>(a);
+}
+
+void launch_sweep32_batch(int dir, const sweep_args<float>& a, int grid, cudaStream_t s) {
+    switch (a.k) {
+        case 1:  sweep32_batch_dir<1>(dir, a, grid, s); break;
+        case 2:  sweep32_batch_dir<2>(dir, a, grid, s); break;
+        case 4:  sweep32_batch_dir<4>(dir, a, grid, s); break;
+        case 8:  sweep32_batch_dir<8>(dir, a, grid, s); break;
+        default: sweep32_batch_dir<16>(dir, a, grid, s); break;
+    }
+}
+
+template <int K>
+int occ32_batch() {
+    int b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_dw32<1, K>, kSweepThreads, 0);
+    return b;
+}
+
+int sweep_grid32_batch(int k, int num_sms) {
+    int b = 1;
+    switch (k) {
+        case 1: b = occ32_batch<1>(); break;
+        case 2: b = occ32_batch<2>(); break;
+        case 4: b = occ32_batch<4>(); break;
+        case 8: b = occ32_batch<8>(); break;
+        default: b = occ32_batch<16>(); break;
+    }
     return (b > 0 ? b : 1) * num_sms;
 }
 
