@@ -181,6 +181,43 @@ __global__ void __launch_bounds__(kBT) k_b_spmv(bp P, const double* X, double* Y
     }
 }
 
+// The same for k >= 2 with the flat pair layout: a row's k columns are held by
+// k/2 consecutive threads, two columns each, so every nonzero's operand row is
+// read as one coalesced k*8-byte access; p.Ap partials through col_store. The
+// row's own p (for p.Ap) is taken from the diagonal's gather when the row
+// stores its diagonal.
+template <int K>
+__global__ void __launch_bounds__(kBT) k_b_spmv_pairs(bp P, const double* X, double* Y, int mode) {
+    if (*P.all_done && mode == 0) return;
+    constexpr unsigned kRows = 2 * kBT / K;      // rows per pass of the block
+    const unsigned c0 = (2 * threadIdx.x) % K, rsub = (2 * threadIdx.x) / K;
+    for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
+        double acc[1][2] = {{0.0, 0.0}};
+        for (unsigned row = P.tile_lo[t] + rsub; row < P.tile_hi[t]; row += kRows) {
+            double a0 = 0.0, a1 = 0.0;
+            double2 own = make_double2(0.0, 0.0);
+            bool have_own = false;
+            const int e = __ldg(P.a_ptr + row + 1);
+#pragma unroll 4
+            for (int k = __ldg(P.a_ptr + row); k < e; ++k) {
+                const double w = __ldg(P.a_val + k);
+                const unsigned col = static_cast<unsigned>(__ldg(P.a_idx + k));
+                const double2 v = *reinterpret_cast<const double2*>(X + static_cast<size_t>(col) * K + c0);
+                a0 = fma(w, v.x, a0);
+                a1 = fma(w, v.y, a1);
+                if (col == row) { own = v; have_own = true; }
+            }
+            *reinterpret_cast<double2*>(Y + static_cast<size_t>(row) * K + c0) = make_double2(a0, a1);
+            if (mode == 0) {
+                if (!have_own) own = *reinterpret_cast<const double2*>(X + static_cast<size_t>(row) * K + c0);
+                acc[0][0] = fma(own.x, a0, acc[0][0]);
+                acc[0][1] = fma(own.y, a1, acc[0][1]);
+            }
+        }
+        if (mode == 0) col_store<K, 1>(acc, P.partials + static_cast<size_t>(t) * K * 2);
+    }
+}
+
 // x += alpha p; r -= alpha Ap (not for fresh or done slots); r.r and sum(r) partials.
 template <int K>
 __global__ void __launch_bounds__(kBT) k_b_xr(bp P) {
@@ -316,6 +353,8 @@ __device__ __forceinline__ void slot_sums(const bp& P, unsigned sl, int nv, doub
     const unsigned lane = threadIdx.x & 31u;
     const unsigned i = sl / P.K, c = sl % P.K;
     s0 = 0.0; s1 = 0.0;
+    // unrolled so the loads overlap; the additions stay in tile order
+#pragma unroll 8
     for (unsigned t = P.inst_t0[i] + lane; t < P.inst_t1[i]; t += 32) {
         const double* src = P.partials + static_cast<size_t>(t) * P.K * 2;
         s0 += src[c];
@@ -675,7 +714,8 @@ void batch_plan(const std::vector<const apxb_factor*>& fs, const std::vector<uin
 template <int K>
 int launch_iteration_k(apxb_batch* bt, const bp& P, cudaStream_t s, unsigned long long h, int use_cond) {
     const int g = bt->e->vec_grid;
-    k_b_spmv<K><<<g, kBT, 0, s>>>(P, P.p, P.Ap, 0);
+    if constexpr (K == 1) k_b_spmv<K><<<g, kBT, 0, s>>>(P, P.p, P.Ap, 0);
+    else k_b_spmv_pairs<K><<<g, kBT, 0, s>>>(P, P.p, P.Ap, 0);
     k_b_fin<<<1, kBT, 0, s>>>(P, kFinSpmv);
     k_b_xr<K><<<g, kBT, 0, s>>>(P);
     k_b_fin<<<1, kBT, 0, s>>>(P, kFinXr);
@@ -714,7 +754,8 @@ void launch_finish_k(apxb_batch* bt, const bp& P, double* X, bool resid, cudaStr
     k_b_xmean<<<1, kBT, 0, s>>>(P);
     k_b_out<K><<<g, kBT, 0, s>>>(P, X);
     if (resid) {
-        k_b_spmv<K><<<g, kBT, 0, s>>>(P, P.x, P.Ap, 1);
+        if constexpr (K == 1) k_b_spmv<K><<<g, kBT, 0, s>>>(P, P.x, P.Ap, 1);
+        else k_b_spmv_pairs<K><<<g, kBT, 0, s>>>(P, P.x, P.Ap, 1);
         k_b_resid<K><<<g, kBT, 0, s>>>(P);
         k_b_fin<<<1, kBT, 0, s>>>(P, kFinResid);
     }
@@ -1089,6 +1130,29 @@ int apxb_batch_solve(apxb_batch* bt, const double* B, double* X, const int* nrhs
         res[sl].residual = bt->h_sd[7 * ns + sl];
         res[sl].true_residual = (flags & APXB_TRUE_RESIDUAL) ? bt->h_sd[12 * ns + sl] : -1.0;
         res[sl].seconds = ms * 1e-3;
+    }
+    return APXB_OK;
+}
+
+// Host-only: the batch plans of one factor for k right-hand sides, built and
+// checked as apxb_batch_create does (no GPU).
+int apxb_batch_plan_host(uint32_t n, const uint32_t* colptr, const uint32_t* rowidx, const float* vals,
+                         const uint32_t* perm, int sddm, const uint64_t* rounds, uint32_t n_rounds, double drop_rel,
+                         int k, uint32_t* n_items, uint32_t* n_chunks) {
+    if (!colptr || !rowidx || !vals || !perm || !n_items || !n_chunks) return fail(APXB_ERR_INVALID, "NULL argument");
+    if (k != 1 && k != 2 && k != 4 && k != 8 && k != 16) return fail(APXB_ERR_INVALID, "k must be 1, 2, 4, 8 or 16");
+    apxb_factor f;
+    const std::string why = apxb::prepare_factor(n, colptr, rowidx, vals, perm, sddm != 0, rounds, n_rounds,
+                                                 drop_rel < 0.0 ? apxb::kDropRelDefault : drop_rel, f.h);
+    if (!why.empty()) return fail(APXB_ERR_BAD_FACTOR, why);
+    const uint32_t col_lanes = k >= 8 ? static_cast<uint32_t>(k / 4) : 1u;
+    for (int dir = 0; dir < 2; ++dir) {
+        apxb::sweep_plan pl;
+        batch_plan({&f}, {0u}, dir, col_lanes, pl);
+        const std::string bad = apxb::check_batch_plan(f.h.m, dir == 0 ? f.h.fwd_level : f.h.bck_level, pl, col_lanes);
+        if (!bad.empty()) return fail(APXB_ERR_INVALID, "batch plan: " + bad);
+        n_items[dir] = pl.n_items;
+        n_chunks[dir] = static_cast<uint32_t>(pl.chunk.size() - 1);
     }
     return APXB_OK;
 }

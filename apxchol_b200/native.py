@@ -79,6 +79,8 @@ _SIGS = {
                                 ctypes.POINTER(PcgResult)]),
     "apxb_test_stalled_sweep": (ctypes.c_int, [c_p, c_p, ctypes.c_uint64]),
     "apxb_batch_create": (ctypes.c_int, [c_p, ctypes.c_int, c_p, c_p, ctypes.c_int, ctypes.POINTER(c_p)]),
+    "apxb_batch_plan_host": (ctypes.c_int, [ctypes.c_uint32, c_p, c_p, c_p, c_p, ctypes.c_int, c_p, ctypes.c_uint32,
+                                            ctypes.c_double, ctypes.c_int, c_p, c_p]),
     "apxb_batch_destroy": (ctypes.c_int, [c_p]),
     "apxb_batch_size": (ctypes.c_int, [c_p, c_p, c_p, c_p]),
     "apxb_batch_solve": (ctypes.c_int, [c_p, c_p, c_p, c_p, ctypes.c_double, ctypes.c_int, ctypes.c_int, c_p]),
@@ -310,6 +312,20 @@ def prepare_host(fac, drop_rel: float = -1.0):
                                                                 "csc_val", "fwd_thin", "bck_thin")]))
     out["m"], out["nnz"], out["levels"] = M, N, (int(lv[0]), int(lv[1]))
     return out
+
+
+def batch_plan_host(fac, k: int, drop_rel: float = -1.0):
+    """Host-only build + check of the batch sweep plans (no GPU): ((items fwd, bck), (chunks fwd, bck))."""
+    lib = load()
+    cp_ = np.ascontiguousarray(fac.colptr, np.uint32)
+    ri = np.ascontiguousarray(fac.rowidx, np.uint32)
+    va = np.ascontiguousarray(fac.vals, np.float32)
+    pe = np.ascontiguousarray(fac.perm, np.uint32)
+    ro = np.ascontiguousarray(fac.rounds, np.uint64)
+    items, chunks = np.zeros(2, np.uint32), np.zeros(2, np.uint32)
+    check(lib.apxb_batch_plan_host(fac.n, ptr(cp_), ptr(ri), ptr(va), ptr(pe), int(fac.sddm),
+                                   ptr(ro) if ro.size else None, ro.size, drop_rel, k, ptr(items), ptr(chunks)))
+    return tuple(int(v) for v in items), tuple(int(v) for v in chunks)
 
 
 class Batch:

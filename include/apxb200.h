@@ -198,6 +198,14 @@ int apxb_batch_size(const apxb_batch* b, int* n_inst, int* k, uint32_t* n_total)
 int apxb_batch_solve(apxb_batch* b, const double* B, double* X, const int* nrhs, double tol, int max_iter,
                      int flags, apxb_pcg_result* res);
 
+/* Host-only (no GPU): builds and checks the batch sweep plans apxb_batch_create
+ * would build for this factor and k (column lanes, oldest-dependency-first
+ * entries, chunked claims); n_items[2] / n_chunks[2] receive their sizes per
+ * direction. */
+int apxb_batch_plan_host(uint32_t n, const uint32_t* colptr, const uint32_t* rowidx, const float* vals,
+                         const uint32_t* perm, int sddm, const uint64_t* rounds, uint32_t n_rounds, double drop_rel,
+                         int k, uint32_t* n_items, uint32_t* n_chunks);
+
 /* ---- continuous batching (the serving form; no counterpart in the reference) ----
  * Slots are admitted and retired one at a time while the other slots keep
  * iterating. Slot s belongs to instance s / k; a new batch has every slot idle.

