@@ -148,6 +148,18 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
+def profiled_traffic(k: int, grid_n: int):
+    """DRAM bytes per launch of the batched sweep from the committed ncu summary
+    for this k and grid (profiles/k_dw32_k{k}_grid3d_{grid}.md), else None."""
+    import re
+    p = os.path.join(ROOT, "profiles", f"k_dw32_k{k}_grid3d_{grid_n}.md")
+    try:
+        m = re.search(r"traffic_bytes_per_launch:\s*([0-9]+)", open(p).read())
+        return (int(m.group(1)), os.path.relpath(p, ROOT)) if m else (None, None)
+    except OSError:
+        return None, None
+
+
 def max_over_ranks(values, world: int, device):
     """Element-wise max of a list of floats over all ranks (identity at world 1)."""
     if world <= 1:
@@ -355,6 +367,7 @@ def run_ours(args, rank, world, local_rank):
     sweep_s = (fwd_s + bck_s) / 2
     peak, peak_kind = measured_peak_hbm()
     achieved = sweep_bytes / sweep_s / 1e9
+    traffic, traffic_src = profiled_traffic(k, args.grid)
     b_iter = 2 * (nnz_s * 8 + 4 * (m + 1)) + A.nnz * 12 + 4 * (n + 1)
     iter_s = dev_s / max(1, sum(iters_timed))
     iter_gbs = b_iter / iter_s / 1e9
@@ -409,7 +422,8 @@ def run_ours(args, rank, world, local_rank):
         "e2e": {"value": world * args.steps * k / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": 8 * n * k,
                 "d2h_bytes_per_step": 8 * n * k + 24 * k},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": f"k_df32<DIR,{k}> (fp32 sweep, {k} RHS)",
+                     "traffic": traffic, "traffic_source": traffic_src,
+                     "kernel": f"k_dw32<DIR,{k}> (batched fp32 sweep, {k} RHS)",
                      "bytes_per_launch": sweep_bytes, "fwd_us": fwd_s * 1e6, "bck_us": bck_s * 1e6,
                      "peak_kind": peak_kind, "iter_bytes": b_iter, "iter_gbs": iter_gbs, "iter_frac": iter_gbs / peak},
         "plain_fp64": plain,
