@@ -48,6 +48,7 @@ struct bp {
     int *iters, *done, *status, *pmode, *center, *fresh;
     unsigned long long* applies;
     int* all_done;
+    int* any_center;           // some live slot centres its next preconditioner input
     int max_iter, stag, center_k;
     double* partials;          // [n_tiles][K][2]
     apxb::dev_error* err;
@@ -187,9 +188,10 @@ __global__ void __launch_bounds__(kBT) k_b_spmv(bp P, const double* X, double* Y
 // row's own p (for p.Ap) is taken from the diagonal's gather when the row
 // stores its diagonal.
 template <int K>
-__global__ void __launch_bounds__(kBT) k_b_spmv_pairs(bp P, const double* X, double* Y, int mode) {
+__global__ void __launch_bounds__(kBT, 4) k_b_spmv_pairs(bp P, const double* X, double* Y, int mode) {
     if (*P.all_done && mode == 0) return;
     constexpr unsigned kRows = 2 * kBT / K;      // rows per pass of the block
+    constexpr int kE = 4;                        // nonzeros whose gathers are in flight together
     const unsigned c0 = (2 * threadIdx.x) % K, rsub = (2 * threadIdx.x) / K;
     for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
         double acc[1][2] = {{0.0, 0.0}};
@@ -198,14 +200,25 @@ __global__ void __launch_bounds__(kBT) k_b_spmv_pairs(bp P, const double* X, dou
             double2 own = make_double2(0.0, 0.0);
             bool have_own = false;
             const int e = __ldg(P.a_ptr + row + 1);
-#pragma unroll 4
-            for (int k = __ldg(P.a_ptr + row); k < e; ++k) {
-                const double w = __ldg(P.a_val + k);
-                const unsigned col = static_cast<unsigned>(__ldg(P.a_idx + k));
-                const double2 v = *reinterpret_cast<const double2*>(X + static_cast<size_t>(col) * K + c0);
-                a0 = fma(w, v.x, a0);
-                a1 = fma(w, v.y, a1);
-                if (col == row) { own = v; have_own = true; }
+            for (int k0 = __ldg(P.a_ptr + row); k0 < e; k0 += kE) {
+                // indices and weights of the next kE nonzeros, then all their gathers, then the fmas
+                // in CSR order
+                unsigned col[kE];
+                double w[kE];
+                double2 v[kE];
+#pragma unroll
+                for (int j = 0; j < kE; ++j)
+                    if (k0 + j < e) { col[j] = static_cast<unsigned>(__ldg(P.a_idx + k0 + j)); w[j] = __ldg(P.a_val + k0 + j); }
+#pragma unroll
+                for (int j = 0; j < kE; ++j)
+                    if (k0 + j < e) v[j] = *reinterpret_cast<const double2*>(X + static_cast<size_t>(col[j]) * K + c0);
+#pragma unroll
+                for (int j = 0; j < kE; ++j)
+                    if (k0 + j < e) {
+                        a0 = fma(w[j], v[j].x, a0);
+                        a1 = fma(w[j], v[j].y, a1);
+                        if (col[j] == row) { own = v[j]; have_own = true; }
+                    }
             }
             *reinterpret_cast<double2*>(Y + static_cast<size_t>(row) * K + c0) = make_double2(a0, a1);
             if (mode == 0) {
@@ -218,7 +231,16 @@ __global__ void __launch_bounds__(kBT) k_b_spmv_pairs(bp P, const double* X, dou
     }
 }
 
-// x += alpha p; r -= alpha Ap (not for fresh or done slots); r.r and sum(r) partials.
+// Whether slot sl's next preconditioner application centres its input (the
+// center-k schedule of kFinXr: application count + 1, or 1 for a fresh slot).
+__device__ __forceinline__ bool centres_next(const bp& P, unsigned i, unsigned sl) {
+    const unsigned long long ap = P.fresh[sl] ? 1ull : P.applies[sl] + 1ull;
+    return P.inst_lap[i] && (ap % static_cast<unsigned long long>(P.center_k)) == 0;
+}
+
+// x += alpha p; r -= alpha Ap (not for fresh or done slots); r.r and sum(r)
+// partials. Slots whose next preconditioner input is not centred get it here,
+// as fp32 r (k_b_prep writes the centred ones).
 template <int K>
 __global__ void __launch_bounds__(kBT) k_b_xr(bp P) {
     if (*P.all_done) return;
@@ -228,6 +250,7 @@ __global__ void __launch_bounds__(kBT) k_b_xr(bp P) {
         const unsigned s0 = i * K + c0, s1 = i * K + c1;
         const double a0 = (P.fresh[s0] || P.done[s0]) ? 0.0 : P.alpha[s0];
         const double a1 = (P.fresh[s1] || P.done[s1]) ? 0.0 : P.alpha[s1];
+        const bool w0 = !centres_next(P, i, s0), w1 = !centres_next(P, i, s1);
         double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
         FLAT_PAIRS(t, {
             if (two) {
@@ -239,12 +262,19 @@ __global__ void __launch_bounds__(kBT) k_b_xr(bp P) {
                 r.x = fma(-a0, ap.x, r.x); r.y = fma(-a1, ap.y, r.y);
                 *reinterpret_cast<double2*>(P.x + q) = x;
                 *reinterpret_cast<double2*>(P.r + q) = r;
+                if (w0 && w1) {
+                    *reinterpret_cast<float2*>(P.rhs32 + q) = make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
+                } else {
+                    if (w0) P.rhs32[q] = static_cast<float>(r.x);
+                    if (w1) P.rhs32[q + 1] = static_cast<float>(r.y);
+                }
                 acc[0][0] = fma(r.x, r.x, acc[0][0]); acc[0][1] = fma(r.y, r.y, acc[0][1]);
                 acc[1][0] += r.x; acc[1][1] += r.y;
             } else {
                 P.x[q] = fma(a0, P.p[q], P.x[q]);
                 const double r = fma(-a0, P.Ap[q], P.r[q]);
                 P.r[q] = r;
+                if (w0) P.rhs32[q] = static_cast<float>(r);
                 acc[0][0] = fma(r, r, acc[0][0]);
                 acc[1][0] += r;
             }
@@ -253,20 +283,24 @@ __global__ void __launch_bounds__(kBT) k_b_xr(bp P) {
     }
 }
 
-// fp32 preconditioner input: r - mean (the center-k input centring).
+// fp32 preconditioner input r - mean of the slots that centre it this
+// application (the center-k input centring); the others got theirs in k_b_xr.
 template <int K>
 __global__ void __launch_bounds__(kBT) k_b_prep(bp P) {
-    if (*P.all_done) return;
+    if (*P.all_done || !*P.any_center) return;
     const int c0 = K == 1 ? 0 : static_cast<int>((2 * threadIdx.x) % K), c1 = K == 1 ? 0 : c0 + 1;
     for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
         const unsigned i = P.tile_inst[t];
-        const double m0 = P.mean[i * K + c0], m1 = P.mean[i * K + c1];
+        const unsigned s0 = i * K + c0, s1 = i * K + c1;
+        const bool w0 = P.center[s0] && !P.done[s0], w1 = P.center[s1] && !P.done[s1];
+        if (!w0 && !w1) continue;
+        const double m0 = P.mean[s0], m1 = P.mean[s1];
         FLAT_PAIRS(t, {
             if (two) {
                 const double2 r = *reinterpret_cast<const double2*>(P.r + q);
-                *reinterpret_cast<float2*>(P.rhs32 + q) = make_float2(static_cast<float>(r.x - m0),
-                                                                       static_cast<float>(r.y - m1));
-            } else {
+                if (w0) P.rhs32[q] = static_cast<float>(r.x - m0);
+                if (w1) P.rhs32[q + 1] = static_cast<float>(r.y - m1);
+            } else if (w0) {
                 P.rhs32[q] = static_cast<float>(P.r[q] - m0);
             }
         })
@@ -367,9 +401,11 @@ __device__ __forceinline__ void slot_sums(const bp& P, unsigned sl, int nv, doub
     }
 }
 
-__global__ void __launch_bounds__(kBT) k_b_fin(bp P, int mode) {
-    __shared__ int any_live;
-    if (threadIdx.x == 0) any_live = 0;
+constexpr int kFinThreads = 1024;   // one warp per slot, up to 32 slots at a time
+
+__global__ void __launch_bounds__(kFinThreads) k_b_fin(bp P, int mode) {
+    __shared__ int any_live, any_cen;
+    if (threadIdx.x == 0) { any_live = 0; any_cen = 0; }
     __syncthreads();
     const unsigned nslots = P.S * P.K;
     const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -450,9 +486,15 @@ __global__ void __launch_bounds__(kBT) k_b_fin(bp P, int mode) {
     __syncthreads();
     if (mode == kFinXr || mode == kFinSpmv) {
         for (unsigned sl = threadIdx.x; sl < nslots; sl += blockDim.x)
-            if (!P.done[sl]) any_live = 1;
+            if (!P.done[sl]) {
+                any_live = 1;
+                if (mode == kFinXr && P.center[sl]) any_cen = 1;
+            }
         __syncthreads();
-        if (threadIdx.x == 0) *P.all_done = any_live ? 0 : 1;
+        if (threadIdx.x == 0) {
+            *P.all_done = any_live ? 0 : 1;
+            if (mode == kFinXr) *P.any_center = any_cen;
+        }
     }
 }
 
@@ -588,7 +630,7 @@ struct apxb_batch {
     float *rhs32 = nullptr, *Yf = nullptr, *Zf = nullptr;
     bool y_armed = false;
     double* sd = nullptr;   // kSd double arrays of S*K
-    int* si = nullptr;      // 6 int arrays of S*K + all_done
+    int* si = nullptr;      // 6 int arrays of S*K, all_done, any_center
     unsigned long long* applies = nullptr;
     double* partials = nullptr;
     double* d_B = nullptr;  // staging of right-hand sides / solutions in the caller layout
@@ -656,7 +698,7 @@ struct apxb_batch {
         P.xmean = d + 11 * ns; P.tres = d + 12 * ns; P.tol = d + 13 * ns;
         int* s = si;
         P.iters = s; P.done = s + ns; P.status = s + 2 * ns; P.pmode = s + 3 * ns; P.center = s + 4 * ns;
-        P.fresh = s + 5 * ns; P.all_done = s + 6 * ns;
+        P.fresh = s + 5 * ns; P.all_done = s + 6 * ns; P.any_center = s + 6 * ns + 1;
         P.applies = applies;
         P.max_iter = max_iter; P.stag = 50; P.center_k = e->center_k;
         P.partials = partials; P.err = e->d_err;
@@ -716,9 +758,9 @@ int launch_iteration_k(apxb_batch* bt, const bp& P, cudaStream_t s, unsigned lon
     const int g = bt->e->vec_grid;
     if constexpr (K == 1) k_b_spmv<K><<<g, kBT, 0, s>>>(P, P.p, P.Ap, 0);
     else k_b_spmv_pairs<K><<<g, kBT, 0, s>>>(P, P.p, P.Ap, 0);
-    k_b_fin<<<1, kBT, 0, s>>>(P, kFinSpmv);
+    k_b_fin<<<1, kFinThreads, 0, s>>>(P, kFinSpmv);
     k_b_xr<K><<<g, kBT, 0, s>>>(P);
-    k_b_fin<<<1, kBT, 0, s>>>(P, kFinXr);
+    k_b_fin<<<1, kFinThreads, 0, s>>>(P, kFinXr);
     k_b_prep<K><<<g, kBT, 0, s>>>(P);
     apxb::sweep_args<float> a{};
     a.k = K; a.err = bt->e->d_err; a.budget_ns = bt->e->budget_ns; a.skip = P.all_done;
@@ -728,9 +770,9 @@ int launch_iteration_k(apxb_batch* bt, const bp& P, cudaStream_t s, unsigned lon
         apxb::launch_sweep32_batch(dir, a, bt->grid32, s);
     }
     k_b_zsum<K><<<g, kBT, 0, s>>>(P);
-    k_b_fin<<<1, kBT, 0, s>>>(P, kFinZsum);
+    k_b_fin<<<1, kFinThreads, 0, s>>>(P, kFinZsum);
     k_b_rz<K><<<g, kBT, 0, s>>>(P);
-    k_b_fin<<<1, kBT, 0, s>>>(P, kFinRz);
+    k_b_fin<<<1, kFinThreads, 0, s>>>(P, kFinRz);
     k_b_up<K><<<g, kBT, 0, s>>>(P, h, use_cond);
     const cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return fail(APXB_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(err));
@@ -757,7 +799,7 @@ void launch_finish_k(apxb_batch* bt, const bp& P, double* X, bool resid, cudaStr
         if constexpr (K == 1) k_b_spmv<K><<<g, kBT, 0, s>>>(P, P.x, P.Ap, 1);
         else k_b_spmv_pairs<K><<<g, kBT, 0, s>>>(P, P.x, P.Ap, 1);
         k_b_resid<K><<<g, kBT, 0, s>>>(P);
-        k_b_fin<<<1, kBT, 0, s>>>(P, kFinResid);
+        k_b_fin<<<1, kFinThreads, 0, s>>>(P, kFinResid);
     }
 }
 
@@ -993,7 +1035,7 @@ int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, a
     if ((rc = bt->dalloc(&bt->x, nk)) || (rc = bt->dalloc(&bt->r, nk)) || (rc = bt->dalloc(&bt->p, nk)) ||
         (rc = bt->dalloc(&bt->Ap, nk)) || (rc = bt->dalloc(&bt->b, nk)) || (rc = bt->dalloc(&bt->rhs32, nk)) ||
         (rc = bt->dalloc(&bt->Yf, nk)) || (rc = bt->dalloc(&bt->Zf, nk)) || (rc = bt->dalloc(&bt->sd, kSd * ns)) ||
-        (rc = bt->dalloc(&bt->si, 6 * ns + 1)) || (rc = bt->dalloc(&bt->applies, ns)) ||
+        (rc = bt->dalloc(&bt->si, 6 * ns + 2)) || (rc = bt->dalloc(&bt->applies, ns)) ||
         (rc = bt->dalloc(&bt->partials, static_cast<size_t>(bt->n_tiles) * k * 2)) || (rc = bt->dalloc(&bt->d_B, nk)))
         return rc;
     APXB_CK(cudaMallocHost(&bt->h_sd, sizeof(double) * kSd * ns));
@@ -1002,7 +1044,7 @@ int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, a
     std::fill(bt->h_si, bt->h_si + 6 * ns + 1, 0);
     std::fill(bt->h_si + ns, bt->h_si + 2 * ns, 1);   // host mirror of the idle state below
     APXB_CK(cudaMemsetAsync(bt->sd, 0, sizeof(double) * kSd * ns, s));
-    APXB_CK(cudaMemsetAsync(bt->si, 0, sizeof(int) * (6 * ns + 1), s));
+    APXB_CK(cudaMemsetAsync(bt->si, 0, sizeof(int) * (6 * ns + 2), s));
     {   // every slot starts idle: done, and the batch all done
         std::vector<int> idle(ns + 1, 1);
         APXB_CK(cudaMemcpyAsync(bt->si + ns, idle.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, s));
