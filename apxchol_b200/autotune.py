@@ -79,3 +79,34 @@ def tune(eng: native.Engine, factor: native.DeviceFactor, op: native.DeviceOpera
         eng.set_sweep_grid(0)
     best.table = table
     return best
+
+
+def tune_lanes(mat, fac, rhs, k: int, lanes_list=(2, 3, 4), tol: float = 1e-8, max_iter: int = 500,
+               device: int = 0, log=None):
+    """Solves/s of `lanes` concurrent k-slot batches (apxchol_b200.lanes), for
+    each lane count; returns [(lanes, grid, solves/s, iterations)]."""
+    import time
+    import torch
+    from .lanes import Lanes
+    table = []
+    for nl in lanes_list:
+        ln = Lanes(mat, fac, k, lanes=nl, device=device)
+        try:
+            B, nrhs = ln.pack(np.stack([rhs(c) for c in range(k)]))
+            dB = [torch.from_numpy(B).cuda(device) for _ in range(nl)]
+            dX = [torch.empty_like(b) for b in dB]
+            res = ln.solve_raw(dB, dX, nrhs, tol=tol, max_iter=max_iter, flags=native.DEVICE_PTRS)   # warm-up
+            torch.cuda.synchronize(device)
+            t0 = time.perf_counter()
+            res = ln.solve_raw(dB, dX, nrhs, tol=tol, max_iter=max_iter, flags=native.DEVICE_PTRS)
+            torch.cuda.synchronize(device)
+            dt = time.perf_counter() - t0
+            its = max(r.iterations for lane in res for r in lane[:k])
+            table.append((nl, ln.grid, nl * k / dt, its))
+            if log:
+                log(f"[autotune] lanes={nl} k={k} grid={ln.grid}: {dt * 1e3:8.2f} ms per round, "
+                    f"{nl * k / dt:8.1f} solves/s")
+        finally:
+            ln.close()
+            del ln
+    return table

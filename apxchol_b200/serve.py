@@ -18,6 +18,7 @@ its cpu_solver::solve (src/solve.cpp:478-654) with the request's tolerance.
 from __future__ import annotations
 
 import collections
+import concurrent.futures
 import time
 from dataclasses import dataclass, field
 
@@ -50,30 +51,47 @@ class Request:
 
 
 @dataclass
-class _Resident:
-    mid: object
+class _Lane:
+    """One k-slot batch of a resident matrix on its own engine (CUDA stream)."""
     eng: native.Engine
     factor: native.DeviceFactor
     op: native.DeviceOperator
     batch: native.Batch
-    n: int
-    nbytes: int
     bbuf: list                     # pinned right-hand-side staging per slot
     xbuf: list                     # pinned solution staging per slot
-    queue: collections.deque = field(default_factory=collections.deque)
-    slots: list = field(default_factory=list)          # live Request per slot, or None
-    first_step: list = field(default_factory=list)     # first step id whose states show the slot's request
+    slots: list                    # live Request per slot, or None
+    first_step: list               # first step id whose states show the slot's request
+    staging: list = field(default_factory=list)        # (Request, future of its b copy) per slot, or None
     inflight: collections.deque = field(default_factory=collections.deque)   # step ids not yet consumed
-    retiring: list = field(default_factory=list)       # (slot, Request) whose x copy is in flight
+    retiring: list = field(default_factory=list)       # [slot, Request, future of the x copy or None]
     next_step: int = 0
-    last_used: float = 0.0
+
+    def free(self, s: int) -> bool:
+        return self.slots[s] is None and self.staging[s] is None
 
     def busy(self) -> bool:
-        return bool(self.queue) or bool(self.retiring) or bool(self.inflight) or \
-            any(s is not None for s in self.slots)
+        return bool(self.retiring) or bool(self.inflight) or any(s is not None for s in self.slots) or \
+            any(s is not None for s in self.staging)
 
     def close(self):
         self.batch.close(); self.op.close(); self.factor.close(); self.eng.close()
+
+
+@dataclass
+class _Resident:
+    mid: object
+    n: int
+    nbytes: int
+    lanes: list
+    queue: collections.deque = field(default_factory=collections.deque)
+    last_used: float = 0.0
+
+    def busy(self) -> bool:
+        return bool(self.queue) or any(ln.busy() for ln in self.lanes)
+
+    def close(self):
+        for ln in self.lanes:
+            ln.close()
 
 
 def estimate_bytes(n: int, nnz_factor: int, nnz_a: int, k: int) -> int:
@@ -96,8 +114,12 @@ class SolveServer:
     requests at their arrival times while serving."""
 
     def __init__(self, device: int = 0, budget_bytes: int = 60 * 10**9, k: int = 8, iters_per_step: int = 2,
-                 max_iter: int = 500, depth: int = 2):
+                 max_iter: int = 500, depth: int = 2, lanes: int = 1, sweep_grid: int = 0, copy_threads: int = 4):
         self.device, self.budget, self.k = device, int(budget_bytes), k
+        self.n_lanes, self.sweep_grid = max(1, lanes), sweep_grid   # batches (streams) per matrix, their sweep grid
+        # host copies of right-hand sides into pinned staging and of solutions out of it run on
+        # worker threads (numpy releases the GIL for bulk copies), off the pump loop
+        self.pool = concurrent.futures.ThreadPoolExecutor(copy_threads) if copy_threads > 0 else None
         self.iters_per_step, self.max_iter = iters_per_step, max_iter
         self.depth = max(1, min(2, depth))      # steps kept queued per matrix (the batch keeps two state copies)
         self.resident: dict = {}
@@ -114,7 +136,7 @@ class SolveServer:
 
     def estimate(self, mid) -> int:
         mat, fac = self.catalog[mid]
-        return estimate_bytes(mat.n, fac.nnz, mat.nnz, self.k)
+        return self.n_lanes * estimate_bytes(mat.n, fac.nnz, mat.nnz, self.k)
 
     def used_bytes(self) -> int:
         """Bytes reserved by resident matrices (each: the larger of its estimate and its measured use)."""
@@ -132,8 +154,30 @@ class SolveServer:
                                   "by busy matrices")
             victim = min(idle, key=lambda r: r.last_used)
             self.evict(victim.mid)
+        import torch   # pinned host staging (page-locked buffers make the copies asynchronous)
+        grid = self.sweep_grid
+        if grid <= 0 and self.n_lanes > 1:
+            grid = max(1, 2 * torch.cuda.get_device_properties(self.device).multi_processor_count // self.n_lanes)
+        lanes = []
+        try:
+            for _ in range(self.n_lanes):
+                lanes.append(self._make_lane(mat, fac, grid, self.budget - self.used_bytes()
+                                             - sum(ln.eng.memory_used() for ln in lanes)))
+        except Exception:
+            for ln in lanes:
+                ln.close()
+            raise
+        used = sum(ln.eng.memory_used() for ln in lanes)
+        r = _Resident(mid=mid, n=mat.n, nbytes=max(need, used), lanes=lanes, last_used=time.perf_counter())
+        self.resident[mid] = r
+        self.admissions += 1
+        return r
+
+    def _make_lane(self, mat, fac, grid: int, budget: int) -> _Lane:
+        import torch
         eng = native.Engine(self.device)
-        eng.set_memory_budget(self.budget - self.used_bytes())   # the engine refuses what would overrun the budget
+        eng.set_memory_budget(max(1, budget))   # the engine refuses what would overrun the budget
+        eng.set_sweep_grid(grid)
         f = op = None
         try:
             f = native.DeviceFactor(eng, fac, precision=native.PREC_FP32)
@@ -146,15 +190,11 @@ class SolveServer:
             if ex.code == native.ERR_BUDGET:
                 raise BudgetError(str(ex)) from ex
             raise
-        import torch   # pinned host staging (page-locked buffers make the copies asynchronous)
+        eng.set_sweep_grid(0)
         bbuf = [torch.empty(mat.n, dtype=torch.float64).pin_memory().numpy() for _ in range(self.k)]
         xbuf = [torch.empty(mat.n, dtype=torch.float64).pin_memory().numpy() for _ in range(self.k)]
-        r = _Resident(mid=mid, eng=eng, factor=f, op=op, batch=bt, n=mat.n, nbytes=max(need, eng.memory_used()),
-                      bbuf=bbuf, xbuf=xbuf, slots=[None] * self.k, first_step=[0] * self.k,
-                      last_used=time.perf_counter())
-        self.resident[mid] = r
-        self.admissions += 1
-        return r
+        return _Lane(eng=eng, factor=f, op=op, batch=bt, bbuf=bbuf, xbuf=xbuf, slots=[None] * self.k,
+                     first_step=[0] * self.k, staging=[None] * self.k)
 
     def evict(self, mid):
         r = self.resident[mid]
@@ -175,61 +215,92 @@ class SolveServer:
         r.queue.append(req)
         return req
 
-    def _deliver(self, r: _Resident, wait: bool = False) -> bool:
-        """Hand over the solutions whose copies have landed."""
+    def _run(self, fn, *args):
+        if self.pool is None:
+            f = concurrent.futures.Future()
+            f.set_result(fn(*args))
+            return f
+        return self.pool.submit(fn, *args)
+
+    @staticmethod
+    def _copy_out(req, buf):
+        req.x = buf.copy()
+        req.finish = time.perf_counter()
+
+    def _deliver(self, ln: _Lane, wait: bool = False) -> bool:
+        """Start the host copy of every solution whose device copy has landed,
+        and hand over the requests whose host copy is done."""
         progressed = False
         keep = []
-        for s, req in r.retiring:
-            if wait or r.batch.retired(s):
-                while not r.batch.retired(s):
+        for ent in ln.retiring:
+            s, req, fut = ent
+            if fut is None and (wait or ln.batch.retired(s)):
+                while not ln.batch.retired(s):
                     time.sleep(20e-6)
-                req.x = r.xbuf[s].copy()
-                req.finish = time.perf_counter()
+                fut = ent[2] = self._run(self._copy_out, req, ln.xbuf[s])
+            if fut is not None and (wait or fut.done()):
+                fut.result()
                 self.completed.append(req)
                 progressed = True
             else:
-                keep.append((s, req))
-        r.retiring = keep
+                keep.append(ent)
+        ln.retiring = keep
         return progressed
 
     def _service(self, r: _Resident) -> bool:
         """One non-blocking pass over a resident matrix; returns whether anything happened.
 
-        Steps stay queued on the device (up to `depth`) while the host reads the
-        states of the oldest finished step, retires the slots that finished
-        (their x copies are enqueued behind the queued steps) and admits
-        waiting requests into the freed slots (they join at the next step)."""
-        progressed = self._deliver(r)
-        if r.inflight and r.batch.ready(r.inflight[0]):
-            sid = r.inflight.popleft()
-            progressed = True
-            done, its, st, res = r.batch.slots(sid)
-            for s, req in enumerate(r.slots):
-                if req is None or sid < r.first_step[s] or not done[s]:
-                    continue
-                if any(q == s for q, _ in r.retiring):
-                    self._deliver(r, wait=True)           # the slot's previous solution is still in its buffer
-                req.iterations, req.status, req.residual = int(its[s]), int(st[s]), float(res[s])
-                r.batch.retire(s, r.xbuf[s])
-                r.retiring.append((s, req))
-                r.slots[s] = None
-        # admit waiting requests into free slots
-        for s in range(self.k):
-            if r.slots[s] is None and r.queue:
-                req = r.queue.popleft()
-                req.start = time.perf_counter()
-                np.copyto(r.bbuf[s], req.b)
-                r.batch.admit(s, r.bbuf[s], req.tol, self.max_iter)
-                r.slots[s] = req
-                r.first_step[s] = r.next_step
+        In every lane, steps stay queued on the device (up to `depth`) while
+        the host reads the states of the oldest finished step, retires the slots
+        that finished (their x copies are enqueued behind the queued steps) and
+        admits waiting requests into the freed slots (they join at the next
+        step once their right-hand side is staged). Waiting requests go to the
+        lane with the most free slots."""
+        progressed = False
+        for ln in r.lanes:
+            progressed |= self._deliver(ln)
+            if ln.inflight and ln.batch.ready(ln.inflight[0]):
+                sid = ln.inflight.popleft()
                 progressed = True
-        # keep the device busy
-        while len(r.inflight) < self.depth and any(x is not None for x in r.slots):
-            sid = r.batch.step(self.iters_per_step)
-            r.next_step = sid + 1
-            r.inflight.append(sid)
-            r.last_used = time.perf_counter()
+                done, its, st, res = ln.batch.slots(sid)
+                for s, req in enumerate(ln.slots):
+                    if req is None or sid < ln.first_step[s] or not done[s]:
+                        continue
+                    if any(e[0] == s for e in ln.retiring):
+                        self._deliver(ln, wait=True)       # the slot's previous solution is still in its buffer
+                    req.iterations, req.status, req.residual = int(its[s]), int(st[s]), float(res[s])
+                    ln.batch.retire(s, ln.xbuf[s])
+                    ln.retiring.append([s, req, None])
+                    ln.slots[s] = None
+            # staged right-hand sides join the batch
+            for s in range(self.k):
+                stg = ln.staging[s]
+                if stg is not None and stg[1].done():
+                    stg[1].result()
+                    req = stg[0]
+                    ln.batch.admit(s, ln.bbuf[s], req.tol, self.max_iter)
+                    ln.slots[s] = req
+                    ln.first_step[s] = ln.next_step
+                    ln.staging[s] = None
+                    progressed = True
+        while r.queue:
+            ln = max(r.lanes, key=lambda x: sum(1 for q in range(self.k) if x.free(q)))
+            free = [s for s in range(self.k) if ln.free(s)]
+            if not free:
+                break
+            s = free[0]
+            req = r.queue.popleft()
+            req.start = time.perf_counter()
+            ln.staging[s] = (req, self._run(np.copyto, ln.bbuf[s], req.b))
             progressed = True
+        # keep the device busy
+        for ln in r.lanes:
+            while len(ln.inflight) < self.depth and any(x is not None for x in ln.slots):
+                sid = ln.batch.step(self.iters_per_step)
+                ln.next_step = sid + 1
+                ln.inflight.append(sid)
+                r.last_used = time.perf_counter()
+                progressed = True
         return progressed
 
     def pump(self) -> bool:
@@ -270,6 +341,9 @@ class SolveServer:
     def close(self):
         for mid in list(self.resident):
             self.resident.pop(mid).close()
+        if self.pool is not None:
+            self.pool.shutdown(wait=True)
+            self.pool = None
 
 
 def latency_stats(reqs):

@@ -236,16 +236,16 @@ def run_reference(args, rank, world):
     return 0
 
 
-def serving_run(A, F, k, iters_per_step, rate, n_req, seed, log_fn):
+def serving_run(A, F, k, nlanes, grid, iters_per_step, rate, n_req, seed, log_fn):
     """Open-loop Poisson requests through SolveServer; returns its summary."""
     from apxchol_b200 import gen
     from apxchol_b200.serve import SolveServer, latency_stats
-    srv = SolveServer(k=k, iters_per_step=iters_per_step)
+    srv = SolveServer(k=k, iters_per_step=iters_per_step, lanes=nlanes, sweep_grid=grid)
     try:
         srv.register("g", A, F)
         srv.admit_matrix("g")
         pool = [gen.rhs(A.n, 7000 + j, False) for j in range(8)]
-        for j in range(k):                       # warm the graphs
+        for j in range(k * nlanes):              # warm the graphs
             srv.submit("g", pool[j % 8], TOL)
         srv.drain()
         srv.completed.clear()
@@ -264,7 +264,7 @@ def serving_run(A, F, k, iters_per_step, rate, n_req, seed, log_fn):
             worst = max(worst, float(np.linalg.norm(q.b - A.matvec(q.x)) / np.linalg.norm(q.b)) / q.tol)
         out = {"rate_req_s": rate, "requests": len(done), "solves_s": len(done) / wall, "p50_ms": st["p50_ms"],
                "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "k": k, "iters_per_step": iters_per_step,
-               "not_converged": bad, "max_true_relres_over_tol": worst}
+               "lanes": nlanes, "not_converged": bad, "max_true_relres_over_tol": worst}
         log_fn(f"[bench] serving {rate:.0f} req/s: {out['solves_s']:.1f} solves/s, p50 {st['p50_ms']:.1f} ms, "
                f"p99 {st['p99_ms']:.1f} ms, {bad} not converged, worst fp64 relres/tol {worst:.2f}")
         return out
@@ -275,6 +275,7 @@ def serving_run(A, F, k, iters_per_step, rate, n_req, seed, log_fn):
 def run_ours(args, rank, world, local_rank):
     import torch
     from apxchol_b200 import autotune, gen, native
+    from apxchol_b200.lanes import Lanes
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
@@ -291,38 +292,51 @@ def run_ours(args, rank, world, local_rank):
     def rhs(j):
         return gen.rhs(n, 1000 + 100000 * rank + j, False)
 
-    # ---- pick k and the sweep grid ----
+    # ---- pick k, the sweep grid and the lane count ----
+    tuned = None
     if args.k:
-        k, grid, tuned = args.k, args.sweep_grid, None
+        k, grid, nlanes = args.k, args.sweep_grid, max(1, args.lanes)
     else:
-        ch = autotune.tune(eng, D32, Op, rhs, tol=TOL, max_iter=MAX_ITER, log=log if rank == 0 else None)
-        k, grid, tuned = ch.k, ch.grid, ch.table
-    k, grid = (int(v) for v in from_rank0([k, grid], world, dev))   # every replica runs rank 0's choice
-    eng.set_sweep_grid(grid)
-    bt = native.Batch(eng, [D32], [Op], k)
-    eng.set_sweep_grid(0)
+        lg = log if rank == 0 else None
+        ch = autotune.tune(eng, D32, Op, rhs, tol=TOL, max_iter=MAX_ITER, log=lg)
+        k, grid, nlanes, best = ch.k, ch.grid, 1, ch.solves_per_s
+        tuned = [{"k": t[0], "lanes": 1, "grid": t[1] or "resident", "solves_s": t[2]} for t in ch.table]
+        for nl, g, sps, _ in autotune.tune_lanes(A, F, rhs, k, tol=TOL, max_iter=MAX_ITER, device=local_rank, log=lg):
+            tuned.append({"k": k, "lanes": nl, "grid": g, "solves_s": sps})
+            if sps > best:
+                grid, nlanes, best = g, nl, sps
+    k, grid, nlanes = (int(v) for v in from_rank0([k, grid, nlanes], world, dev))   # every replica runs rank 0's choice
+    D32.close()
+    Op.close()
+    lanes = Lanes(A, F, k, lanes=nlanes, grid=grid, device=local_rank)
+    grid = lanes.grid
+    bt = lanes.lanes[0].batch
+    streams = [torch.cuda.ExternalStream(h) for h in lanes.streams]
     sets = []
     for p in range(POOL):
-        Bf, nrhs = bt.pack([np.stack([rhs(p * k + c) for c in range(k)])])
+        Bf, nrhs = lanes.pack(np.stack([rhs(p * k + c) for c in range(k)]))
         sets.append((Bf, torch.from_numpy(Bf).to(dev)))
-    dX = torch.empty_like(sets[0][1])
+    dXs = [torch.empty_like(sets[0][1]) for _ in range(nlanes)]
     torch.cuda.synchronize()
 
     def step_dev(i, flags=native.DEVICE_PTRS):
-        return bt.solve_raw(sets[i % POOL][1], dX, nrhs, tol=TOL, max_iter=MAX_ITER, flags=flags)
+        # lane j solves set (i * lanes + j) of the pool
+        return lanes.solve_raw([sets[(i * nlanes + j) % POOL][1] for j in range(nlanes)], dXs, nrhs, tol=TOL,
+                               max_iter=MAX_ITER, flags=flags)
 
     for i in range(args.warmup):
         step_dev(i)
     # FP64 verification of every slot of one step, on the device and on the host
     res = step_dev(0, native.DEVICE_PTRS | native.TRUE_RESIDUAL)
-    its = [res[c].iterations for c in range(k)]
-    dev_tres = max(res[c].true_residual for c in range(k))
-    X0 = dX.cpu().numpy()
+    its = [r.iterations for lane in res for r in lane[:k]]
+    dev_tres = max(r.true_residual for lane in res for r in lane[:k])
     host_tres = 0.0
-    for c in range(k):
-        bcol, xcol = sets[0][0][c * n:(c + 1) * n], X0[c * n:(c + 1) * n]
-        host_tres = max(host_tres, float(np.linalg.norm(bcol - A.matvec(xcol)) / np.linalg.norm(bcol)))
-    log(f"[bench] rank {rank}: k={k} grid={grid or 'resident'}: iterations {min(its)}-{max(its)}, "
+    for j in range(nlanes):
+        X0, B0 = dXs[j].cpu().numpy(), sets[j % POOL][0]
+        for c in range(k):
+            bcol, xcol = B0[c * n:(c + 1) * n], X0[c * n:(c + 1) * n]
+            host_tres = max(host_tres, float(np.linalg.norm(bcol - A.matvec(xcol)) / np.linalg.norm(bcol)))
+    log(f"[bench] rank {rank}: k={k} lanes={nlanes} grid={grid or 'resident'}: iterations {min(its)}-{max(its)}, "
         f"fp64 true relres max {host_tres:.2e} (device {dev_tres:.2e})")
 
     def barrier():
@@ -332,52 +346,69 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- value: device-resident batched solves ----
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    lane_ev = [torch.cuda.Event() for _ in streams]
+
+    def open_region():
+        # every lane's stream starts after ev0 on lane 0's stream
+        ev0.record(streams[0])
+        for st in streams[1:]:
+            st.wait_event(ev0)
+
+    def close_region():
+        # ev1 on lane 0's stream after every lane's work
+        for st, e in zip(streams, lane_ev):
+            e.record(st)
+            streams[0].wait_event(e)
+        ev1.record(streams[0])
+
     iters_timed = []
     with ClockSampler(local_rank) as clk:
         barrier()
-        ev0.record(stream)
+        open_region()
         for i in range(args.steps):
             r = step_dev(i + 1)
-            iters_timed.append(max(r[c].iterations for c in range(k)))
-        ev1.record(stream)
+            iters_timed.append(max(x.iterations for lane in r for x in lane[:k]))
+        close_region()
         barrier()
     dev_s = ev0.elapsed_time(ev1) * 1e-3
-    # ---- e2e: pinned host buffers through the C ABI ----
+    # ---- e2e: pinned host buffers through the C ABI (apxb_batch_solve, one call per lane) ----
     hB = [torch.from_numpy(s[0]).pin_memory() for s in sets]
-    hX = torch.empty(n * k, dtype=torch.float64).pin_memory()
+    hX = [torch.empty(n * k, dtype=torch.float64).pin_memory() for _ in range(nlanes)]
 
     def step_host(i):
-        res_h = (native.PcgResult * (k))()
-        native.check(eng.lib.apxb_batch_solve(bt.h, hB[i % POOL].data_ptr(), hX.data_ptr(), native.ptr(nrhs),
-                                              TOL, MAX_ITER, 0, res_h))
-        return res_h
+        return lanes.solve_raw([hB[(i * nlanes + j) % POOL] for j in range(nlanes)], hX, nrhs, tol=TOL,
+                               max_iter=MAX_ITER, flags=0)
 
     step_host(0)
     barrier()
-    ev0.record(stream)
+    open_region()
     for i in range(args.steps):
         step_host(i + 1)
-    ev1.record(stream)
+    close_region()
     barrier()
     e2e_s = ev0.elapsed_time(ev1) * 1e-3
-    # ---- roofline: the batch's own fp32 k-RHS sweeps ----
-    fwd_s, bck_s = bt.sweep_timed(10)
+    # ---- roofline: the batches' own fp32 k-RHS sweeps, all lanes running them at once ----
+    st = lanes.sweep_timed(10)
+    fwd_s = sum(t[0] for t in st) / len(st)
+    bck_s = sum(t[1] for t in st) / len(st)
     m, nnz_s = D32.info.m, D32.info.nnz_stored
     sweep_bytes = nnz_s * 8 + 4 * (m + 1) + 2 * m * 4 * k
     sweep_s = (fwd_s + bck_s) / 2
     peak, peak_kind = measured_peak_hbm()
-    achieved = sweep_bytes / sweep_s / 1e9
+    achieved = sum(2 * sweep_bytes / (t[0] + t[1]) for t in st) / 1e9   # summed over the concurrent lanes
     traffic, traffic_src = profiled_traffic(k, args.grid)
     b_iter = 2 * (nnz_s * 8 + 4 * (m + 1)) + A.nnz * 12 + 4 * (n + 1)
+    b_iter *= nlanes   # every lane reads the factor and the matrix once per iteration
     iter_s = dev_s / max(1, sum(iters_timed))
     iter_gbs = b_iter / iter_s / 1e9
     dev_s, e2e_s = max_over_ranks([dev_s, e2e_s], world, dev)
-    bt.close()
+    lanes.close()
 
     # ---- plain fp64 single-RHS path ----
     plain = None
     if not args.no_plain:
         D64 = native.DeviceFactor(eng, F, precision=native.PREC_FP64)
+        Op = native.DeviceOperator(eng, A, F.perm)
         db = torch.from_numpy(rhs(0)).to(dev)
         dx = torch.empty_like(db)
         for _ in range(3):
@@ -397,39 +428,42 @@ def run_ours(args, rank, world, local_rank):
         plain = {"solves_s": ns / sum(secs), "ms_per_solve": sum(secs) / ns * 1e3, "iterations": pits,
                  "sweep_us": pair64 / 2 * 1e6, "sweep_gbs": b64 / (pair64 / 2) / 1e9}
         D64.close()
+        Op.close()
         log(f"[bench] plain fp64: {plain['solves_s']:.1f} solves/s ({plain['ms_per_solve']:.1f} ms, {pits} it), "
             f"fp64 sweep {plain['sweep_us']:.0f} us = {plain['sweep_gbs']:.0f} GB/s")
 
-    value = world * args.steps * k / dev_s
+    value = world * args.steps * k * nlanes / dev_s
     serving = None
     if not args.no_serving and rank == 0:
-        serving = serving_run(A, F, k, args.iters_per_step, 0.7 * value / world, args.serve_requests, 11, log)
+        serving = serving_run(A, F, k, nlanes, grid, args.iters_per_step, 0.7 * value / world, args.serve_requests,
+                              11, log)
 
     if rank != 0:
         eng.close()
         return 0
     mean_its = sum(iters_timed) / max(1, len(iters_timed))
-    launches_per_step = 1 + 12 * (mean_its + 1) + 3
+    launches_per_step = nlanes * (1 + 12 * (mean_its + 1) + 3)
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_s / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 sweeps / f64 outer",
         "data": "synthetic (seeded generator, reference factorization)",
-        "config": workload_config(args.grid, A, F, f"batched mixed precision, {k} RHS per step",
-                                  {"k": k, "sweep_grid": grid or "resident", "rhs_sets": POOL,
+        "config": workload_config(args.grid, A, F, f"batched mixed precision, {nlanes} lane(s) x {k} RHS per step",
+                                  {"k": k, "lanes": nlanes, "sweep_grid": grid or "resident", "rhs_sets": POOL,
                                    "parallelism": f"replicas x{world}"}),
         "iterations": [min(iters_timed), max(iters_timed)], "true_relres_max": host_tres,
-        "e2e": {"value": world * args.steps * k / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": 8 * n * k,
-                "d2h_bytes_per_step": 8 * n * k + 24 * k},
+        "e2e": {"value": world * args.steps * k * nlanes / e2e_s, "unit": "solves/s",
+                "h2d_bytes_per_step": 8 * n * k * nlanes, "d2h_bytes_per_step": (8 * n * k + 24 * k) * nlanes},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "traffic_source": traffic_src,
-                     "kernel": f"k_dw32<DIR,{k}> (batched fp32 sweep, {k} RHS)",
+                     "kernel": f"k_dw32<DIR,{k}> (batched fp32 sweep, {k} RHS, {nlanes} concurrent lane(s), "
+                               f"{grid} blocks each)",
                      "bytes_per_launch": sweep_bytes, "fwd_us": fwd_s * 1e6, "bck_us": bck_s * 1e6,
                      "peak_kind": peak_kind, "iter_bytes": b_iter, "iter_gbs": iter_gbs, "iter_frac": iter_gbs / peak},
         "plain_fp64": plain,
         "speedup_vs_plain_fp64": (value / world) / plain["solves_s"] if plain else None,
         "serving": serving,
-        "autotune": [{"k": t[0], "grid": t[1] or "resident", "solves_s": t[2]} for t in tuned] if tuned else None,
+        "autotune": tuned,
         "gpu_launches": int(round(launches_per_step * args.steps)),
         "clocks": clk.summary(),
     }
@@ -451,7 +485,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--grid", type=int, default=128, help="grid side (the workload is 128)")
     ap.add_argument("--k", type=int, default=0, help="right-hand sides per step (0 = autotune)")
-    ap.add_argument("--sweep-grid", type=int, default=0, help="sweep blocks with --k (0 = resident)")
+    ap.add_argument("--sweep-grid", type=int, default=0, help="sweep blocks per lane with --k (0 = resident / lanes)")
+    ap.add_argument("--lanes", type=int, default=1, help="concurrent batches (streams) with --k")
     ap.add_argument("--iters-per-step", type=int, default=2, help="serving: iterations per server step")
     ap.add_argument("--serve-requests", type=int, default=1000)
     ap.add_argument("--no-serving", action="store_true")

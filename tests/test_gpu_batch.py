@@ -84,3 +84,27 @@ def test_autotuner_picks_the_fastest_candidate(eng):
     assert len(ch.table) == 4
     assert ch.solves_per_s == max(t[2] for t in ch.table)
     assert (ch.k, ch.grid) in [(t[0], t[1]) for t in ch.table]
+
+
+def test_lanes_give_the_same_bits_as_one_batch(eng):
+    """Concurrent batches on separate streams (apxchol_b200.lanes) with a cut
+    sweep grid return exactly what one batch returns."""
+    import torch
+    from apxchol_b200.lanes import Lanes
+    A, F, D, Op = _objs(eng, "grid3d_24")
+    k = 4
+    B = np.stack([gen.rhs(A.n, 700 + c, False) for c in range(k)])
+    bt = native.Batch(eng, [D], [Op], k)
+    want, _ = bt.solve([B], tol=TOL)
+    ln = Lanes(A, F, k, lanes=3)
+    try:
+        Bf, nrhs = ln.pack(B)
+        Bs = [torch.from_numpy(Bf).cuda() for _ in range(3)]
+        Xs = [torch.empty_like(b) for b in Bs]
+        res = ln.solve_raw(Bs, Xs, nrhs, tol=TOL, flags=native.DEVICE_PTRS)
+        for j in range(3):
+            got = ln.lanes[j].batch.unpack(Xs[j].cpu().numpy(), nrhs)[0]
+            assert np.array_equal(got, want[0])
+            assert all(r.status == 0 for r in res[j][:k])
+    finally:
+        ln.close()

@@ -38,9 +38,10 @@ def _alone(mat, fac, b, tol):
         eng.close()
 
 
-def test_results_equal_alone_and_in_the_mix():
+@pytest.mark.parametrize("lanes", [1, 2])
+def test_results_equal_alone_and_in_the_mix(lanes):
     mats = {"g2": problem("grid2d_64"), "g3": problem("grid3d_24"), "rr": problem("regular_3000")}
-    srv = SolveServer(k=K, iters_per_step=3)
+    srv = SolveServer(k=K, iters_per_step=3, lanes=lanes)
     try:
         for mid, (A, F) in mats.items():
             srv.register(mid, A, F)
@@ -96,10 +97,10 @@ def test_budget_admission_and_eviction():
         ea, eb = srv.estimate("a"), srv.estimate("b")
         srv.budget = max(ea, eb) + min(ea, eb) // 2     # room for one matrix only
         srv.admit_matrix("a")
-        assert srv.resident["a"].eng.memory_used() <= ea == srv.used_bytes()
+        assert srv.resident["a"].lanes[0].eng.memory_used() <= ea == srv.used_bytes()
         srv.admit_matrix("b")                # evicts idle "a"
         assert "a" not in srv.resident and srv.evictions == 1
-        assert srv.resident["b"].eng.memory_used() <= eb == srv.used_bytes()
+        assert srv.resident["b"].lanes[0].eng.memory_used() <= eb == srv.used_bytes()
         req = srv.submit("b", gen.rhs(A2.n, 1, False), 1e-8)   # "b" busy
         with pytest.raises(BudgetError):
             srv.admit_matrix("a")            # cannot evict a busy matrix
