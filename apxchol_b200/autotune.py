@@ -110,3 +110,31 @@ def tune_lanes(mat, fac, rhs, k: int, lanes_list=(2, 3, 4), tol: float = 1e-8, m
             ln.close()
             del ln
     return table
+
+
+def tune_instances(eng: native.Engine, factors, ops, rhs, tol: float = 1e-8, max_iter: int = 500, ks=KS, log=None):
+    """Pick k for a multi-instance batch: rhs[i] is instance i's (c_i, n_i)
+    right-hand sides. A width k solves them in ceil(max c_i / k) passes of one
+    batch; every pass is timed (device events), and the k with the highest
+    total solves/s wins. Returns (k, [(k, solves/s, seconds)])."""
+    total = sum(int(np.atleast_2d(b).shape[0]) for b in rhs)
+    table = []
+    for k in ks:
+        bt = native.Batch(eng, factors, ops, k)
+        try:
+            cmax = max(int(np.atleast_2d(b).shape[0]) for b in rhs)
+            secs = 0.0
+            for p0 in range(0, cmax, k):
+                part = [np.atleast_2d(b)[p0:p0 + k] for b in rhs]
+                part = [q if q.shape[0] else np.zeros((0, f.n)) for q, f in zip(part, factors)]
+                B, nrhs = bt.pack(part)
+                X = np.empty_like(B)
+                res = bt.solve_raw(B, X, nrhs, tol=tol, max_iter=max_iter)
+                secs += res[0].seconds
+        finally:
+            bt.close()
+        table.append((k, total / secs, secs))
+        if log:
+            log(f"[autotune] instances={len(factors)} k={k:2d}: {secs * 1e3:8.2f} ms, {total / secs:8.1f} solves/s")
+    best = max(table, key=lambda t: t[1])
+    return best[0], table

@@ -102,10 +102,20 @@ __device__ __forceinline__ void col_store(double (&a)[NV][2], double* dst) {
 
 // Flat walk of a tile's [row][K] block in pairs: element q = 2 * (tid + j * kBT)
 // from the tile base; the thread's column pair is fixed (kBT * 2 % K == 0).
+// Pairs are accessed as double2 / float2, so they must start at an even
+// element: for K == 1 a tile starts at its instance's row offset, which can be
+// odd, and then thread 0 takes the first element alone (two == false) and the
+// pairs start one element later. (For K >= 2 the base is always even.)
 #define FLAT_PAIRS(t, ...)                                                                    \
     {                                                                                          \
-        const size_t base_ = static_cast<size_t>(P.tile_lo[t]) * K;                           \
+        const size_t lo_ = static_cast<size_t>(P.tile_lo[t]) * K;                             \
         const size_t end_ = static_cast<size_t>(P.tile_hi[t]) * K;                            \
+        if ((lo_ & 1u) && threadIdx.x == 0 && lo_ < end_) {                                   \
+            const size_t q = lo_;                                                              \
+            const bool two = false;                                                            \
+            __VA_ARGS__                                                                        \
+        }                                                                                      \
+        const size_t base_ = lo_ + (lo_ & 1u);                                                 \
         for (size_t q = base_ + 2 * threadIdx.x; q < end_; q += 2 * kBT) {                   \
             const bool two = q + 1 < end_;                                                     \
             __VA_ARGS__                                                                        \

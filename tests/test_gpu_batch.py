@@ -108,3 +108,55 @@ def test_lanes_give_the_same_bits_as_one_batch(eng):
             assert all(r.status == 0 for r in res[j][:k])
     finally:
         ln.close()
+
+
+def _mixed_instances(count: int, seed: int):
+    """SDDM instances shaped like the uneven multi-instance workload, scaled
+    down: half 2D 5-point grids (weights U[1,2]), half random 6-regular graphs
+    (weights U[0.5,2]), diagonal shift 1e-3 * degree, sizes drawn uniformly."""
+    from apxchol_b200 import refsetup
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        if i % 2 == 0:
+            side = int(rng.integers(20, 90))
+            A = gen.grid2d(side, int(rng.integers(20, 90)), seed=100 + i, shift=1e-3)
+        else:
+            A = gen.random_regular(int(rng.integers(1000, 6000)), seed=100 + i, shift=1e-3)
+        F = refsetup.factorize(A, seed=i, threads=8)
+        out.append((A, F))
+    return out
+
+
+@pytest.mark.parametrize("k", [4, 8])
+def test_many_uneven_instances_in_one_batch(eng, k):
+    insts = _mixed_instances(24, seed=k)
+    Ds = [native.DeviceFactor(eng, F, precision=native.PREC_FP32) for _, F in insts]
+    Ops = [native.DeviceOperator(eng, A, F.perm) for A, F in insts]
+    bt = native.Batch(eng, Ds, Ops, k)
+    rng = np.random.default_rng(7)
+    rhs = [np.stack([gen.rhs(A.n, 1000 * i + j, False) for j in range(int(rng.integers(1, k + 1)))])
+           for i, (A, F) in enumerate(insts)]
+    xs, res = bt.solve(rhs, tol=TOL)
+    for i, (A, F) in enumerate(insts):
+        for c in range(rhs[i].shape[0]):
+            r = res[i][c]
+            assert r.status == 0 and r.true_residual < TRUE_RES_FACTOR * TOL, (i, c, r.true_residual)
+            relres = np.linalg.norm(rhs[i][c] - A.matvec(xs[i][c])) / np.linalg.norm(rhs[i][c])
+            assert relres < TRUE_RES_FACTOR * TOL
+    # a few instances alone give the same bits
+    for i in (0, 5, 23):
+        alone = native.Batch(eng, [Ds[i]], [Ops[i]], k)
+        xa, _ = alone.solve([rhs[i]], tol=TOL)
+        assert np.array_equal(xs[i], xa[0]), i
+
+
+def test_instance_autotuner(eng):
+    from apxchol_b200 import autotune
+    insts = _mixed_instances(6, seed=3)
+    Ds = [native.DeviceFactor(eng, F, precision=native.PREC_FP32) for _, F in insts]
+    Ops = [native.DeviceOperator(eng, A, F.perm) for A, F in insts]
+    rhs = [np.stack([gen.rhs(A.n, 50 * i + j, False) for j in range(1 + i % 5)]) for i, (A, F) in enumerate(insts)]
+    k, table = autotune.tune_instances(eng, Ds, Ops, rhs, ks=(1, 2, 4, 8))
+    assert [t[0] for t in table] == [1, 2, 4, 8]
+    assert k == max(table, key=lambda t: t[1])[0]
