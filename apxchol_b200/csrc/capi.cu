@@ -656,6 +656,13 @@ int enqueue_iteration(apxb_operator* a, apxb_factor* f, const apxb::pcg_ptrs& p,
     return enqueue_apply(a, f, p, handle, use_cond);
 }
 
+// APXB_NO_GRAPH=1: no conditional graph (the loop falls back to one-iteration
+// graphs launched by the host), so a profiler sees every kernel.
+bool conditional_graph_off() {
+    const char* v = std::getenv("APXB_NO_GRAPH");
+    return v && *v && *v != '0';
+}
+
 // Graph of the whole iteration loop: a conditional WHILE node whose body is one
 // iteration; the body's last kernel clears the condition once `done` is set.
 int build_loop_graph(apxb_operator* a, apxb_factor* f) {
@@ -668,7 +675,8 @@ int build_loop_graph(apxb_operator* a, apxb_factor* f) {
     cudaGraph_t g = nullptr;
     APXB_CK(cudaGraphCreate(&g, 0));
     cudaGraphConditionalHandle h;
-    cudaError_t err = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+    cudaError_t err = conditional_graph_off() ? cudaErrorNotSupported
+                                              : cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
     if (err == cudaSuccess) {
         cudaGraphNodeParams cp = {};
         cp.type = cudaGraphNodeTypeConditional;
