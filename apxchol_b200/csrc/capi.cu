@@ -622,6 +622,10 @@ apxb::pcg_ptrs pcg_ptrs_of(apxb_operator* a, apxb_factor* f) {
     p.b_orig = a->b_orig; p.x_orig = a->x_orig;
     p.st = a->st; p.err = a->e->d_err; p.partials = a->e->d_partials; p.counters = a->e->d_counters;
     p.n = a->n; p.grid = a->e->vec_grid;
+    // lanes per SpMV row from the average row length: a thread per row keeps a
+    // short row's gathers in flight together; long rows share lanes
+    const double avg = a->n ? static_cast<double>(a->nnz) / a->n : 0.0;
+    p.spmv_lanes = avg <= 16.0 ? 1 : (avg <= 64.0 ? 8 : 32);
     return p;
 }
 

@@ -100,6 +100,7 @@ struct pcg_ptrs {
     unsigned* counters;   // [8]
     unsigned n;
     int grid;
+    int spmv_lanes;       // 1: a thread per row (short rows), else lanes per row
 };
 
 void launch_pcg_init(const pcg_ptrs& p, cudaStream_t s);

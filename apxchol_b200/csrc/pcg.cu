@@ -149,6 +149,50 @@ __global__ void __launch_bounds__(kThreads) k_pcg_spmv(pcg_ptrs p) {
     }
 }
 
+// The same for short rows: a thread per row, the row's entries summed in CSR
+// order, their gathers issued 8 at a time.
+__global__ void __launch_bounds__(kThreads) k_pcg_spmv_rows(pcg_ptrs p) {
+    pcg_state* st = p.st;
+    if (stopped(st, p.err)) return;
+    constexpr int kE = 8;
+    double v[1] = {0.0};
+    for (unsigned row = blockIdx.x * blockDim.x + threadIdx.x; row < p.n; row += gridDim.x * blockDim.x) {
+        const int b = __ldg(p.a_ptr + row), e = __ldg(p.a_ptr + row + 1);
+        double s = 0.0, own = 0.0;
+        bool have_own = false;
+        for (int k0 = b; k0 < e; k0 += kE) {
+            int col[kE];
+            double w[kE], x[kE];
+#pragma unroll
+            for (int j = 0; j < kE; ++j)
+                if (k0 + j < e) { col[j] = __ldg(p.a_idx + k0 + j); w[j] = __ldg(p.a_val + k0 + j); }
+#pragma unroll
+            for (int j = 0; j < kE; ++j)
+                if (k0 + j < e) x[j] = p.p[col[j]];
+#pragma unroll
+            for (int j = 0; j < kE; ++j)
+                if (k0 + j < e) {
+                    s = fma(w[j], x[j], s);
+                    if (col[j] == static_cast<int>(row)) { own = x[j]; have_own = true; }
+                }
+        }
+        p.Ap[row] = s;
+        if (!have_own) own = p.p[row];
+        v[0] = fma(own, s, v[0]);
+    }
+    double tot[1];
+    if (grid_sum<1>(v, p.partials, p.counters + kCSpmv, tot)) {
+        st->pAp = tot[0];
+        st->pmode = 0;
+        if (tot[0] <= 0.0) {
+            st->done = 1;
+            st->status = 3;
+        } else {
+            st->alpha = st->rz / tot[0];
+        }
+    }
+}
+
 // x += alpha p; r -= alpha Ap; r.r and sum(r) (src/solve.cpp:169-208), then
 // the stop rules (solve.cpp:600-615) and the next application's centring.
 __global__ void __launch_bounds__(kThreads) k_pcg_update_xr(pcg_ptrs p) {
@@ -271,7 +315,11 @@ void launch_pcg_rz(const pcg_ptrs& p, cudaStream_t s) { k_pcg_rz<<<p.grid, kThre
 void launch_pcg_update_p(const pcg_ptrs& p, cudaStream_t s, unsigned long long h, int use_cond) {
     k_pcg_update_p<<<p.grid, kThreads, 0, s>>>(p, h, use_cond);
 }
-void launch_pcg_spmv(const pcg_ptrs& p, cudaStream_t s) { k_pcg_spmv<8><<<p.grid, kThreads, 0, s>>>(p); }
+void launch_pcg_spmv(const pcg_ptrs& p, cudaStream_t s) {
+    if (p.spmv_lanes == 1) k_pcg_spmv_rows<<<p.grid, kThreads, 0, s>>>(p);
+    else if (p.spmv_lanes == 8) k_pcg_spmv<8><<<p.grid, kThreads, 0, s>>>(p);
+    else k_pcg_spmv<32><<<p.grid, kThreads, 0, s>>>(p);
+}
 void launch_pcg_update_xr(const pcg_ptrs& p, cudaStream_t s) { k_pcg_update_xr<<<p.grid, kThreads, 0, s>>>(p); }
 void launch_pcg_finish(const pcg_ptrs& p, cudaStream_t s) {
     k_pcg_xsum<<<p.grid, kThreads, 0, s>>>(p);
