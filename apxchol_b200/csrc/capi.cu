@@ -203,8 +203,10 @@ int apxb_factor_create(apxb_engine* e, uint32_t n, const uint32_t* colptr, const
         const apxb::sweep_plan& pl = dir == 0 ? h.fwd_plan : h.bck_plan;
         if ((rc = f->dalloc(&f->info[dir], pl.info.size())) || (rc = f->dalloc(&f->ord[dir], pl.ord.size())) ||
             (rc = f->dalloc(&f->ptr[dir], pl.ptr.size())) || (rc = f->dalloc(&f->idx[dir], pl.idx.size())) ||
-            (rc = f->dalloc(&f->val[dir], pl.val.size())))
+            (rc = f->dalloc(&f->val[dir], pl.val.size())) || (rc = f->dalloc(&f->chunk[dir], pl.chunk.size())))
             return rc;
+        f->n_chunks[dir] = static_cast<uint32_t>(pl.chunk.size() - 1);
+        APXB_CK(cudaMemcpyAsync(f->chunk[dir], pl.chunk.data(), 4 * pl.chunk.size(), cudaMemcpyHostToDevice, s));
         APXB_CK(cudaMemcpyAsync(f->info[dir], pl.info.data(), 4 * pl.info.size(), cudaMemcpyHostToDevice, s));
         APXB_CK(cudaMemcpyAsync(f->ord[dir], pl.ord.data(), 4 * pl.ord.size(), cudaMemcpyHostToDevice, s));
         APXB_CK(cudaMemcpyAsync(f->ptr[dir], pl.ptr.data(), 4 * pl.ptr.size(), cudaMemcpyHostToDevice, s));
@@ -308,6 +310,8 @@ void plan_args(const apxb_factor* f, int dir, apxb::sweep_args<T>& a) {
     a.seg_ptr = f->seg_ptr[dir];
     a.seg_idx = f->seg_idx[dir];
     a.seg_val = f->seg_val[dir];
+    a.chunk = f->chunk[dir];
+    a.n_chunks = f->n_chunks[dir];
 }
 
 apxb::sweep_args<double> sweep64_args(apxb_factor* f, int dir) {
@@ -811,7 +815,7 @@ extern "C" int apxb_test_stalled_sweep(apxb_engine* e, apxb_factor* f, uint64_t 
     int rc = e->ensure_stage(f->h.n);
     if (rc) return rc;
     APXB_CK(cudaMemsetAsync(e->d_stage_a, 0, 8 * static_cast<size_t>(f->h.n), s));
-    // Start the forward work counter past chunk 0: rows 0..31 are never solved.
+    // Start the forward work counter past claim unit 0: its rows are never solved.
     const apxb::sweep_ctl start{1u, 0u};
     APXB_CK(cudaMemcpyAsync(f->ctl, &start, sizeof(start), cudaMemcpyHostToDevice, s));
     const unsigned long long saved = e->budget_ns;

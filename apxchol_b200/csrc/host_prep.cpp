@@ -109,10 +109,11 @@ void build_plan(uint32_t m, const std::vector<int32_t>& level, int32_t n_levels,
                 item_rows.push_back(r);
                 if (++in_item == cap) {
                     plan.info.push_back(in_item | (lg << 8) | (thin << 16));
+                    plan.item_level.push_back(l);
                     in_item = 0;
                 }
             }
-            if (in_item) plan.info.push_back(in_item | (lg << 8) | (thin << 16));
+            if (in_item) { plan.info.push_back(in_item | (lg << 8) | (thin << 16)); plan.item_level.push_back(l); }
         }
         std::vector<uint32_t>().swap(rows);
     }
@@ -145,6 +146,7 @@ void build_plan(uint32_t m, const std::vector<int32_t>& level, int32_t n_levels,
     plan.ptr[npos] = e;
     plan.idx.resize(e);
     plan.val.resize(e);
+    chunk_plan(plan);
 }
 
 // Plan invariants the kernels rely on (checked at every setup): every row is
@@ -191,6 +193,9 @@ std::string check_plan(uint32_t m, const std::vector<int32_t>& level, const swee
     }
     for (uint32_t r = 0; r < m; ++r)
         if (!seen[r]) return "plan misses row " + std::to_string(r);
+    if (pl.chunk.empty() || pl.chunk.front() != 0 || pl.chunk.back() != pl.n_items) return "bad chunk table";
+    for (size_t i = 0; i + 1 < pl.chunk.size(); ++i)
+        if (pl.chunk[i + 1] <= pl.chunk[i] || pl.chunk[i + 1] - pl.chunk[i] > 8) return "bad chunk";
     return {};
 }
 

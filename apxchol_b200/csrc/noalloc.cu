@@ -73,6 +73,7 @@ apxb::sweep_args<double> noalloc_args(const apxb_factor* f, int dir, apxb::sweep
     a.seg_first = pl.seg_first; a.seg_rows = pl.seg_rows; a.seg_levels = pl.seg_levels;
     a.seg_row = f->seg_row[dir]; a.seg_lvl = f->seg_lvl[dir]; a.seg_ptr = f->seg_ptr[dir];
     a.seg_idx = f->seg_idx[dir]; a.seg_val = f->seg_val[dir];
+    a.chunk = f->chunk[dir]; a.n_chunks = f->n_chunks[dir];
     a.ctl = ctl + dir;
     a.err = f->e->d_err;
     a.budget_ns = f->e->budget_ns;

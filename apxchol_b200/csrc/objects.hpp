@@ -129,6 +129,8 @@ struct apxb_factor {
     uint32_t* ptr[2] = {nullptr, nullptr};
     uint32_t* idx[2] = {nullptr, nullptr};
     float* val[2] = {nullptr, nullptr};
+    uint32_t* chunk[2] = {nullptr, nullptr};           // claim units (host_prep.hpp, chunk_plan)
+    uint32_t n_chunks[2] = {0, 0};
     uint32_t *seg_row[2] = {nullptr, nullptr}, *seg_lvl[2] = {nullptr, nullptr};
     uint32_t *seg_ptr[2] = {nullptr, nullptr}, *seg_idx[2] = {nullptr, nullptr};
     float* seg_val[2] = {nullptr, nullptr};

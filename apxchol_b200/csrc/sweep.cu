@@ -194,6 +194,49 @@ __device__ __forceinline__ lane_view view_of(const stage_desc& d) {
     return v;
 }
 
+// Warp-uniform chunked claim: the items of the current chunk, then those of
+// the pending chunk, whose ticket was taken when the current one began and
+// whose bounds are loaded when the current chunk hands out its last item.
+// A contended same-address atomic takes about (claimers x 0.7 ns), so the
+// ticket is only read a chunk later.
+struct chunk_claim {
+    template <class T>
+    __device__ __forceinline__ void start(const sweep_args<T>& a) {
+        unsigned t = 0;
+        if ((threadIdx.x & 31u) == 0) t = atomicAdd(&a.ctl->ticket, 1u);
+        pend = __shfl_sync(kFull, t, 0);
+    }
+    unsigned cur = 0, end = 0;
+    unsigned pend = 0;            // ticket of the next chunk
+    unsigned plo = 0, phi = 0;    // its bounds (valid when loaded)
+    bool loaded = false;
+    template <class T>
+    __device__ __forceinline__ void load_pending(const sweep_args<T>& a) {
+        if (!loaded && pend < a.n_chunks) {
+            plo = __ldg(a.chunk + pend);
+            phi = __ldg(a.chunk + pend + 1);
+            loaded = true;
+        }
+    }
+    template <class T>
+    __device__ __forceinline__ unsigned next(const sweep_args<T>& a) {
+        if (cur >= end) {
+            if (pend >= a.n_chunks) return a.n_items;
+            load_pending(a);
+            cur = plo;
+            end = phi;
+            loaded = false;
+            unsigned t = 0;
+            if ((threadIdx.x & 31u) == 0) t = atomicAdd(&a.ctl->ticket, 1u);
+            pend = __shfl_sync(kFull, t, 0);
+            return cur++;
+        }
+        const unsigned c = cur++;
+        if (cur >= end) load_pending(a);
+        return c;
+    }
+};
+
 // ---------------------------------------------------------------------------
 // fp64 dataflow sweep.
 
@@ -366,27 +409,21 @@ template <int DIR>
 __global__ void __launch_bounds__(kSweepThreads, 2) k_df64(const sweep_args<double> a) {
     if (a.skip && *a.skip) return;
     const unsigned lane = threadIdx.x & 31u;
-    // prologue: tickets for the first three stages
-    unsigned tk = 0;
-    if (lane == 0) tk = atomicAdd(&a.ctl->ticket, 1u);
+    chunk_claim cc;
+    cc.start(a);
     stage_desc dD;
-    load_desc(a, __shfl_sync(kFull, tk, 0), dD);
-    if (lane == 0) tk = atomicAdd(&a.ctl->ticket, 1u);
+    load_desc(a, cc.next(a), dD);
     stage_data64 sL;
     load_data64(a, dD, sL);
-    load_desc(a, __shfl_sync(kFull, tk, 0), dD);
-    if (lane == 0) tk = atomicAdd(&a.ctl->ticket, 1u);
+    load_desc(a, cc.next(a), dD);
+    int bad = 0;   // the error word, read one item late so the load is never waited on
     while (sL.v.c < a.n_items) {
-        // rotate: run L, data for D, descriptor for the claimed ticket, claim the next
+        // rotate: run L, data for D, descriptor of the next claimed item
         stage_data64 sR = sL;
         load_data64(a, dD, sL);
-        load_desc(a, __shfl_sync(kFull, tk, 0), dD);
-        int bad = 0;
-        if (lane == 0) {
-            tk = atomicAdd(&a.ctl->ticket, 1u);
-            bad = ld_relaxed_int(&a.err->code);
-        }
+        load_desc(a, cc.next(a), dD);
         if (__shfl_sync(kFull, bad, 0)) break;
+        if (lane == 0) bad = ld_relaxed_int(&a.err->code);
         if (!run64<DIR>(a, sR)) break;
     }
     leave(a.ctl);
@@ -557,25 +594,20 @@ template <int DIR, int K>
 __global__ void __launch_bounds__(kSweepThreads, 2) k_df32(const sweep_args<float> a, const double* in64) {
     if (a.skip && *a.skip) return;
     const unsigned lane = threadIdx.x & 31u;
-    unsigned tk = 0;
-    if (lane == 0) tk = atomicAdd(&a.ctl->ticket, 1u);
+    chunk_claim cc;
+    cc.start(a);
     stage_desc dD;
-    load_desc(a, __shfl_sync(kFull, tk, 0), dD);
-    if (lane == 0) tk = atomicAdd(&a.ctl->ticket, 1u);
+    load_desc(a, cc.next(a), dD);
     stage_data32<K> sL;
     load_data32<K>(a, in64, dD, sL);
-    load_desc(a, __shfl_sync(kFull, tk, 0), dD);
-    if (lane == 0) tk = atomicAdd(&a.ctl->ticket, 1u);
+    load_desc(a, cc.next(a), dD);
+    int bad = 0;   // the error word, read one item late
     while (sL.v.c < a.n_items) {
         stage_data32<K> sR = sL;
         load_data32<K>(a, in64, dD, sL);
-        load_desc(a, __shfl_sync(kFull, tk, 0), dD);
-        int bad = 0;
-        if (lane == 0) {
-            tk = atomicAdd(&a.ctl->ticket, 1u);
-            bad = ld_relaxed_int(&a.err->code);
-        }
+        load_desc(a, cc.next(a), dD);
         if (__shfl_sync(kFull, bad, 0)) break;
+        if (lane == 0) bad = ld_relaxed_int(&a.err->code);
         if (!run32<DIR, K>(a, sR)) break;
     }
     leave(a.ctl);
@@ -707,51 +739,12 @@ __device__ __forceinline__ bool run_wide(const sweep_args<float>& a, stage_wide<
     return true;
 }
 
-// Warp-uniform chunked claim: the items of the current chunk, then those of
-// the pending chunk, whose ticket was taken when the current one began and
-// whose bounds are loaded when the current chunk hands out its last item.
-// A contended same-address atomic takes about (claimers x 0.7 ns), so the
-// ticket is only read a chunk later.
-struct chunk_claim {
-    unsigned cur = 0, end = 0;
-    unsigned pend = 0;            // ticket of the next chunk
-    unsigned plo = 0, phi = 0;    // its bounds (valid when loaded)
-    bool loaded = false;
-    __device__ __forceinline__ void load_pending(const sweep_args<float>& a) {
-        if (!loaded && pend < a.n_chunks) {
-            plo = __ldg(a.chunk + pend);
-            phi = __ldg(a.chunk + pend + 1);
-            loaded = true;
-        }
-    }
-    __device__ __forceinline__ unsigned next(const sweep_args<float>& a) {
-        if (cur >= end) {
-            if (pend >= a.n_chunks) return a.n_items;
-            load_pending(a);
-            cur = plo;
-            end = phi;
-            loaded = false;
-            unsigned t = 0;
-            if ((threadIdx.x & 31u) == 0) t = atomicAdd(&a.ctl->ticket, 1u);
-            pend = __shfl_sync(kFull, t, 0);
-            return cur++;
-        }
-        const unsigned c = cur++;
-        if (cur >= end) load_pending(a);
-        return c;
-    }
-};
-
 template <int DIR, int K>
 __global__ void __launch_bounds__(kSweepThreads, 2) k_dw32(const sweep_args<float> a) {
     if (a.skip && *a.skip) return;
     const unsigned lane = threadIdx.x & 31u;
     chunk_claim cc;
-    {
-        unsigned t = 0;
-        if (lane == 0) t = atomicAdd(&a.ctl->ticket, 1u);
-        cc.pend = __shfl_sync(kFull, t, 0);
-    }
+    cc.start(a);
     stage_desc dD;
     load_desc(a, cc.next(a), dD);
     stage_wide<K> sL;
