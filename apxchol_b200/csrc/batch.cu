@@ -27,6 +27,11 @@ namespace {
 constexpr uint32_t kTile = 2048;   // rows per reduction tile
 constexpr int kBT = 256;           // threads per block of the vector kernels
 constexpr int kSd = 14;            // per-slot double arrays (bp::rz .. bp::tol)
+// SpMV rows longer than kLongRow nonzeros (power-law hubs) are cut into
+// chunks of kChunkNnz, each summed by one block; the row's chunks are then
+// added in order (deterministic). Other rows stay with the row kernels.
+constexpr uint32_t kLongRow = 128;
+constexpr uint32_t kChunkNnz = 512;
 
 enum fin_mode : int { kFinSpmv = 0, kFinXr = 1, kFinZsum = 2, kFinRz = 3, kFinResid = 4 };
 
@@ -38,6 +43,11 @@ struct bp {
     const unsigned* inst_t0; const unsigned* inst_t1;
     const unsigned* inst_off; const unsigned* inst_n; const int* inst_lap;
     const int32_t* a_ptr; const int32_t* a_idx; const double* a_val;
+    // long SpMV rows: long row i is lr_row[i], its chunks [lr_first[i], lr_first[i+1]);
+    // chunk c covers entries [ch_lo[c], ch_hi[c]); its partial sums go to ch_part[c][K]
+    const uint32_t* lr_row; const uint32_t* lr_first; const uint32_t* ch_lo; const uint32_t* ch_hi;
+    unsigned n_long, n_sp_chunks;
+    double* ch_part;
     const uint32_t* gperm;     // original (global) index -> permuted position
     const uint32_t* inst_of;   // original (global) index -> instance
     double *x, *r, *p, *Ap, *b;
@@ -156,8 +166,17 @@ __global__ void __launch_bounds__(kBT) k_b_spmv(bp P, const double* X, double* Y
 #pragma unroll
             for (int c = 0; c < K; ++c) acc[c] = 0.0;
             const int e = __ldg(P.a_ptr + row + 1);
+            const int b0 = __ldg(P.a_ptr + row);
+            if (static_cast<uint32_t>(e - b0) > kLongRow) {
+                // a long row: its sums were made by the chunk kernels
+                if (mode == 0)
+#pragma unroll
+                    for (int c = 0; c < K; ++c)
+                        part[c] = fma(X[static_cast<size_t>(row) * K + c], Y[static_cast<size_t>(row) * K + c], part[c]);
+                continue;
+            }
 #pragma unroll 2
-            for (int k = __ldg(P.a_ptr + row); k < e; ++k) {
+            for (int k = b0; k < e; ++k) {
                 const double w = __ldg(P.a_val + k);
                 const double* src = X + static_cast<size_t>(__ldg(P.a_idx + k)) * K;
                 if constexpr (K == 1) {
@@ -210,7 +229,18 @@ __global__ void __launch_bounds__(kBT, 4) k_b_spmv_pairs(bp P, const double* X, 
             double2 own = make_double2(0.0, 0.0);
             bool have_own = false;
             const int e = __ldg(P.a_ptr + row + 1);
-            for (int k0 = __ldg(P.a_ptr + row); k0 < e; k0 += kE) {
+            const int b0 = __ldg(P.a_ptr + row);
+            if (static_cast<uint32_t>(e - b0) > kLongRow) {
+                // a long row: its sums were made by the chunk kernels
+                const double2 y = *reinterpret_cast<const double2*>(Y + static_cast<size_t>(row) * K + c0);
+                if (mode == 0) {
+                    own = *reinterpret_cast<const double2*>(X + static_cast<size_t>(row) * K + c0);
+                    acc[0][0] = fma(own.x, y.x, acc[0][0]);
+                    acc[0][1] = fma(own.y, y.y, acc[0][1]);
+                }
+                continue;
+            }
+            for (int k0 = b0; k0 < e; k0 += kE) {
                 // indices and weights of the next kE nonzeros, then all their gathers, then the fmas
                 // in CSR order
                 unsigned col[kE];
@@ -238,6 +268,58 @@ __global__ void __launch_bounds__(kBT, 4) k_b_spmv_pairs(bp P, const double* X, 
             }
         }
         if (mode == 0) col_store<K, 1>(acc, P.partials + static_cast<size_t>(t) * K * 2);
+    }
+}
+
+// Long SpMV rows, step 1: every chunk's partial sums (one block per chunk). For
+// K >= 2 a thread holds a column pair and an entry lane; the entry lanes'
+// sums are added in lane order. For K == 1 a fixed block tree.
+template <int K>
+__global__ void __launch_bounds__(kBT) k_b_spmv_chunks(bp P, const double* X, int mode) {
+    if (*P.all_done && mode == 0) return;
+    __shared__ double red[2 * kBT];
+    for (unsigned ch = blockIdx.x; ch < P.n_sp_chunks; ch += gridDim.x) {
+        const uint32_t lo = P.ch_lo[ch], hi = P.ch_hi[ch];
+        double a0 = 0.0, a1 = 0.0;
+        if constexpr (K == 1) {
+            for (uint32_t q = lo + threadIdx.x; q < hi; q += kBT)
+                a0 = fma(__ldg(P.a_val + q), X[__ldg(P.a_idx + q)], a0);
+            double v[1] = {a0};
+            apxb::block_sum<1>(v, red);
+            if (threadIdx.x == 0) P.ch_part[ch] = v[0];
+        } else {
+            constexpr unsigned kLanes = 2 * kBT / K;   // entry lanes
+            const unsigned c0 = (2 * threadIdx.x) % K, el = (2 * threadIdx.x) / K;
+            for (uint32_t q = lo + el; q < hi; q += kLanes) {
+                const double w = __ldg(P.a_val + q);
+                const double2 v = *reinterpret_cast<const double2*>(X + static_cast<size_t>(__ldg(P.a_idx + q)) * K + c0);
+                a0 = fma(w, v.x, a0);
+                a1 = fma(w, v.y, a1);
+            }
+            red[2 * threadIdx.x] = a0;
+            red[2 * threadIdx.x + 1] = a1;
+            __syncthreads();
+            if (threadIdx.x < static_cast<unsigned>(K)) {
+                // column c: thread (lane * K/2 + c/2), component c % 2, lanes in order
+                const unsigned c = threadIdx.x;
+                double sum = 0.0;
+                for (unsigned l = 0; l < kLanes; ++l) sum += red[2 * (l * (K / 2) + c / 2) + (c & 1u)];
+                P.ch_part[static_cast<size_t>(ch) * K + c] = sum;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Long SpMV rows, step 2: each row's chunk sums in chunk order -> Y.
+template <int K>
+__global__ void __launch_bounds__(kBT) k_b_spmv_long(bp P, double* Y, int mode) {
+    if (*P.all_done && mode == 0) return;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n_long * K; i += gridDim.x * blockDim.x) {
+        const unsigned r = i / K, c = i % K;
+        double sum = 0.0;
+        for (uint32_t ch = P.lr_first[r]; ch < P.lr_first[r + 1]; ++ch) sum += P.ch_part[static_cast<size_t>(ch) * K + c];
+        Y[static_cast<size_t>(P.lr_row[r]) * K + c] = sum;
     }
 }
 
@@ -627,6 +709,10 @@ struct apxb_batch {
     // operator (combined, permuted) and permutation
     const int32_t *a_ptr = nullptr, *a_idx = nullptr;
     const double* a_val = nullptr;
+    // long SpMV rows (bp::lr_row ...)
+    uint32_t n_long = 0, n_sp_chunks = 0;
+    uint32_t *lr_row = nullptr, *lr_first = nullptr, *ch_lo = nullptr, *ch_hi = nullptr;
+    double* ch_part = nullptr;
     uint32_t* gperm = nullptr;
     uint32_t* inst_of = nullptr;
     // tiles
@@ -700,6 +786,8 @@ struct apxb_batch {
         P.tile_inst = tile_inst; P.tile_lo = tile_lo; P.tile_hi = tile_hi; P.inst_t0 = inst_t0; P.inst_t1 = inst_t1;
         P.inst_off = inst_off; P.inst_n = inst_n; P.inst_lap = inst_lap;
         P.a_ptr = a_ptr; P.a_idx = a_idx; P.a_val = a_val; P.gperm = gperm; P.inst_of = inst_of;
+        P.lr_row = lr_row; P.lr_first = lr_first; P.ch_lo = ch_lo; P.ch_hi = ch_hi;
+        P.n_long = n_long; P.n_sp_chunks = n_sp_chunks; P.ch_part = ch_part;
         P.x = x; P.r = r; P.p = p; P.Ap = Ap; P.b = b; P.rhs32 = rhs32; P.z = Zf;
         const size_t ns = slots();
         double* d = sd;
@@ -766,6 +854,10 @@ void batch_plan(const std::vector<const apxb_factor*>& fs, const std::vector<uin
 template <int K>
 int launch_iteration_k(apxb_batch* bt, const bp& P, cudaStream_t s, unsigned long long h, int use_cond) {
     const int g = bt->e->vec_grid;
+    if (bt->n_long) {
+        k_b_spmv_chunks<K><<<std::min<unsigned>(bt->n_sp_chunks, 4u * g), kBT, 0, s>>>(P, P.p, 0);
+        k_b_spmv_long<K><<<g, kBT, 0, s>>>(P, P.Ap, 0);
+    }
     if constexpr (K == 1) k_b_spmv<K><<<g, kBT, 0, s>>>(P, P.p, P.Ap, 0);
     else k_b_spmv_pairs<K><<<g, kBT, 0, s>>>(P, P.p, P.Ap, 0);
     k_b_fin<<<1, kFinThreads, 0, s>>>(P, kFinSpmv);
@@ -806,6 +898,10 @@ void launch_finish_k(apxb_batch* bt, const bp& P, double* X, bool resid, cudaStr
     k_b_xmean<<<1, kBT, 0, s>>>(P);
     k_b_out<K><<<g, kBT, 0, s>>>(P, X);
     if (resid) {
+        if (bt->n_long) {
+            k_b_spmv_chunks<K><<<std::min<unsigned>(bt->n_sp_chunks, 4u * g), kBT, 0, s>>>(P, P.x, 1);
+            k_b_spmv_long<K><<<g, kBT, 0, s>>>(P, P.Ap, 1);
+        }
         if constexpr (K == 1) k_b_spmv<K><<<g, kBT, 0, s>>>(P, P.x, P.Ap, 1);
         else k_b_spmv_pairs<K><<<g, kBT, 0, s>>>(P, P.x, P.Ap, 1);
         k_b_resid<K><<<g, kBT, 0, s>>>(P);
@@ -1006,6 +1102,32 @@ int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, a
         }
         APXB_CK(cudaMemcpy(ap, hp.data(), 4 * hp.size(), cudaMemcpyHostToDevice));
         bt->a_ptr = ap; bt->a_idx = ai; bt->a_val = av;
+    }
+    // ---- long SpMV rows ----
+    {
+        std::vector<int32_t> hp(bt->n_tot + 1);
+        APXB_CK(cudaMemcpy(hp.data(), bt->a_ptr, 4 * hp.size(), cudaMemcpyDeviceToHost));
+        std::vector<uint32_t> lrow, lfirst, clo, chi;
+        for (uint32_t r = 0; r < bt->n_tot; ++r) {
+            const uint32_t b0 = static_cast<uint32_t>(hp[r]), e0 = static_cast<uint32_t>(hp[r + 1]);
+            if (e0 - b0 <= kLongRow) continue;
+            lrow.push_back(r);
+            lfirst.push_back(static_cast<uint32_t>(clo.size()));
+            for (uint32_t q = b0; q < e0; q += kChunkNnz) { clo.push_back(q); chi.push_back(std::min(e0, q + kChunkNnz)); }
+        }
+        if (!lrow.empty()) {
+            lfirst.push_back(static_cast<uint32_t>(clo.size()));
+            bt->n_long = static_cast<uint32_t>(lrow.size());
+            bt->n_sp_chunks = static_cast<uint32_t>(clo.size());
+            if ((rc = bt->dalloc(&bt->lr_row, lrow.size())) || (rc = bt->dalloc(&bt->lr_first, lfirst.size())) ||
+                (rc = bt->dalloc(&bt->ch_lo, clo.size())) || (rc = bt->dalloc(&bt->ch_hi, chi.size())) ||
+                (rc = bt->dalloc(&bt->ch_part, static_cast<size_t>(clo.size()) * k)))
+                return rc;
+            APXB_CK(cudaMemcpy(bt->lr_row, lrow.data(), 4 * lrow.size(), cudaMemcpyHostToDevice));
+            APXB_CK(cudaMemcpy(bt->lr_first, lfirst.data(), 4 * lfirst.size(), cudaMemcpyHostToDevice));
+            APXB_CK(cudaMemcpy(bt->ch_lo, clo.data(), 4 * clo.size(), cudaMemcpyHostToDevice));
+            APXB_CK(cudaMemcpy(bt->ch_hi, chi.data(), 4 * chi.size(), cudaMemcpyHostToDevice));
+        }
     }
     // ---- permutation (permuted position -> original global index), tiles ----
     {

@@ -568,6 +568,32 @@ int apxb_operator_create(apxb_engine* e, uint32_t n, const int32_t* colptr, cons
     APXB_CK(cudaMemcpyAsync(a->idx, idx.data(), 4 * a->nnz, cudaMemcpyHostToDevice, s));
     APXB_CK(cudaMemcpyAsync(a->val, val.data(), 8 * a->nnz, cudaMemcpyHostToDevice, s));
     APXB_CK(cudaMemcpyAsync(a->perm, perm, 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s));
+    {   // long rows: cut into chunks summed by one block each (power-law hubs)
+        std::vector<uint32_t> lrow, lfirst, clo, chi;
+        for (uint32_t r = 0; r < n; ++r) {
+            const uint32_t b0 = static_cast<uint32_t>(ptr[r]), e0 = static_cast<uint32_t>(ptr[r + 1]);
+            if (e0 - b0 <= apxb::kLongRowPlain) continue;
+            lrow.push_back(r);
+            lfirst.push_back(static_cast<uint32_t>(clo.size()));
+            for (uint32_t q = b0; q < e0; q += apxb::kChunkNnzPlain) {
+                clo.push_back(q);
+                chi.push_back(std::min(e0, q + apxb::kChunkNnzPlain));
+            }
+        }
+        if (!lrow.empty()) {
+            lfirst.push_back(static_cast<uint32_t>(clo.size()));
+            a->n_long = static_cast<uint32_t>(lrow.size());
+            a->n_chunks = static_cast<uint32_t>(clo.size());
+            if ((rc = a->dalloc(&a->lr_row, lrow.size())) || (rc = a->dalloc(&a->lr_first, lfirst.size())) ||
+                (rc = a->dalloc(&a->ch_lo, clo.size())) || (rc = a->dalloc(&a->ch_hi, chi.size())) ||
+                (rc = a->dalloc(&a->ch_part, clo.size())))
+                return rc;
+            APXB_CK(cudaMemcpyAsync(a->lr_row, lrow.data(), 4 * lrow.size(), cudaMemcpyHostToDevice, s));
+            APXB_CK(cudaMemcpyAsync(a->lr_first, lfirst.data(), 4 * lfirst.size(), cudaMemcpyHostToDevice, s));
+            APXB_CK(cudaMemcpyAsync(a->ch_lo, clo.data(), 4 * clo.size(), cudaMemcpyHostToDevice, s));
+            APXB_CK(cudaMemcpyAsync(a->ch_hi, chi.data(), 4 * chi.size(), cudaMemcpyHostToDevice, s));
+        }
+    }
     APXB_CK(cudaStreamSynchronize(s));
     e->children++;
     *out = a.release();
@@ -630,6 +656,8 @@ apxb::pcg_ptrs pcg_ptrs_of(apxb_operator* a, apxb_factor* f) {
     // short row's gathers in flight together; long rows share lanes
     const double avg = a->n ? static_cast<double>(a->nnz) / a->n : 0.0;
     p.spmv_lanes = avg <= 16.0 ? 1 : (avg <= 64.0 ? 8 : 32);
+    p.lr_row = a->lr_row; p.lr_first = a->lr_first; p.ch_lo = a->ch_lo; p.ch_hi = a->ch_hi;
+    p.n_long = a->n_long; p.n_chunks = a->n_chunks; p.ch_part = a->ch_part;
     return p;
 }
 

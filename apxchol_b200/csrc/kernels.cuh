@@ -101,7 +101,14 @@ struct pcg_ptrs {
     unsigned n;
     int grid;
     int spmv_lanes;       // 1: a thread per row (short rows), else lanes per row
+    // rows longer than kLongRowPlain nonzeros: long row i is lr_row[i], its
+    // chunks [lr_first[i], lr_first[i+1]) cover entries [ch_lo[c], ch_hi[c])
+    const uint32_t* lr_row; const uint32_t* lr_first; const uint32_t* ch_lo; const uint32_t* ch_hi;
+    unsigned n_long, n_chunks;
+    double* ch_part;
 };
+constexpr uint32_t kLongRowPlain = 128;
+constexpr uint32_t kChunkNnzPlain = 512;
 
 void launch_pcg_init(const pcg_ptrs& p, cudaStream_t s);
 void launch_pcg_zsum(const pcg_ptrs& p, cudaStream_t s);

@@ -162,6 +162,10 @@ struct apxb_operator {
     int32_t *ptr = nullptr, *idx = nullptr;
     double* val = nullptr;
     uint32_t* perm = nullptr;
+    // SpMV rows longer than apxb::kLongRowPlain (see pcg_ptrs)
+    uint32_t n_long = 0, n_chunks = 0;
+    uint32_t *lr_row = nullptr, *lr_first = nullptr, *ch_lo = nullptr, *ch_hi = nullptr;
+    double* ch_part = nullptr;
     // PCG workspace (permuted ordering) + original-ordering staging
     double *x = nullptr, *r = nullptr, *p = nullptr, *Ap = nullptr, *b_orig = nullptr, *x_orig = nullptr;
     apxb::pcg_state* st = nullptr;

@@ -124,15 +124,19 @@ __global__ void __launch_bounds__(kThreads) k_pcg_spmv(pcg_ptrs p) {
     for (unsigned base = warp * kRowsPerWarp; base < p.n; base += nwarps * kRowsPerWarp) {
         const unsigned row = base + ((threadIdx.x & 31) / G);
         double s = 0.0;
+        bool is_long = false;
         if (row < p.n) {
             const int b = __ldg(p.a_ptr + row), e = __ldg(p.a_ptr + row + 1);
-            for (int k = b + static_cast<int>(lane); k < e; k += G)
-                s = fma(__ldg(p.a_val + k), p.p[__ldg(p.a_idx + k)], s);
+            is_long = static_cast<uint32_t>(e - b) > kLongRowPlain;   // summed by the chunk kernels
+            if (!is_long)
+                for (int k = b + static_cast<int>(lane); k < e; k += G)
+                    s = fma(__ldg(p.a_val + k), p.p[__ldg(p.a_idx + k)], s);
         }
 #pragma unroll
         for (int o = G / 2; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o, G);
         if (lane == 0 && row < p.n) {
-            p.Ap[row] = s;
+            if (is_long) s = p.Ap[row];
+            else p.Ap[row] = s;
             v[0] = fma(p.p[row], s, v[0]);
         }
     }
@@ -158,6 +162,10 @@ __global__ void __launch_bounds__(kThreads) k_pcg_spmv_rows(pcg_ptrs p) {
     double v[1] = {0.0};
     for (unsigned row = blockIdx.x * blockDim.x + threadIdx.x; row < p.n; row += gridDim.x * blockDim.x) {
         const int b = __ldg(p.a_ptr + row), e = __ldg(p.a_ptr + row + 1);
+        if (static_cast<uint32_t>(e - b) > kLongRowPlain) {   // summed by the chunk kernels
+            v[0] = fma(p.p[row], p.Ap[row], v[0]);
+            continue;
+        }
         double s = 0.0, own = 0.0;
         bool have_own = false;
         for (int k0 = b; k0 < e; k0 += kE) {
@@ -315,7 +323,36 @@ void launch_pcg_rz(const pcg_ptrs& p, cudaStream_t s) { k_pcg_rz<<<p.grid, kThre
 void launch_pcg_update_p(const pcg_ptrs& p, cudaStream_t s, unsigned long long h, int use_cond) {
     k_pcg_update_p<<<p.grid, kThreads, 0, s>>>(p, h, use_cond);
 }
+// Long rows: chunk sums (one block per chunk, fixed block tree), then each
+// row's chunks added in order into Ap.
+__global__ void __launch_bounds__(kThreads) k_pcg_spmv_chunks(pcg_ptrs p) {
+    if (stopped(p.st, p.err)) return;
+    __shared__ double red[32];
+    for (unsigned ch = blockIdx.x; ch < p.n_chunks; ch += gridDim.x) {
+        double a = 0.0;
+        for (uint32_t q = p.ch_lo[ch] + threadIdx.x; q < p.ch_hi[ch]; q += blockDim.x)
+            a = fma(__ldg(p.a_val + q), p.p[__ldg(p.a_idx + q)], a);
+        double v[1] = {a};
+        block_sum<1>(v, red);
+        if (threadIdx.x == 0) p.ch_part[ch] = v[0];
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_pcg_spmv_long(pcg_ptrs p) {
+    if (stopped(p.st, p.err)) return;
+    for (unsigned r = blockIdx.x * blockDim.x + threadIdx.x; r < p.n_long; r += gridDim.x * blockDim.x) {
+        double sum = 0.0;
+        for (uint32_t ch = p.lr_first[r]; ch < p.lr_first[r + 1]; ++ch) sum += p.ch_part[ch];
+        p.Ap[p.lr_row[r]] = sum;
+    }
+}
+
 void launch_pcg_spmv(const pcg_ptrs& p, cudaStream_t s) {
+    if (p.n_long) {
+        k_pcg_spmv_chunks<<<std::min<unsigned>(p.n_chunks, 4u * static_cast<unsigned>(p.grid)), kThreads, 0, s>>>(p);
+        k_pcg_spmv_long<<<p.grid, kThreads, 0, s>>>(p);
+    }
     if (p.spmv_lanes == 1) k_pcg_spmv_rows<<<p.grid, kThreads, 0, s>>>(p);
     else if (p.spmv_lanes == 8) k_pcg_spmv<8><<<p.grid, kThreads, 0, s>>>(p);
     else k_pcg_spmv<32><<<p.grid, kThreads, 0, s>>>(p);

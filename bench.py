@@ -477,6 +477,186 @@ def run_ours(args, rank, world, local_rank):
     return 0
 
 
+def _verify(A, B_rows, X_rows):
+    """Largest FP64 relative residual ||b - A x|| / ||b|| over the given columns."""
+    worst = 0.0
+    for b, x in zip(B_rows, X_rows):
+        worst = max(worst, float(np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b)))
+    return worst
+
+
+def run_rmat22(args, rank, world, local_rank):
+    """R-MAT scale-22 Laplacian: batched mixed precision (autotuned k), the plain
+    FP64 path, and one reference cpu_solver solve (iterations, time)."""
+    import torch
+    import oracle
+    from apxchol_b200 import autotune, gen, native, workloads
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    A, F = workloads.rmat_22(log)
+    n = A.n
+    rhs = lambda j: gen.rhs(n, 3000 + j, True)
+    eng = native.Engine(local_rank)
+    D32 = native.DeviceFactor(eng, F, precision=native.PREC_FP32)
+    Op = native.DeviceOperator(eng, A, F.perm)
+    ch = autotune.tune(eng, D32, Op, rhs, tol=TOL, max_iter=MAX_ITER, ks=(1, 4, 8, 16), grids=(0,), log=log)
+    k = ch.k
+    bt = native.Batch(eng, [D32], [Op], k)
+    B = np.stack([rhs(c) for c in range(k)])
+    Bf, nrhs = bt.pack([B])
+    dB = torch.from_numpy(Bf).to(dev)
+    dX = torch.empty_like(dB)
+    stream = torch.cuda.ExternalStream(eng.stream)
+    for _ in range(args.warmup):
+        bt.solve_raw(dB, dX, nrhs, tol=TOL, max_iter=MAX_ITER, flags=native.DEVICE_PTRS)
+    steps = max(1, min(args.steps, 5))
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(steps):
+        res = bt.solve_raw(dB, dX, nrhs, tol=TOL, max_iter=MAX_ITER, flags=native.DEVICE_PTRS)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    secs = ev0.elapsed_time(ev1) * 1e-3
+    X = dX.cpu().numpy()
+    tres = _verify(A, [B[c] for c in range(k)], [X[c * n:(c + 1) * n] for c in range(k)])
+    its = [res[c].iterations for c in range(k)]
+    bt.close(); D32.close()
+    D64 = native.DeviceFactor(eng, F, precision=native.PREC_FP64)
+    x64, r64 = native.pcg(eng, D64, Op, B[0], tol=TOL, max_iter=MAX_ITER)
+    _, r64 = native.pcg(eng, D64, Op, B[0], tol=TOL, max_iter=MAX_ITER)
+    tres64 = _verify(A, [B[0]], [x64])
+    D64.close(); Op.close(); eng.close()
+    ref = None
+    if oracle.ref_available():
+        oracle.set_threads(os.cpu_count() or 1)
+        xr, itr, _, sr = oracle.Ref(A, F).solve(B[0], TOL, MAX_ITER)
+        ref = {"iterations": int(itr), "seconds": sr, "solves_s": 1.0 / sr, "cores": os.cpu_count()}
+    line = {"metric": METRIC, "value": k * steps / secs, "unit": "solves/s", "n_gpus": world, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": secs / steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 sweeps / f64 outer", "data": "synthetic (seeded generator)",
+            "config": {"workload": "rmat_22 LCC Laplacian, batched mixed precision", "n": n, "nnz_A": int(A.nnz),
+                       "nnz_factor": int(F.nnz), "k": k, "tol": TOL},
+            "iterations": [min(its), max(its)], "true_relres_max": tres,
+            "plain_fp64": {"solves_s": 1.0 / r64.seconds, "iterations": r64.iterations, "true_relres": tres64},
+            "reference_cpu": ref,
+            "autotune": [{"k": t[0], "solves_s": t[2]} for t in ch.table]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_instances256(args, rank, world, local_rank):
+    """256 uneven SDDM instances in one batch (autotuned k)."""
+    import torch
+    from apxchol_b200 import autotune, gen, native, workloads
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    insts = workloads.instances_256(log)
+    eng = native.Engine(local_rank)
+    Ds = [native.DeviceFactor(eng, F, precision=native.PREC_FP32) for _, F, _ in insts]
+    Ops = [native.DeviceOperator(eng, A, F.perm) for A, F, _ in insts]
+    rhs = [np.stack([gen.rhs(A.n, 5000 + 10 * i + j, False) for j in range(c)]) for i, (A, F, c) in enumerate(insts)]
+    total = sum(r.shape[0] for r in rhs)
+    k, table = autotune.tune_instances(eng, Ds, Ops, rhs, tol=TOL, max_iter=MAX_ITER, log=log)
+    bt = native.Batch(eng, Ds, Ops, k)
+    cmax = max(r.shape[0] for r in rhs)
+    passes = []
+    for p0 in range(0, cmax, k):
+        part = [r[p0:p0 + k] if r.shape[0] > p0 else np.zeros((0, r.shape[1])) for r in rhs]
+        Bf, nrhs = bt.pack(part)
+        passes.append((torch.from_numpy(Bf).to(dev), nrhs, part))
+    dX = torch.empty_like(passes[0][0])
+    stream = torch.cuda.ExternalStream(eng.stream)
+    for _ in range(args.warmup):
+        for dB, nrhs, _ in passes:
+            bt.solve_raw(dB, dX, nrhs, tol=TOL, max_iter=MAX_ITER, flags=native.DEVICE_PTRS)
+    steps = max(1, min(args.steps, 5))
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(steps):
+        for dB, nrhs, _ in passes:
+            bt.solve_raw(dB, dX, nrhs, tol=TOL, max_iter=MAX_ITER, flags=native.DEVICE_PTRS)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    secs = ev0.elapsed_time(ev1) * 1e-3
+    worst, bad = 0.0, 0
+    for dB, nrhs, part in passes:
+        res = bt.solve_raw(dB, dX, nrhs, tol=TOL, max_iter=MAX_ITER, flags=native.DEVICE_PTRS | native.TRUE_RESIDUAL)
+        for i, q in enumerate(part):
+            for c in range(q.shape[0]):
+                r = res[i * k + c]
+                worst = max(worst, r.true_residual)
+                bad += r.status != 0
+    line = {"metric": METRIC, "value": total * steps / secs, "unit": "solves/s", "n_gpus": world, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": secs / steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 sweeps / f64 outer", "data": "synthetic (seeded generator)",
+            "config": {"workload": "instances_256: uneven SDDM instances in one batch", "instances": len(insts),
+                       "sum_n": int(sum(A.n for A, _, _ in insts)), "rhs": total, "k": k, "passes": len(passes),
+                       "tol": TOL},
+            "true_relres_max": worst, "not_converged": int(bad),
+            "autotune": [{"k": t[0], "solves_s": t[1]} for t in table]}
+    bt.close()
+    for o in Ops + Ds:
+        o.close()
+    eng.close()
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_serving8(args, rank, world, local_rank):
+    """8 resident matrices, open-loop Poisson requests at 50/200/800 req/s
+    (matrix uniform, tol from {1e-6, 1e-8, 1e-10}); two matrices are admitted
+    only when their first request arrives (60 GB budget)."""
+    import torch
+    from apxchol_b200 import gen, workloads
+    from apxchol_b200.serve import SolveServer, latency_stats
+    torch.cuda.set_device(local_rank)
+    mats = workloads.serving_8(log)
+    srv = SolveServer(device=local_rank, budget_bytes=60 * 10**9, k=8, iters_per_step=2, sweep_grid=args.sweep_grid)
+    rates = []
+    try:
+        for name, A, F in mats:
+            srv.register(name, A, F)
+        for name, A, F in mats[:6]:
+            srv.admit_matrix(name)
+            for j in range(8):
+                srv.submit(name, gen.rhs(A.n, 10 + j, not F.sddm), TOL)
+        srv.drain()
+        srv.completed.clear()
+        pools = {name: [gen.rhs(A.n, 100 + j, not F.sddm) for j in range(4)] for name, A, F in mats}
+        names = [nm for nm, _, _ in mats]
+        for rate, nreq in ((50, 400), (200, 1000), (800, 2400)):
+            rng = np.random.default_rng(rate)
+            t = np.cumsum(rng.exponential(1.0 / rate, size=nreq))
+            tols = (1e-6, 1e-8, 1e-10)
+            arrivals = [(float(t[j]), names[int(rng.integers(len(names)))], None, tols[int(rng.integers(3))])
+                        for j in range(nreq)]
+            arrivals = [(dt, nm, pools[nm][j % 4], tol) for j, (dt, nm, _, tol) in enumerate(arrivals)]
+            adm0 = srv.admissions
+            t0 = time.perf_counter()
+            done = srv.run_open_loop(arrivals)
+            wall = time.perf_counter() - t0
+            st = latency_stats(done)
+            rates.append({"rate_req_s": rate, "requests": len(done), "solves_s": len(done) / wall,
+                          "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "not_converged": sum(q.status != 0 for q in done),
+                          "matrix_admissions": srv.admissions - adm0})
+            log(f"[bench] serving_8 {rate} req/s: {len(done) / wall:.1f} solves/s, p50 {st['p50_ms']:.1f} ms, "
+                f"p99 {st['p99_ms']:.1f} ms")
+        resident_gb = srv.used_bytes() / 1e9
+    finally:
+        srv.close()
+    line = {"metric": METRIC, "value": rates[-1]["solves_s"], "unit": "solves/s", "n_gpus": world, "steps": len(rates),
+            "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 sweeps / f64 outer", "data": "synthetic (seeded generator)",
+            "config": {"workload": "serving_8: 8 matrices, Poisson arrivals", "k": 8, "budget_gb": 60,
+                       "sweep_grid": args.sweep_grid or "resident",
+                       "resident_gb": resident_gb},
+            "serving": rates}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -492,6 +672,8 @@ def main():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="grid3d_128", choices=["grid3d_128", "rmat_22", "instances_256", "serving_8"],
+                    help="grid3d_128 is the benchmark; the others measure the other workloads, one JSON line each")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -499,6 +681,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload != "grid3d_128":
+        fn = {"rmat_22": run_rmat22, "instances_256": run_instances256, "serving_8": run_serving8}[args.workload]
+        return fn(args, rank, world, local_rank)
     if world > 1:
         import datetime
         import torch

@@ -11,6 +11,7 @@ SPECS = {
     "grid3d_48": (lambda: gen.grid3d(48, seed=1), 1),                       # SDDM, high contrast
     "regular_3000": (lambda: gen.random_regular(3000, seed=3, shift=1e-3), 1),  # SDDM
     "rmat_12": (lambda: gen.rmat(12, seed=2), 2),                           # Laplacian, power law
+    "rmat_14": (lambda: gen.rmat(14, seed=2), 2),                           # Laplacian, one 3676-entry row
     "path_200": (lambda: gen.grid2d(200, 1, seed=5), 0),                    # Laplacian, a path
 }
 
