@@ -44,6 +44,7 @@ class Request:
     iterations: int = 0
     status: int = -1
     residual: float = float("nan")
+    error: str = ""                # why a request failed (its matrix could not be admitted)
 
     @property
     def latency(self) -> float:
@@ -114,15 +115,23 @@ class SolveServer:
     requests at their arrival times while serving."""
 
     def __init__(self, device: int = 0, budget_bytes: int = 60 * 10**9, k: int = 8, iters_per_step: int = 2,
-                 max_iter: int = 500, depth: int = 2, lanes: int = 1, sweep_grid: int = 0, copy_threads: int = 4):
+                 max_iter: int = 500, depth: int = 2, lanes: int = 1, sweep_grid: int | None = None,
+                 copy_threads: int = 4):
         self.device, self.budget, self.k = device, int(budget_bytes), k
-        self.n_lanes, self.sweep_grid = max(1, lanes), sweep_grid   # batches (streams) per matrix, their sweep grid
+        # batches (streams) per matrix, and the sweep grid of each: None = the
+        # resident grid divided among min(4, registered matrices x lanes), so the
+        # latency-bound sweeps of different matrices run side by side instead of
+        # each holding every SM; 0 = the resident grid; > 0 = that many blocks
+        self.n_lanes, self.sweep_grid = max(1, lanes), sweep_grid
         # host copies of right-hand sides into pinned staging and of solutions out of it run on
         # worker threads (numpy releases the GIL for bulk copies), off the pump loop
         self.pool = concurrent.futures.ThreadPoolExecutor(copy_threads) if copy_threads > 0 else None
         self.iters_per_step, self.max_iter = iters_per_step, max_iter
         self.depth = max(1, min(2, depth))      # steps kept queued per matrix (the batch keeps two state copies)
         self.resident: dict = {}
+        self.pending: dict = {}          # mid -> [future of its _Resident, reserved bytes, queued requests]
+        # matrices are built (host preparation, uploads) on a worker thread while the pump keeps serving
+        self.admitter = concurrent.futures.ThreadPoolExecutor(1)
         self.catalog: dict = {}          # mid -> (matrix, factor) that can be (re)admitted
         self.completed: list = []
         self.evictions = 0
@@ -139,13 +148,13 @@ class SolveServer:
         return self.n_lanes * estimate_bytes(mat.n, fac.nnz, mat.nnz, self.k)
 
     def used_bytes(self) -> int:
-        """Bytes reserved by resident matrices (each: the larger of its estimate and its measured use)."""
-        return sum(r.nbytes for r in self.resident.values())
+        """Bytes reserved by resident matrices (each: the larger of its estimate and its measured
+        use) and by matrices being admitted (their estimate)."""
+        return sum(r.nbytes for r in self.resident.values()) + sum(p[1] for p in self.pending.values())
 
-    def admit_matrix(self, mid):
-        if mid in self.resident:
-            return self.resident[mid]
-        mat, fac = self.catalog[mid]
+    def _reserve(self, mid) -> int:
+        """Make room for mid under the budget (evicting idle matrices, least
+        recently used first); returns the bytes reserved."""
         need = self.estimate(mid)
         while self.used_bytes() + need > self.budget:
             idle = [r for r in self.resident.values() if not r.busy()]
@@ -154,24 +163,60 @@ class SolveServer:
                                   "by busy matrices")
             victim = min(idle, key=lambda r: r.last_used)
             self.evict(victim.mid)
+        return need
+
+    def admit_matrix(self, mid):
+        """Admit a matrix now (waits for an admission already under way)."""
+        if mid in self.resident:
+            return self.resident[mid]
+        if mid in self.pending:
+            self.pending[mid][0].result()
+            self._collect_admissions()
+            return self.resident[mid]
+        need = self._reserve(mid)
+        r = self._build(mid, need, self.budget - self.used_bytes())
+        self.resident[mid] = r
+        self.admissions += 1
+        return r
+
+    def _build(self, mid, need: int, room: int) -> _Resident:
+        """The lanes of one matrix (engines, factor, operator, batch): room is
+        the device budget its engines may use."""
+        mat, fac = self.catalog[mid]
         import torch   # pinned host staging (page-locked buffers make the copies asynchronous)
         grid = self.sweep_grid
-        if grid <= 0 and self.n_lanes > 1:
-            grid = max(1, 2 * torch.cuda.get_device_properties(self.device).multi_processor_count // self.n_lanes)
+        if grid is None:
+            parts = min(4, max(1, len(self.catalog)) * self.n_lanes)
+            grid = 0 if parts == 1 else max(1, 2 * torch.cuda.get_device_properties(self.device).multi_processor_count
+                                                // parts)
         lanes = []
         try:
             for _ in range(self.n_lanes):
-                lanes.append(self._make_lane(mat, fac, grid, self.budget - self.used_bytes()
-                                             - sum(ln.eng.memory_used() for ln in lanes)))
+                lanes.append(self._make_lane(mat, fac, grid, room + need - sum(ln.eng.memory_used() for ln in lanes)))
         except Exception:
             for ln in lanes:
                 ln.close()
             raise
         used = sum(ln.eng.memory_used() for ln in lanes)
-        r = _Resident(mid=mid, n=mat.n, nbytes=max(need, used), lanes=lanes, last_used=time.perf_counter())
-        self.resident[mid] = r
-        self.admissions += 1
-        return r
+        return _Resident(mid=mid, n=mat.n, nbytes=max(need, used), lanes=lanes, last_used=time.perf_counter())
+
+    def _collect_admissions(self) -> bool:
+        """Make the matrices whose admission finished resident, with their queued requests."""
+        progressed = False
+        for mid in [m for m, p in self.pending.items() if p[0].done()]:
+            fut, need, queue = self.pending.pop(mid)
+            progressed = True
+            try:
+                r = fut.result()
+            except Exception as ex:   # the requests of a matrix that could not be admitted fail
+                for req in queue:
+                    req.status, req.finish, req.error = native.ERR_BUDGET, time.perf_counter(), str(ex)
+                    self.completed.append(req)
+                continue
+            r.queue.extend(queue)
+            self.resident[mid] = r
+            self.admissions += 1
+        return progressed
 
     def _make_lane(self, mat, fac, grid: int, budget: int) -> _Lane:
         import torch
@@ -211,8 +256,16 @@ class SolveServer:
         self._rid += 1
         req = Request(rid=self._rid, mid=mid, b=np.ascontiguousarray(b, np.float64), tol=tol,
                       arrival=time.perf_counter() if arrival is None else arrival)
-        r = self.admit_matrix(mid)
-        r.queue.append(req)
+        if mid in self.resident:
+            self.resident[mid].queue.append(req)
+        elif mid in self.pending:
+            self.pending[mid][2].append(req)
+        else:
+            # admission on a worker thread; the request waits in the admission's queue
+            need = self._reserve(mid)
+            room = self.budget - self.used_bytes()
+            self.pending[mid] = [self.admitter.submit(self._build, mid, need, room), need,
+                                 collections.deque([req])]
         return req
 
     def _run(self, fn, *args):
@@ -305,13 +358,13 @@ class SolveServer:
 
     def pump(self) -> bool:
         """Service every resident matrix once."""
-        any_progress = False
+        any_progress = self._collect_admissions()
         for r in list(self.resident.values()):
             any_progress |= self._service(r)
         return any_progress
 
     def idle(self) -> bool:
-        return not any(r.busy() for r in self.resident.values())
+        return not self.pending and not any(r.busy() for r in self.resident.values())
 
     def drain(self, timeout: float = 600.0):
         t0 = time.perf_counter()
@@ -339,6 +392,13 @@ class SolveServer:
         return self.completed[start_n:]
 
     def close(self):
+        for mid in list(self.pending):
+            try:
+                self.pending[mid][0].result()
+            except Exception:
+                pass
+        self._collect_admissions()
+        self.admitter.shutdown(wait=True)
         for mid in list(self.resident):
             self.resident.pop(mid).close()
         if self.pool is not None:

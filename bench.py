@@ -613,7 +613,8 @@ def run_serving8(args, rank, world, local_rank):
     from apxchol_b200.serve import SolveServer, latency_stats
     torch.cuda.set_device(local_rank)
     mats = workloads.serving_8(log)
-    srv = SolveServer(device=local_rank, budget_bytes=60 * 10**9, k=8, iters_per_step=2, sweep_grid=args.sweep_grid)
+    srv = SolveServer(device=local_rank, budget_bytes=60 * 10**9, k=8, iters_per_step=2,
+                      sweep_grid=args.sweep_grid or None)
     rates = []
     try:
         for name, A, F in mats:
@@ -650,7 +651,7 @@ def run_serving8(args, rank, world, local_rank):
             "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 sweeps / f64 outer", "data": "synthetic (seeded generator)",
             "config": {"workload": "serving_8: 8 matrices, Poisson arrivals", "k": 8, "budget_gb": 60,
-                       "sweep_grid": args.sweep_grid or "resident",
+                       "sweep_grid": args.sweep_grid or "auto (resident grid / 4)",
                        "resident_gb": resident_gb},
             "serving": rates}
     print(json.dumps(line), flush=True)
