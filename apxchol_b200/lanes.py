@@ -90,6 +90,27 @@ class Lanes:
             raise errs[0]
         return out
 
+    def each(self, fn):
+        """Run fn(i, lane) for every lane concurrently (one host thread per lane,
+        joined once at the end); returns the results in lane order."""
+        out = [None] * len(self.lanes)
+        errs = []
+
+        def run(i):
+            try:
+                out[i] = fn(i, self.lanes[i])
+            except Exception as ex:   # re-raised on the calling thread
+                errs.append(ex)
+
+        threads = [threading.Thread(target=run, args=(i,)) for i in range(len(self.lanes))]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        if errs:
+            raise errs[0]
+        return out
+
     def sweep_timed(self, reps: int = 10):
         """Every lane's forward and backward sweeps timed (CUDA events on its own
         stream) while all lanes run them concurrently: [(fwd s, bck s)] per lane."""

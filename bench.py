@@ -11,8 +11,10 @@ SpMV, residual, dots and centring. k and the sweep grid are picked by the
 autotuner (apxchol_b200/autotune.py) unless --k is given. Every step solves a
 fresh set of N(0,1) right-hand sides from a pool of distinct sets. The line
 reports:
-  * value      solves/s over K device-resident steps (CUDA events on the
-               engine stream).
+  * value      solves/s over K device-resident steps: every lane (a batch on
+               its own stream, apxchol_b200/lanes.py) solves K batches back to
+               back, the lanes joined once at the end; CUDA events on lane 0's
+               stream, which waits for every lane.
   * e2e        the same solves through the public C ABI (apxb_batch_solve)
                from pinned host buffers: B uploaded and X downloaded inside the
                timed region.
@@ -361,16 +363,27 @@ def run_ours(args, rank, world, local_rank):
             streams[0].wait_event(e)
         ev1.record(streams[0])
 
-    iters_timed = []
+    def lane_steps(flags, bufs, outs):
+        # each lane solves its `steps` batches back to back (lane j, step i: set (i * lanes + j));
+        # the lanes are joined once, at the end of the timed region
+        def run(j, lane):
+            its = []
+            for i in range(args.steps):
+                r = lane.batch.solve_raw(bufs[((i + 1) * nlanes + j) % POOL], outs[j], nrhs, tol=TOL,
+                                         max_iter=MAX_ITER, flags=flags)
+                its.append(max(x.iterations for x in r[:k]))
+            return its
+        return lanes.each(run)
+
+    dev_bufs = [s_[1] for s_ in sets]
     with ClockSampler(local_rank) as clk:
         barrier()
         open_region()
-        for i in range(args.steps):
-            r = step_dev(i + 1)
-            iters_timed.append(max(x.iterations for lane in r for x in lane[:k]))
+        per_lane = lane_steps(native.DEVICE_PTRS, dev_bufs, dXs)
         close_region()
         barrier()
     dev_s = ev0.elapsed_time(ev1) * 1e-3
+    iters_timed = [max(col) for col in zip(*per_lane)]
     # ---- e2e: pinned host buffers through the C ABI (apxb_batch_solve, one call per lane) ----
     hB = [torch.from_numpy(s[0]).pin_memory() for s in sets]
     hX = [torch.empty(n * k, dtype=torch.float64).pin_memory() for _ in range(nlanes)]
@@ -382,8 +395,7 @@ def run_ours(args, rank, world, local_rank):
     step_host(0)
     barrier()
     open_region()
-    for i in range(args.steps):
-        step_host(i + 1)
+    lane_steps(0, hB, hX)
     close_region()
     barrier()
     e2e_s = ev0.elapsed_time(ev1) * 1e-3
