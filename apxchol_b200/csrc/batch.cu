@@ -59,6 +59,8 @@ struct bp {
     unsigned long long* applies;
     int* all_done;
     int* any_center;           // some live slot centres its next preconditioner input
+    int* refresh_due;          // some live slot refreshes its residual this iteration
+    int refresh_every;         // a slot's residual is recomputed as b - A x every this many of its iterations (0: never)
     int max_iter, stag, center_k;
     double* partials;          // [n_tiles][K][2]
     apxb::dev_error* err;
@@ -157,6 +159,7 @@ __global__ void __launch_bounds__(kBT) k_b_admit(bp P, const double* B, const in
 template <int K>
 __global__ void __launch_bounds__(kBT) k_b_spmv(bp P, const double* X, double* Y, int mode) {
     if (*P.all_done && mode == 0) return;
+    if (mode == 2 && !*P.refresh_due) return;   // the residual refresh's A x, only when due
     for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
         double part[K];
 #pragma unroll
@@ -219,6 +222,7 @@ __global__ void __launch_bounds__(kBT) k_b_spmv(bp P, const double* X, double* Y
 template <int K>
 __global__ void __launch_bounds__(kBT, 4) k_b_spmv_pairs(bp P, const double* X, double* Y, int mode) {
     if (*P.all_done && mode == 0) return;
+    if (mode == 2 && !*P.refresh_due) return;   // the residual refresh's A x, only when due
     constexpr unsigned kRows = 2 * kBT / K;      // rows per pass of the block
     constexpr int kE = 4;                        // nonzeros whose gathers are in flight together
     const unsigned c0 = (2 * threadIdx.x) % K, rsub = (2 * threadIdx.x) / K;
@@ -277,6 +281,7 @@ __global__ void __launch_bounds__(kBT, 4) k_b_spmv_pairs(bp P, const double* X, 
 template <int K>
 __global__ void __launch_bounds__(kBT) k_b_spmv_chunks(bp P, const double* X, int mode) {
     if (*P.all_done && mode == 0) return;
+    if (mode == 2 && !*P.refresh_due) return;   // the residual refresh's A x, only when due
     __shared__ double red[2 * kBT];
     for (unsigned ch = blockIdx.x; ch < P.n_sp_chunks; ch += gridDim.x) {
         const uint32_t lo = P.ch_lo[ch], hi = P.ch_hi[ch];
@@ -315,11 +320,42 @@ __global__ void __launch_bounds__(kBT) k_b_spmv_chunks(bp P, const double* X, in
 template <int K>
 __global__ void __launch_bounds__(kBT) k_b_spmv_long(bp P, double* Y, int mode) {
     if (*P.all_done && mode == 0) return;
+    if (mode == 2 && !*P.refresh_due) return;   // the residual refresh's A x, only when due
     for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n_long * K; i += gridDim.x * blockDim.x) {
         const unsigned r = i / K, c = i % K;
         double sum = 0.0;
         for (uint32_t ch = P.lr_first[r]; ch < P.lr_first[r + 1]; ++ch) sum += P.ch_part[static_cast<size_t>(ch) * K + c];
         Y[static_cast<size_t>(P.lr_row[r]) * K + c] = sum;
+    }
+}
+
+// Whether slot sl refreshes its residual at the start of this iteration: every
+// refresh_every of its own completed iterations (so a slot's arithmetic does not
+// depend on the other slots).
+__device__ __forceinline__ bool refresh_slot(const bp& P, unsigned sl) {
+    const int it = P.iters[sl];
+    return P.refresh_every > 0 && !P.done[sl] && !P.fresh[sl] && it > 0 && it % P.refresh_every == 0;
+}
+
+// Periodic true-residual refresh (fp64): r = b - A x for the due slots, with A x
+// in Ap from the mode-2 SpMV just before. The iteration's x/r update then
+// continues from the recomputed residual.
+template <int K>
+__global__ void __launch_bounds__(kBT) k_b_refresh(bp P) {
+    if (!*P.refresh_due) return;
+    const int c0 = K == 1 ? 0 : static_cast<int>((2 * threadIdx.x) % K), c1 = K == 1 ? 0 : c0 + 1;
+    for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
+        const unsigned i = P.tile_inst[t];
+        const bool w0 = refresh_slot(P, i * K + c0), w1 = refresh_slot(P, i * K + c1);
+        if (!w0 && !w1) continue;
+        FLAT_PAIRS(t, {
+            if (two) {
+                if (w0) P.r[q] = P.b[q] - P.Ap[q];
+                if (w1) P.r[q + 1] = P.b[q + 1] - P.Ap[q + 1];
+            } else if (w0) {
+                P.r[q] = P.b[q] - P.Ap[q];
+            }
+        })
     }
 }
 
@@ -576,6 +612,12 @@ __global__ void __launch_bounds__(kFinThreads) k_b_fin(bp P, int mode) {
         }
     }
     __syncthreads();
+    if (mode == kFinRz) {   // the next iteration's residual refresh
+        for (unsigned sl = threadIdx.x; sl < nslots; sl += blockDim.x)
+            if (refresh_slot(P, sl)) any_cen = 1;
+        __syncthreads();
+        if (threadIdx.x == 0) *P.refresh_due = any_cen;
+    }
     if (mode == kFinXr || mode == kFinSpmv) {
         for (unsigned sl = threadIdx.x; sl < nslots; sl += blockDim.x)
             if (!P.done[sl]) {
@@ -726,7 +768,8 @@ struct apxb_batch {
     float *rhs32 = nullptr, *Yf = nullptr, *Zf = nullptr;
     bool y_armed = false;
     double* sd = nullptr;   // kSd double arrays of S*K
-    int* si = nullptr;      // 6 int arrays of S*K, all_done, any_center
+    int* si = nullptr;      // 6 int arrays of S*K, all_done, any_center, refresh_due
+    int refresh_every = 25; // periodic fp64 residual refresh (bp::refresh_every)
     unsigned long long* applies = nullptr;
     double* partials = nullptr;
     double* d_B = nullptr;  // staging of right-hand sides / solutions in the caller layout
@@ -796,7 +839,8 @@ struct apxb_batch {
         P.xmean = d + 11 * ns; P.tres = d + 12 * ns; P.tol = d + 13 * ns;
         int* s = si;
         P.iters = s; P.done = s + ns; P.status = s + 2 * ns; P.pmode = s + 3 * ns; P.center = s + 4 * ns;
-        P.fresh = s + 5 * ns; P.all_done = s + 6 * ns; P.any_center = s + 6 * ns + 1;
+        P.fresh = s + 5 * ns; P.all_done = s + 6 * ns; P.any_center = s + 6 * ns + 1; P.refresh_due = s + 6 * ns + 2;
+        P.refresh_every = refresh_every;
         P.applies = applies;
         P.max_iter = max_iter; P.stag = 50; P.center_k = e->center_k;
         P.partials = partials; P.err = e->d_err;
@@ -854,6 +898,15 @@ void batch_plan(const std::vector<const apxb_factor*>& fs, const std::vector<uin
 template <int K>
 int launch_iteration_k(apxb_batch* bt, const bp& P, cudaStream_t s, unsigned long long h, int use_cond) {
     const int g = bt->e->vec_grid;
+    if (bt->refresh_every > 0) {   // r = b - A x for the slots due (every launch exits at once otherwise)
+        if (bt->n_long) {
+            k_b_spmv_chunks<K><<<std::min<unsigned>(bt->n_sp_chunks, 4u * g), kBT, 0, s>>>(P, P.x, 2);
+            k_b_spmv_long<K><<<g, kBT, 0, s>>>(P, P.Ap, 2);
+        }
+        if constexpr (K == 1) k_b_spmv<K><<<g, kBT, 0, s>>>(P, P.x, P.Ap, 2);
+        else k_b_spmv_pairs<K><<<g, kBT, 0, s>>>(P, P.x, P.Ap, 2);
+        k_b_refresh<K><<<g, kBT, 0, s>>>(P);
+    }
     if (bt->n_long) {
         k_b_spmv_chunks<K><<<std::min<unsigned>(bt->n_sp_chunks, 4u * g), kBT, 0, s>>>(P, P.p, 0);
         k_b_spmv_long<K><<<g, kBT, 0, s>>>(P, P.Ap, 0);
@@ -1167,7 +1220,7 @@ int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, a
     if ((rc = bt->dalloc(&bt->x, nk)) || (rc = bt->dalloc(&bt->r, nk)) || (rc = bt->dalloc(&bt->p, nk)) ||
         (rc = bt->dalloc(&bt->Ap, nk)) || (rc = bt->dalloc(&bt->b, nk)) || (rc = bt->dalloc(&bt->rhs32, nk)) ||
         (rc = bt->dalloc(&bt->Yf, nk)) || (rc = bt->dalloc(&bt->Zf, nk)) || (rc = bt->dalloc(&bt->sd, kSd * ns)) ||
-        (rc = bt->dalloc(&bt->si, 6 * ns + 2)) || (rc = bt->dalloc(&bt->applies, ns)) ||
+        (rc = bt->dalloc(&bt->si, 6 * ns + 3)) || (rc = bt->dalloc(&bt->applies, ns)) ||
         (rc = bt->dalloc(&bt->partials, static_cast<size_t>(bt->n_tiles) * k * 2)) || (rc = bt->dalloc(&bt->d_B, nk)))
         return rc;
     APXB_CK(cudaMallocHost(&bt->h_sd, sizeof(double) * kSd * ns));
@@ -1176,7 +1229,7 @@ int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, a
     std::fill(bt->h_si, bt->h_si + 6 * ns + 1, 0);
     std::fill(bt->h_si + ns, bt->h_si + 2 * ns, 1);   // host mirror of the idle state below
     APXB_CK(cudaMemsetAsync(bt->sd, 0, sizeof(double) * kSd * ns, s));
-    APXB_CK(cudaMemsetAsync(bt->si, 0, sizeof(int) * (6 * ns + 2), s));
+    APXB_CK(cudaMemsetAsync(bt->si, 0, sizeof(int) * (6 * ns + 3), s));
     {   // every slot starts idle: done, and the batch all done
         std::vector<int> idle(ns + 1, 1);
         APXB_CK(cudaMemcpyAsync(bt->si + ns, idle.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, s));
@@ -1259,6 +1312,7 @@ int apxb_batch_solve(apxb_batch* bt, const double* B, double* X, const int* nrhs
     APXB_CK(cudaMemsetAsync(P.done, 0, sizeof(int) * ns, s));
     APXB_CK(cudaMemcpyAsync(P.fresh, ones.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, s));
     APXB_CK(cudaMemsetAsync(P.all_done, 0, sizeof(int), s));
+    APXB_CK(cudaMemsetAsync(P.refresh_due, 0, sizeof(int), s));
     // Only the forward output needs its markers now: the forward sweep re-arms
     // every factor row of Zf itself, and Zf's grounded rows must stay 0.
     if (!bt->y_armed) apxb::launch_fill_sent32(bt->Yf, nk, s);
@@ -1328,6 +1382,21 @@ int apxb_batch_plan_host(uint32_t n, const uint32_t* colptr, const uint32_t* row
         n_items[dir] = pl.n_items;
         n_chunks[dir] = static_cast<uint32_t>(pl.chunk.size() - 1);
     }
+    return APXB_OK;
+}
+
+int apxb_batch_set_refresh(apxb_batch* bt, int every) {
+    if (!bt || every < 0) return fail(APXB_ERR_INVALID, "bad argument");
+    for (char busy : bt->slot_busy)
+        if (busy) return fail(APXB_ERR_BUSY, "slots are admitted");
+    if (every == bt->refresh_every) return APXB_OK;
+    APXB_CK(cudaSetDevice(bt->e->device));
+    APXB_CK(cudaStreamSynchronize(bt->e->stream));
+    bt->refresh_every = every;
+    // the iteration graphs hold the refresh launches: rebuild them on next use
+    if (bt->loop) { cudaGraphExecDestroy(bt->loop); bt->loop = nullptr; }
+    if (bt->one) { cudaGraphExecDestroy(bt->one); bt->one = nullptr; }
+    bt->graph_max = -1;
     return APXB_OK;
 }
 

@@ -84,6 +84,7 @@ _SIGS = {
     "apxb_batch_destroy": (ctypes.c_int, [c_p]),
     "apxb_batch_size": (ctypes.c_int, [c_p, c_p, c_p, c_p]),
     "apxb_batch_solve": (ctypes.c_int, [c_p, c_p, c_p, c_p, ctypes.c_double, ctypes.c_int, ctypes.c_int, c_p]),
+    "apxb_batch_set_refresh": (ctypes.c_int, [c_p, ctypes.c_int]),
     "apxb_batch_admit": (ctypes.c_int, [c_p, ctypes.c_int, c_p, ctypes.c_double, ctypes.c_int, ctypes.c_int]),
     "apxb_batch_step": (ctypes.c_int, [c_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]),
     "apxb_batch_query": (ctypes.c_int, [c_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int)]),
@@ -389,6 +390,10 @@ class Batch:
         res = (PcgResult * (self.S * self.k))()
         check(self.lib.apxb_batch_solve(self.h, ptr(B), ptr(X), ptr(nrhs), tol, max_iter, flags, res))
         return res
+
+    def set_refresh(self, every: int):
+        """Recompute a slot's residual as b - A x (fp64) every `every` of its iterations (0: never)."""
+        check(self.lib.apxb_batch_set_refresh(self.h, every))
 
     # -- continuous batching (every call enqueues and returns) --
     def admit(self, slot: int, b, tol: float = 1e-8, max_iter: int = 500, device_ptrs: bool = False):

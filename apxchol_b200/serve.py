@@ -116,13 +116,14 @@ class SolveServer:
 
     def __init__(self, device: int = 0, budget_bytes: int = 60 * 10**9, k: int = 8, iters_per_step: int = 2,
                  max_iter: int = 500, depth: int = 2, lanes: int = 1, sweep_grid: int | None = None,
-                 copy_threads: int = 4):
+                 copy_threads: int = 4, refresh_every: int | None = None):
         self.device, self.budget, self.k = device, int(budget_bytes), k
         # batches (streams) per matrix, and the sweep grid of each: None = the
         # resident grid divided among min(4, registered matrices x lanes), so the
         # latency-bound sweeps of different matrices run side by side instead of
         # each holding every SM; 0 = the resident grid; > 0 = that many blocks
         self.n_lanes, self.sweep_grid = max(1, lanes), sweep_grid
+        self.refresh_every = refresh_every   # fp64 residual refresh period (None: the library default)
         # host copies of right-hand sides into pinned staging and of solutions out of it run on
         # worker threads (numpy releases the GIL for bulk copies), off the pump loop
         self.pool = concurrent.futures.ThreadPoolExecutor(copy_threads) if copy_threads > 0 else None
@@ -228,6 +229,8 @@ class SolveServer:
             f = native.DeviceFactor(eng, fac, precision=native.PREC_FP32)
             op = native.DeviceOperator(eng, mat, fac.perm)
             bt = native.Batch(eng, [f], [op], self.k)
+            if self.refresh_every is not None:
+                bt.set_refresh(self.refresh_every)
         except native.ApxbError as ex:
             for o in (op, f, eng):
                 if o is not None:

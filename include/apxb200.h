@@ -197,6 +197,12 @@ int apxb_batch_size(const apxb_batch* b, int* n_inst, int* k, uint32_t* n_total)
  * APXB_TRUE_RESIDUAL. */
 int apxb_batch_solve(apxb_batch* b, const double* B, double* X, const int* nrhs, double tol, int max_iter,
                      int flags, apxb_pcg_result* res);
+/* Periodic true-residual refresh (fp64): every `every` iterations of a slot
+ * (its own count, so a slot's arithmetic does not depend on the other
+ * slots) its residual is recomputed as b - A x before the x/r update, which
+ * keeps the fp64 recurrence from drifting away from the true residual. Default
+ * 25; 0 turns it off. Only while no slot is admitted (else APXB_ERR_BUSY). */
+int apxb_batch_set_refresh(apxb_batch* b, int every);
 
 /* Host-only (no GPU): builds and checks the batch sweep plans apxb_batch_create
  * would build for this factor and k (column lanes, oldest-dependency-first

@@ -179,3 +179,21 @@ def test_long_operator_rows(eng, k):
         assert r1[0][c].status == 0 and r1[0][c].true_residual < TRUE_RES_FACTOR * TOL
         xo, ito, _ = O.solve(B[c], TOL, 500)
         assert np.linalg.norm(x1[0][c] - xo) <= 1e-6 * np.linalg.norm(xo)
+
+
+@pytest.mark.parametrize("every", [0, 3])
+def test_residual_refresh(eng, every):
+    """The periodic fp64 residual refresh (r = b - A x every `every` iterations of
+    a slot) keeps convergence and accuracy, and repeats bit for bit."""
+    A, F, D, Op = _objs(eng, "grid3d_24")
+    bt = native.Batch(eng, [D], [Op], 4)
+    bt.set_refresh(every)
+    B = np.stack([gen.rhs(A.n, 400 + c, False) for c in range(4)])
+    x1, r1 = bt.solve([B], tol=TOL)
+    x2, r2 = bt.solve([B], tol=TOL)
+    assert np.array_equal(x1[0], x2[0])
+    O = oracle.Oracle(A, F, nt=8)
+    for c in range(4):
+        assert r1[0][c].status == 0 and r1[0][c].true_residual < TRUE_RES_FACTOR * TOL
+        xo, ito, _ = O.solve(B[c], TOL, 500)
+        assert np.linalg.norm(x1[0][c] - xo) <= 1e-6 * np.linalg.norm(xo)

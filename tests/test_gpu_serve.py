@@ -23,13 +23,15 @@ def cuda():
     torch.cuda.init()
 
 
-def _alone(mat, fac, b, tol):
+def _alone(mat, fac, b, tol, refresh=None):
     """The same right-hand side solved by itself (one slot of a fresh batch)."""
     eng = native.Engine(0)
     try:
         D = native.DeviceFactor(eng, fac, precision=native.PREC_FP32)
         Op = native.DeviceOperator(eng, mat, fac.perm)
         bt = native.Batch(eng, [D], [Op], K)
+        if refresh is not None:
+            bt.set_refresh(refresh)
         xs, res = bt.solve([b[None, :]], tol=tol)
         out = xs[0][0].copy(), res[0][0]
         bt.close(); Op.close(); D.close()
@@ -38,10 +40,12 @@ def _alone(mat, fac, b, tol):
         eng.close()
 
 
-@pytest.mark.parametrize("lanes", [1, 2])
-def test_results_equal_alone_and_in_the_mix(lanes):
+@pytest.mark.parametrize("lanes,refresh", [(1, None), (2, None), (1, 3)])
+def test_results_equal_alone_and_in_the_mix(lanes, refresh):
+    """refresh = 3: the periodic fp64 residual refresh runs every 3 iterations of
+    each slot, at different batch iterations for different slots."""
     mats = {"g2": problem("grid2d_64"), "g3": problem("grid3d_24"), "rr": problem("regular_3000")}
-    srv = SolveServer(k=K, iters_per_step=3, lanes=lanes)
+    srv = SolveServer(k=K, iters_per_step=3, lanes=lanes, refresh_every=refresh)
     try:
         for mid, (A, F) in mats.items():
             srv.register(mid, A, F)
@@ -60,7 +64,7 @@ def test_results_equal_alone_and_in_the_mix(lanes):
         assert len(srv.completed) == len(order)
         for req in reqs:
             A, F = mats[req.mid]
-            x_alone, r_alone = _alone(A, F, req.b, req.tol)
+            x_alone, r_alone = _alone(A, F, req.b, req.tol, refresh)
             assert req.status == 0, (req.mid, req.status)
             assert np.array_equal(req.x, x_alone), req.rid
             assert req.iterations == r_alone.iterations
