@@ -182,7 +182,7 @@ def from_rank0(values, world: int, device):
     return [float(v) for v in t.cpu()]
 
 
-def cpu_baseline(A, F, b, samples: int = 3):
+def cpu_baseline(A, F, b, samples: int = 12):
     """The reference cpu_solver on this host (bounded sample of solves)."""
     import oracle
     if not oracle.ref_available():

@@ -97,3 +97,20 @@ def test_batch_plans_hold_their_invariants(name, k):
     for items, chunks in ((fi, fc), (bi, bc)):
         assert m / rows_per_item_max <= items <= m
         assert 1 <= chunks <= items
+
+
+def test_factor_file_round_trip(tmp_path):
+    """A saved factor loads back field for field and prepares to the same arrays."""
+    from apxchol_b200.factor_io import load_factor, save_factor
+    A, F = problem("grid3d_24")
+    save_factor(tmp_path / "f.npz", F)
+    G = load_factor(tmp_path / "f.npz")
+    assert G.n == F.n and G.sddm == F.sddm and G.lumped == F.lumped
+    for name in ("colptr", "rowidx", "vals", "perm", "rounds"):
+        assert np.array_equal(getattr(G, name), getattr(F, name)), name
+    a, b = native.prepare_host(F), native.prepare_host(G)
+    for key in ("csr_ptr", "csr_idx", "csr_val", "csc_val"):
+        assert np.array_equal(a[key], b[key])
+    np.savez(tmp_path / "bad.npz", format=np.array("something else"))
+    with pytest.raises(ValueError):
+        load_factor(tmp_path / "bad.npz")
