@@ -28,7 +28,8 @@ reports:
                (nnz_s*8 + 4(m+1) + 2*m*4*k) / measured sweep time, against the
                measured HBM copy bandwidth. iter_frac: the factor + matrix bytes
                of one PCG iteration (460 MB at 128^3) over the batch's time per
-               iteration.
+               iteration; iter_all_frac: all the iteration's algorithmic bytes
+               (factor, matrix and every vector pass) over that time.
   * cpu_baseline  the reference's own cpu_solver (oracle/_ref) on the host cores.
 Inputs exceed L2 (factor + operator > 400 MB per iteration), so no flush is needed.
 
@@ -413,6 +414,14 @@ def run_ours(args, rank, world, local_rank):
     b_iter *= nlanes   # every lane reads the factor and the matrix once per iteration
     iter_s = dev_s / max(1, sum(iters_timed))
     iter_gbs = b_iter / iter_s / 1e9
+    # all algorithmic traffic of one batched iteration (every vector pass the kernels make), per lane:
+    # SpMV (A, p gathered once, Ap written), x/r update (x, p, r, Ap read; x, r written; fp32 input
+    # written), two sweeps (factor, input read, output and re-armed buffer written), r.z, p update
+    v8, v4 = 8 * n * k, 4 * n * k
+    b_all = (A.nnz * 12 + 4 * (n + 1) + 2 * v8) + (6 * v8 + v4) + \
+        2 * (nnz_s * 8 + 4 * (m + 1) + 3 * v4) + (v8 + v4) + (v4 + 2 * v8)
+    b_all *= nlanes
+    iter_all_gbs = b_all / iter_s / 1e9
     dev_s, e2e_s = max_over_ranks([dev_s, e2e_s], world, dev)
     lanes.close()
 
@@ -454,7 +463,9 @@ def run_ours(args, rank, world, local_rank):
         eng.close()
         return 0
     mean_its = sum(iters_timed) / max(1, len(iters_timed))
-    launches_per_step = nlanes * (1 + 12 * (mean_its + 1) + 3)
+    # per batched solve: admit; per iteration 12 kernels plus the residual refresh's SpMV and update
+    # (on by default; no long rows here); x out
+    launches_per_step = nlanes * (1 + 14 * (mean_its + 1) + 3)
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_s / args.steps * 1e3,
@@ -471,7 +482,8 @@ def run_ours(args, rank, world, local_rank):
                      "kernel": f"k_dw32<DIR,{k}> (batched fp32 sweep, {k} RHS, {nlanes} concurrent lane(s), "
                                f"{grid} blocks each)",
                      "bytes_per_launch": sweep_bytes, "fwd_us": fwd_s * 1e6, "bck_us": bck_s * 1e6,
-                     "peak_kind": peak_kind, "iter_bytes": b_iter, "iter_gbs": iter_gbs, "iter_frac": iter_gbs / peak},
+                     "peak_kind": peak_kind, "iter_bytes": b_iter, "iter_gbs": iter_gbs, "iter_frac": iter_gbs / peak,
+                     "iter_all_bytes": b_all, "iter_all_gbs": iter_all_gbs, "iter_all_frac": iter_all_gbs / peak},
         "plain_fp64": plain,
         "speedup_vs_plain_fp64": (value / world) / plain["solves_s"] if plain else None,
         "serving": serving,
