@@ -19,6 +19,7 @@
 //  * The iteration is a CUDA graph; a full solve runs it under a conditional
 //    WHILE node until every slot is done.
 #include <algorithm>
+#include <thread>
 
 #include "objects.hpp"
 
@@ -1099,18 +1100,25 @@ int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, a
     cudaStream_t s = e->stream;
     const size_t nk = static_cast<size_t>(bt->n_tot) * k, ns = bt->slots();
     int rc;
-    // ---- sweep plans (batch plans for this k) ----
+    // ---- sweep plans (batch plans for this k; the two directions on two threads) ----
     {
         const uint32_t col_lanes = k >= 8 ? static_cast<uint32_t>(k / 4) : 1u;
+        apxb::sweep_plan plans[2];
+        std::string bad[2];
+        {
+            auto make = [&](int dir) {
+                batch_plan(fs, bt->off, dir, col_lanes, plans[dir]);
+                if (n_inst == 1)
+                    bad[dir] = apxb::check_batch_plan(fs[0]->h.m, dir == 0 ? fs[0]->h.fwd_level : fs[0]->h.bck_level,
+                                                      plans[dir], col_lanes);
+            };
+            std::thread bck(make, 1);
+            make(0);
+            bck.join();
+        }
         for (int dir = 0; dir < 2; ++dir) {
-            apxb::sweep_plan pl;
-            batch_plan(fs, bt->off, dir, col_lanes, pl);
-            if (n_inst == 1) {
-                const std::string bad = apxb::check_batch_plan(fs[0]->h.m, dir == 0 ? fs[0]->h.fwd_level
-                                                                                    : fs[0]->h.bck_level,
-                                                               pl, col_lanes);
-                if (!bad.empty()) return fail(APXB_ERR_INVALID, "internal batch plan error: " + bad);
-            }
+            const apxb::sweep_plan& pl = plans[dir];
+            if (!bad[dir].empty()) return fail(APXB_ERR_INVALID, "internal batch plan error: " + bad[dir]);
             uint32_t *info, *ord, *ptr, *idx, *chunk;
             float* val;
             if ((rc = bt->dalloc(&info, pl.info.size())) || (rc = bt->dalloc(&ord, pl.ord.size())) ||

@@ -4,7 +4,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <chrono>
+#include <cstdio>
 #include <numeric>
+#include <thread>
 
 namespace apxb {
 
@@ -199,6 +202,58 @@ std::string check_plan(uint32_t m, const std::vector<int32_t>& level, const swee
     return {};
 }
 
+// Threads for a pass over `work` items: 1 below a million, else up to 8.
+// APXB_PREP_THREADS=T (1..64) sets T whatever the size, so that tests can
+// compare the threaded passes with the serial ones on small inputs.
+unsigned prep_threads(uint64_t work) {
+    if (const char* e = std::getenv("APXB_PREP_THREADS")) {
+        const long t = std::strtol(e, nullptr, 10);
+        if (t >= 1 && t <= 64) return static_cast<unsigned>(t);
+    }
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    return work < (1u << 20) ? 1u : std::min(8u, hw);
+}
+
+// body(t) for t in [0, T), t = 0 on the calling thread.
+template <class F>
+void run_threads(unsigned T, F&& body) {
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < T; ++t) th.emplace_back(body, t);
+    body(0u);
+    for (auto& x : th) x.join();
+}
+
+// Column ranges of T threads with about equal entry counts: [jb[t], jb[t+1]).
+template <class P>
+std::vector<uint32_t> column_ranges(const P* ptr, uint32_t cols, unsigned T) {
+    std::vector<uint32_t> jb(T + 1, cols);
+    jb[0] = 0;
+    const uint64_t total = ptr[cols] - ptr[0];
+    for (unsigned t = 1; t < T; ++t) {
+        const uint64_t target = ptr[0] + total * t / T;
+        jb[t] = static_cast<uint32_t>(std::lower_bound(ptr, ptr + cols, target) - ptr);
+        jb[t] = std::max(jb[t], jb[t - 1]);
+    }
+    return jb;
+}
+
+// APXB_PREP_TRACE=1: the time of each preparation stage on stderr.
+struct stage_clock {
+    bool on = false;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    stage_clock() {
+        const char* e = std::getenv("APXB_PREP_TRACE");
+        on = e && *e && *e != '0';
+    }
+    void mark(const char* what) {
+        if (!on) return;
+        const auto t = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "[apxb prep] %-22s %8.2f ms\n", what,
+                     std::chrono::duration<double, std::milli>(t - t0).count());
+        t0 = t;
+    }
+};
+
 void level_bits(const std::vector<int32_t>& level, int32_t n_levels, std::vector<uint32_t>& bits) {
     std::vector<uint32_t> cnt(static_cast<size_t>(n_levels) + 1, 0);
     for (int32_t l : level) cnt[l]++;
@@ -341,6 +396,7 @@ std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* r
     out.n = n; out.m = m; out.sddm = sddm;
     const double rel = drop_rel < 0.0 ? kDropRelDefault : drop_rel;
 
+    stage_clock clk;
     // Validate the storage contract: colptr monotone, each column starts
     // with its diagonal, rows strictly ascending and < n.
     if (colptr[0] != 0) return "colptr[0] != 0";
@@ -355,6 +411,7 @@ std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* r
             return "column " + std::to_string(j) + " has a non-positive or non-finite diagonal";
     }
 
+    clk.mark("validate");
     // L11 (drop row n-1 for a Laplacian), then the compacting drop, written
     // straight into the CSC arrays.
     std::vector<uint32_t>& cp = out.csc_ptr;
@@ -403,23 +460,44 @@ std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* r
     out.nnz_stored = ci.size();
     out.dropped = dropped;
 
-    // CSR by the column-order scatter: columns ascend within each row.
+    clk.mark("L11 + drop");
+    // CSR by the column-order scatter: columns ascend within each row. On T
+    // threads: thread t owns a range of columns (equal entry counts), counts
+    // its entries per row, and scatters them at per-row offsets that follow the
+    // ranges of threads 0..t-1 -- the same arrays the serial scatter makes.
     const uint64_t nnz = ci.size();
     out.csr_ptr.assign(static_cast<size_t>(m) + 1, 0);
-    for (uint64_t p = 0; p < nnz; ++p) out.csr_ptr[ci[p] + 1]++;
-    for (uint32_t i = 0; i < m; ++i) out.csr_ptr[i + 1] += out.csr_ptr[i];
     out.csr_idx.resize(nnz);
     out.csr_val.resize(nnz);
     {
-        std::vector<uint32_t> cur(out.csr_ptr.begin(), out.csr_ptr.end() - 1);
-        for (uint32_t j = 0; j < m; ++j)
-            for (uint32_t p = cp[j]; p < cp[j + 1]; ++p) {
-                const uint32_t slot = cur[ci[p]]++;
-                out.csr_idx[slot] = j;
-                out.csr_val[slot] = cv[p];
+        const unsigned T = prep_threads(nnz);
+        const std::vector<uint32_t> jb = column_ranges(cp.data(), m, T);
+        std::vector<std::vector<uint32_t>> cnt(T, std::vector<uint32_t>(m, 0));
+        run_threads(T, [&](unsigned t) {
+            for (uint32_t p = cp[jb[t]]; p < cp[jb[t + 1]]; ++p) cnt[t][ci[p]]++;
+        });
+        // row starts, then each thread's offset inside every row
+        for (uint32_t i = 0; i < m; ++i) {
+            uint32_t acc = out.csr_ptr[i];
+            for (unsigned t = 0; t < T; ++t) {
+                const uint32_t c = cnt[t][i];
+                cnt[t][i] = acc;
+                acc += c;
             }
+            out.csr_ptr[i + 1] = acc;
+        }
+        run_threads(T, [&](unsigned t) {
+            std::vector<uint32_t>& cur = cnt[t];
+            for (uint32_t j = jb[t]; j < jb[t + 1]; ++j)
+                for (uint32_t p = cp[j]; p < cp[j + 1]; ++p) {
+                    const uint32_t slot = cur[ci[p]]++;
+                    out.csr_idx[slot] = j;
+                    out.csr_val[slot] = cv[p];
+                }
+        });
     }
 
+    clk.mark("transpose");
     // Levels: round-as-level when the round bounds fit (omp.h:880-932), with
     // the bounds built as apx_cholesky::install_factor does
     // (preconditioner.h:247-258); else topological depths.
@@ -471,17 +549,26 @@ std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* r
     }
     level_bits(fl, out.fwd_levels, out.fwd_thin_bits);
     level_bits(bl, out.bck_levels, out.bck_thin_bits);
-    // Sweep plans (the kernels' layout), checked before anything is uploaded.
-    build_plan(m, fl, out.fwd_levels, out.fwd_thin_bits, out.csr_ptr, out.csr_idx, out.csr_val, true, done,
-               out.fwd_plan);
-    build_plan(m, bl, out.bck_levels, out.bck_thin_bits, cp, ci, cv, false, done, out.bck_plan);
-    for (int dir = 0; dir < 2; ++dir) {
-        const std::string bad = check_plan(m, dir == 0 ? fl : bl, dir == 0 ? out.fwd_plan : out.bck_plan);
-        if (!bad.empty()) return "internal sweep plan error: " + bad;
+    clk.mark("levels");
+    // Sweep plans (the kernels' layout), checked before anything is uploaded;
+    // the two directions are independent and built on two threads.
+    std::string bad[2];
+    {
+        std::thread bck([&] {
+            build_plan(m, bl, out.bck_levels, out.bck_thin_bits, cp, ci, cv, false, done, out.bck_plan);
+            bad[1] = check_plan(m, bl, out.bck_plan);
+        });
+        build_plan(m, fl, out.fwd_levels, out.fwd_thin_bits, out.csr_ptr, out.csr_idx, out.csr_val, true, done,
+                   out.fwd_plan);
+        bad[0] = check_plan(m, fl, out.fwd_plan);
+        bck.join();
     }
+    for (int dir = 0; dir < 2; ++dir)
+        if (!bad[dir].empty()) return "internal sweep plan error: " + bad[dir];
     out.fwd_level = std::move(fl);
     out.bck_level = std::move(bl);
 
+    clk.mark("plans");
     // Permutation: must be a bijection of [0, n).
     out.perm.assign(perm, perm + n);
     {

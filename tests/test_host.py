@@ -84,6 +84,23 @@ def test_factorization_is_deterministic_for_fixed_threads():
         assert np.array_equal(getattr(F1, k), getattr(F2, k)), k
 
 
+@pytest.mark.parametrize("name", ["grid3d_24", "rmat_12", "path_200"])
+def test_threaded_preparation_matches_serial(name, monkeypatch):
+    """The threaded CSR transpose (per-thread column ranges scattered at
+    per-row offsets) gives the same arrays as the serial scatter, whatever
+    the thread count, including more threads than columns."""
+    A, F = problem(name)
+    outs = []
+    for t in ("1", "3", "8", "64"):
+        monkeypatch.setenv("APXB_PREP_THREADS", t)
+        outs.append((native.prepare_host(F), native.batch_plan_host(F, 16)))
+    base, plans = outs[0]
+    for o, pl in outs[1:]:
+        assert pl == plans
+        for key, v in base.items():
+            assert np.array_equal(o[key], v) if isinstance(v, np.ndarray) else o[key] == v, key
+
+
 @pytest.mark.parametrize("name", ["grid2d_64", "grid3d_24", "rmat_12", "regular_3000", "path_200"])
 @pytest.mark.parametrize("k", [1, 4, 8, 16])
 def test_batch_plans_hold_their_invariants(name, k):
