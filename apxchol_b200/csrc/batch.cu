@@ -165,7 +165,8 @@ __global__ void __launch_bounds__(kBT) k_b_spmv(bp P, const double* X, double* Y
         double part[K];
 #pragma unroll
         for (int c = 0; c < K; ++c) part[c] = 0.0;
-        for (unsigned row = P.tile_lo[t] + threadIdx.x; row < P.tile_hi[t]; row += blockDim.x) {
+        for (unsigned g = P.tile_lo[t] + threadIdx.x; g < P.tile_hi[t]; g += blockDim.x) {
+            const unsigned row = __ldg(P.gperm + g);   // rows in the operator's own order (see k_b_spmv_pairs)
             double acc[K];
 #pragma unroll
             for (int c = 0; c < K; ++c) acc[c] = 0.0;
@@ -220,6 +221,14 @@ __global__ void __launch_bounds__(kBT) k_b_spmv(bp P, const double* X, double* Y
 // read as one coalesced k*8-byte access; p.Ap partials through col_store. The
 // row's own p (for p.Ap) is taken from the diagonal's gather when the row
 // stores its diagonal.
+// Both SpMV row kernels visit the rows in the operator's ORIGINAL order (row
+// gperm[g] for g = tile_lo..tile_hi) while the vectors stay in elimination
+// order. Elimination order lists each round's vertices together, so a
+// vertex's neighbours sit in other rounds' segments and, visited in storage
+// order, an operand row is re-read long after its first read. Visited in the
+// original order, the neighbours of the rows in flight lie in one window of
+// the mesh, and every operand row is reused while it is in L2. Each row's sum
+// is unchanged; only the rows that share a p.Ap tile partial differ.
 template <int K>
 __global__ void __launch_bounds__(kBT, 4) k_b_spmv_pairs(bp P, const double* X, double* Y, int mode) {
     if (*P.all_done && mode == 0) return;
@@ -229,7 +238,8 @@ __global__ void __launch_bounds__(kBT, 4) k_b_spmv_pairs(bp P, const double* X, 
     const unsigned c0 = (2 * threadIdx.x) % K, rsub = (2 * threadIdx.x) / K;
     for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
         double acc[1][2] = {{0.0, 0.0}};
-        for (unsigned row = P.tile_lo[t] + rsub; row < P.tile_hi[t]; row += kRows) {
+        for (unsigned g = P.tile_lo[t] + rsub; g < P.tile_hi[t]; g += kRows) {
+            const unsigned row = __ldg(P.gperm + g);
             double a0 = 0.0, a1 = 0.0;
             double2 own = make_double2(0.0, 0.0);
             bool have_own = false;
