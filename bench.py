@@ -651,7 +651,7 @@ def run_serving8(args, rank, world, local_rank):
         srv.completed.clear()
         pools = {name: [gen.rhs(A.n, 100 + j, not F.sddm) for j in range(4)] for name, A, F in mats}
         names = [nm for nm, _, _ in mats]
-        for rate, nreq in ((50, 400), (200, 1000), (800, 2400)):
+        for rate, nreq in ((50, 1000), (200, 1000), (800, 2400)):   # p50/p99 over >= 1000 requests per rate
             rng = np.random.default_rng(rate)
             t = np.cumsum(rng.exponential(1.0 / rate, size=nreq))
             tols = (1e-6, 1e-8, 1e-10)
