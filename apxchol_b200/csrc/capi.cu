@@ -174,26 +174,69 @@ int apxb_prepare_host(uint32_t n, const uint32_t* colptr, const uint32_t* rowidx
     return APXB_OK;
 }
 
+int apxb_prepare_host_fp16(uint32_t n, const uint32_t* colptr, const uint32_t* rowidx, const float* vals,
+                           const uint32_t* perm, int sddm, const uint64_t* rounds, uint32_t n_rounds,
+                           double drop_rel, uint32_t* m, uint64_t* nnz_stored,
+                           uint32_t* csc_ptr, uint32_t* csc_idx, uint16_t* csc_val16,
+                           uint32_t* csr_ptr, uint32_t* csr_idx, uint16_t* csr_val16,
+                           float* diag, float* inv_scale, uint64_t* stats) {
+    if (!colptr || !rowidx || !vals || !perm || !m || !nnz_stored) return fail(APXB_ERR_INVALID, "NULL argument");
+    if (n_rounds && !rounds) return fail(APXB_ERR_INVALID, "rounds is NULL");
+    apxb::prepared_factor h;
+    const std::string why = apxb::prepare_factor(n, colptr, rowidx, vals, perm, sddm != 0, rounds, n_rounds,
+                                                 drop_rel, h, true);
+    if (!why.empty()) return fail(APXB_ERR_BAD_FACTOR, why);
+    *m = h.m;
+    *nnz_stored = h.nnz_stored;
+    if (csc_ptr) std::memcpy(csc_ptr, h.csc_ptr.data(), 4 * h.csc_ptr.size());
+    if (csc_idx) std::memcpy(csc_idx, h.csc_idx.data(), 4 * h.csc_idx.size());
+    if (csc_val16) std::memcpy(csc_val16, h.csc_h.data(), 2 * h.csc_h.size());
+    if (csr_ptr) std::memcpy(csr_ptr, h.csr_ptr.data(), 4 * h.csr_ptr.size());
+    if (csr_idx) std::memcpy(csr_idx, h.csr_idx.data(), 4 * h.csr_idx.size());
+    if (csr_val16) std::memcpy(csr_val16, h.csr_h.data(), 2 * h.csr_h.size());
+    if (diag) std::memcpy(diag, h.diag16.data(), 4 * h.diag16.size());
+    if (inv_scale) std::memcpy(inv_scale, h.inv_scale.data(), 4 * h.inv_scale.size());
+    if (stats) { stats[0] = h.dropped; stats[1] = h.dropped_flush; stats[2] = h.flushed; }
+    return APXB_OK;
+}
+
 // ---------------------------------------------------------------- factor
 
 int apxb_factor_create(apxb_engine* e, uint32_t n, const uint32_t* colptr, const uint32_t* rowidx,
                        const float* vals, const uint32_t* perm, int sddm, const uint64_t* rounds,
                        uint32_t n_rounds, double drop_rel, int precision, apxb_factor** out) {
     if (!e || !out || !colptr || !rowidx || !vals || !perm) return fail(APXB_ERR_INVALID, "NULL argument");
-    if (precision != APXB_PREC_FP64 && precision != APXB_PREC_FP32) return fail(APXB_ERR_INVALID, "bad precision");
+    if (precision != APXB_PREC_FP64 && precision != APXB_PREC_FP32 && precision != APXB_PREC_FP16)
+        return fail(APXB_ERR_INVALID, "bad precision");
     if (n_rounds && !rounds) return fail(APXB_ERR_INVALID, "rounds is NULL");
     *out = nullptr;
+    const bool fp16 = precision == APXB_PREC_FP16;
     APXB_CK(cudaSetDevice(e->device));
     std::unique_ptr<apxb_factor> f(new (std::nothrow) apxb_factor);
     if (!f) return fail(APXB_ERR_INVALID, "host allocation failed");
     f->e = e;
     f->precision = precision;
     const std::string why = apxb::prepare_factor(n, colptr, rowidx, vals, perm, sddm != 0, rounds, n_rounds,
-                                                 drop_rel, f->h);
+                                                 drop_rel, f->h, fp16);
     if (!why.empty()) return fail(APXB_ERR_BAD_FACTOR, why);
     const auto& h = f->h;
     const size_t m = h.m, nnz = h.nnz_stored;
     if (nnz >= 0xffffffffull) return fail(APXB_ERR_BAD_FACTOR, "factor nnz exceeds the 32-bit offset range");
+    // fp16 storage: (1 / s)^2 in fp64 (an fp32 square overflows for s below
+    // ~5e-20), and a column the storage cannot represent fails here, loudly
+    // (cuda.h:339-358)
+    std::vector<double> inv_scale2;
+    if (fp16) {
+        inv_scale2.resize(m);
+        for (size_t j = 0; j < m; ++j) {
+            const double r = static_cast<double>(h.inv_scale[j]);
+            inv_scale2[j] = r * r;
+            if (!(std::isfinite(h.diag16[j]) && h.diag16[j] != 0.0f && std::isfinite(inv_scale2[j])))
+                return fail(APXB_ERR_BAD_FACTOR, "fp16 factor storage cannot represent column " + std::to_string(j) +
+                                                     " (diag " + std::to_string(h.diag16[j]) + ", inv_scale^2 " +
+                                                     std::to_string(inv_scale2[j]) + ")");
+        }
+    }
     int rc;
     if ((rc = f->dalloc(&f->perm, n)) || (rc = f->dalloc(&f->ctl, 2))) return rc;
     cudaStream_t s = e->stream;
@@ -203,7 +246,8 @@ int apxb_factor_create(apxb_engine* e, uint32_t n, const uint32_t* colptr, const
         const apxb::sweep_plan& pl = dir == 0 ? h.fwd_plan : h.bck_plan;
         if ((rc = f->dalloc(&f->info[dir], pl.info.size())) || (rc = f->dalloc(&f->ord[dir], pl.ord.size())) ||
             (rc = f->dalloc(&f->ptr[dir], pl.ptr.size())) || (rc = f->dalloc(&f->idx[dir], pl.idx.size())) ||
-            (rc = f->dalloc(&f->val[dir], pl.val.size())) || (rc = f->dalloc(&f->chunk[dir], pl.chunk.size())))
+            (rc = fp16 ? f->dalloc(&f->val16[dir], pl.val16.size()) : f->dalloc(&f->val[dir], pl.val.size())) ||
+            (rc = f->dalloc(&f->chunk[dir], pl.chunk.size())))
             return rc;
         f->n_chunks[dir] = static_cast<uint32_t>(pl.chunk.size() - 1);
         APXB_CK(cudaMemcpyAsync(f->chunk[dir], pl.chunk.data(), 4 * pl.chunk.size(), cudaMemcpyHostToDevice, s));
@@ -211,7 +255,10 @@ int apxb_factor_create(apxb_engine* e, uint32_t n, const uint32_t* colptr, const
         APXB_CK(cudaMemcpyAsync(f->ord[dir], pl.ord.data(), 4 * pl.ord.size(), cudaMemcpyHostToDevice, s));
         APXB_CK(cudaMemcpyAsync(f->ptr[dir], pl.ptr.data(), 4 * pl.ptr.size(), cudaMemcpyHostToDevice, s));
         APXB_CK(cudaMemcpyAsync(f->idx[dir], pl.idx.data(), 4 * pl.idx.size(), cudaMemcpyHostToDevice, s));
-        APXB_CK(cudaMemcpyAsync(f->val[dir], pl.val.data(), 4 * pl.val.size(), cudaMemcpyHostToDevice, s));
+        if (fp16)
+            APXB_CK(cudaMemcpyAsync(f->val16[dir], pl.val16.data(), 2 * pl.val16.size(), cudaMemcpyHostToDevice, s));
+        else
+            APXB_CK(cudaMemcpyAsync(f->val[dir], pl.val.data(), 4 * pl.val.size(), cudaMemcpyHostToDevice, s));
         if (pl.seg_rows) {
             if ((rc = f->dalloc(&f->seg_row[dir], pl.seg_row.size())) ||
                 (rc = f->dalloc(&f->seg_lvl[dir], pl.seg_lvl.size())) ||
@@ -225,6 +272,11 @@ int apxb_factor_create(apxb_engine* e, uint32_t n, const uint32_t* colptr, const
             APXB_CK(cudaMemcpyAsync(f->seg_idx[dir], pl.seg_idx.data(), 4 * pl.seg_idx.size(), cudaMemcpyHostToDevice, s));
             APXB_CK(cudaMemcpyAsync(f->seg_val[dir], pl.seg_val.data(), 4 * pl.seg_val.size(), cudaMemcpyHostToDevice, s));
         }
+    }
+    if (fp16) {
+        if ((rc = f->dalloc(&f->diag16, m)) || (rc = f->dalloc(&f->inv_scale2, m))) return rc;
+        APXB_CK(cudaMemcpyAsync(f->diag16, h.diag16.data(), 4 * m, cudaMemcpyHostToDevice, s));
+        APXB_CK(cudaMemcpyAsync(f->inv_scale2, inv_scale2.data(), 8 * m, cudaMemcpyHostToDevice, s));
     }
     if ((rc = f->dalloc(&f->Y, n)) || (rc = f->dalloc(&f->Z, n)) || (rc = f->dalloc(&f->zp, n))) return rc;
     // Z[m] (the grounded entry of a Laplacian) is 0 for good; rows < m start armed.
@@ -302,6 +354,9 @@ void plan_args(const apxb_factor* f, int dir, apxb::sweep_args<T>& a) {
     a.ptr = f->ptr[dir];
     a.idx = f->idx[dir];
     a.val = f->val[dir];
+    a.val16 = f->val16[dir];
+    a.diag16 = f->diag16;
+    a.in_scale2 = nullptr;   // set for the backward of an fp16 factor by its caller
     a.seg_first = pl.seg_first;
     a.seg_rows = pl.seg_rows;
     a.seg_levels = pl.seg_levels;
@@ -361,6 +416,8 @@ int finish(apxb_factor* f) {
     return rc;
 }
 
+int sweep32_one(apxb_factor* f, int dir, const double* d_in, double* d_out);
+
 }  // namespace
 
 extern "C" {
@@ -368,9 +425,9 @@ extern "C" {
 int apxb_sweep(apxb_engine* e, apxb_factor* f, int dir, const double* d_in, double* d_out) {
     if (!e || !f || !d_in || !d_out || (dir != 0 && dir != 1)) return fail(APXB_ERR_INVALID, "bad argument");
     if (f->e != e) return fail(APXB_ERR_INVALID, "factor belongs to another engine");
-    if (f->precision != APXB_PREC_FP64) return fail(APXB_ERR_INVALID, "apxb_sweep needs an fp64 factor");
     APXB_CK(cudaSetDevice(e->device));
-    int rc = run_sweep64(f, dir, d_in, d_out, nullptr, nullptr);
+    int rc = f->precision == APXB_PREC_FP64 ? run_sweep64(f, dir, d_in, d_out, nullptr, nullptr)
+                                            : sweep32_one(f, dir, d_in, d_out);
     if (rc) return rc;
     return finish(f);
 }
@@ -417,6 +474,7 @@ int ensure_f32(apxb_factor* f, int k) {
 
 namespace apxb {
 void launch_cast32to64(const float* in, double* out, size_t n, cudaStream_t s);
+void launch_cast64to32(const double* in, float* out, size_t n, cudaStream_t s);
 }
 
 namespace {
@@ -439,10 +497,48 @@ int pair_fp32(apxb_factor* f, int k, const double* d_in, double* d_out) {
     plan_args(f, 1, a);
     a.ctl = f->ctl + 1;
     a.in = f->Yf; a.out = f->Zf; a.reset = f->Yf;
+    a.in_scale2 = f->inv_scale2;   // fp16 factors: the backward reads D^-2 y'
     apxb::launch_sweep32(1, a, grid, s);
     f->yf_armed = true;
     f->zf_armed = false;
     apxb::launch_cast32to64(f->Zf, d_out, mk, s);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(APXB_ERR_CUDA, std::string("sweep launch: ") + cudaGetErrorString(e));
+    return APXB_OK;
+}
+
+// One fp32 sweep of an fp32 / fp16 factor, fp64 in and out (m entries).
+// Forward: in -> Yf (re-arms Zf). Backward: in is narrowed into Yf, which the
+// sweep reads as its right-hand side (fp16: times inv_scale^2) and re-arms
+// row by row; -> Zf.
+int sweep32_one(apxb_factor* f, int dir, const double* d_in, double* d_out) {
+    int rc = ensure_f32(f, 1);
+    if (rc) return rc;
+    cudaStream_t s = f->e->stream;
+    const size_t m = f->h.m;
+    const int grid = f->e->sweep_grid > 0 ? f->e->sweep_grid : apxb::sweep_grid32(1, f->e->num_sms);
+    apxb::sweep_args<float> a{};
+    a.k = 1;
+    a.err = f->e->d_err; a.budget_ns = f->e->budget_ns;
+    plan_args(f, dir, a);
+    a.ctl = f->ctl + dir;
+    if (dir == 0) {
+        if (!f->yf_armed) apxb::launch_fill_sent32(f->Yf, m, s);
+        a.out = f->Yf; a.reset = f->Zf;
+        apxb::launch_sweep32_from64(0, a, d_in, grid, s);
+        f->yf_armed = false;
+        f->zf_armed = true;
+        apxb::launch_cast32to64(f->Yf, d_out, m, s);
+    } else {
+        if (!f->zf_armed) apxb::launch_fill_sent32(f->Zf, m, s);
+        apxb::launch_cast64to32(d_in, f->Yf, m, s);
+        a.in = f->Yf; a.out = f->Zf; a.reset = f->Yf;
+        a.in_scale2 = f->inv_scale2;
+        apxb::launch_sweep32(1, a, grid, s);
+        f->zf_armed = false;
+        f->yf_armed = true;
+        apxb::launch_cast32to64(f->Zf, d_out, m, s);
+    }
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(APXB_ERR_CUDA, std::string("sweep launch: ") + cudaGetErrorString(e));
     return APXB_OK;

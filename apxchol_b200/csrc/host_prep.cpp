@@ -48,9 +48,12 @@ void relay_row(uint32_t r, bool forward, const std::vector<uint32_t>& ptr, const
     oi.push_back(idx[d]); ov.push_back(val[d]);
 }
 
+// val16 (fp16 storage, nullable): binary16 values beside val, re-laid the
+// same way into plan.val16; such plans have no serial segment.
 void build_plan(uint32_t m, const std::vector<int32_t>& level, int32_t n_levels, const std::vector<uint32_t>& bits,
                 const std::vector<uint32_t>& ptr, const std::vector<uint32_t>& idx, const std::vector<float>& val,
-                bool forward, bool contiguous, sweep_plan& plan) {
+                bool forward, bool contiguous, sweep_plan& plan, const std::vector<uint16_t>* val16 = nullptr) {
+    if (val16) contiguous = false;
     std::vector<std::vector<uint32_t>> by_level(static_cast<size_t>(n_levels));
     for (uint32_t r = 0; r < m; ++r) by_level[level[r]].push_back(r);
     plan = sweep_plan{};
@@ -126,6 +129,7 @@ void build_plan(uint32_t m, const std::vector<int32_t>& level, int32_t n_levels,
     plan.ptr.assign(npos + 1, 0);
     plan.idx.resize(idx.size());
     plan.val.resize(val.size());
+    if (val16) plan.val16.resize(val16->size());
     size_t k = 0;      // index into item_rows
     uint32_t e = 0;    // entry cursor
     for (uint32_t c = 0; c < plan.n_items; ++c) {
@@ -140,15 +144,20 @@ void build_plan(uint32_t m, const std::vector<int32_t>& level, int32_t n_levels,
                 const uint32_t d = forward ? en - 1 : b;                 // diagonal slot
                 for (uint32_t p = b; p < en; ++p) {
                     if (p == d) continue;
-                    plan.idx[e] = idx[p]; plan.val[e] = val[p]; ++e;
+                    plan.idx[e] = idx[p]; plan.val[e] = val[p];
+                    if (val16) plan.val16[e] = (*val16)[p];
+                    ++e;
                 }
-                plan.idx[e] = idx[d]; plan.val[e] = val[d]; ++e;       // diagonal last
+                plan.idx[e] = idx[d]; plan.val[e] = val[d];             // diagonal last
+                if (val16) plan.val16[e] = (*val16)[d];
+                ++e;
             }
         }
     }
     plan.ptr[npos] = e;
     plan.idx.resize(e);
     plan.val.resize(e);
+    if (val16) plan.val16.resize(e);
     chunk_plan(plan);
 }
 
@@ -388,12 +397,12 @@ std::string check_batch_plan(uint32_t m, const std::vector<int32_t>& level, cons
 
 std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* rowidx, const float* vals,
                            const uint32_t* perm, bool sddm, const uint64_t* rounds, uint32_t n_rounds,
-                           double drop_rel, prepared_factor& out) {
+                           double drop_rel, prepared_factor& out, bool fp16) {
     if (n == 0) return "empty factor";
     if (!sddm && n < 2) return "a Laplacian factor needs n >= 2";
     const uint32_t m = sddm ? n : n - 1;
     out = prepared_factor{};
-    out.n = n; out.m = m; out.sddm = sddm;
+    out.n = n; out.m = m; out.sddm = sddm; out.fp16 = fp16;
     const double rel = drop_rel < 0.0 ? kDropRelDefault : drop_rel;
 
     stage_clock clk;
@@ -413,16 +422,23 @@ std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* r
 
     clk.mark("validate");
     // L11 (drop row n-1 for a Laplacian), then the compacting drop, written
-    // straight into the CSC arrays.
+    // straight into the CSC arrays; with fp16 storage each column is then
+    // narrowed (cuda_host.h:202-232).
     std::vector<uint32_t>& cp = out.csc_ptr;
     std::vector<uint32_t>& ci = out.csc_idx;
     std::vector<float>& cv = out.csc_val;
+    std::vector<uint16_t>& ch = out.csc_h;
     cp.assign(static_cast<size_t>(m) + 1, 0);
     ci.reserve(colptr[m]);
     cv.reserve(colptr[m]);
+    if (fp16) {
+        ch.reserve(colptr[m]);
+        out.diag16.resize(m);
+        out.inv_scale.resize(m);
+    }
     std::vector<uint32_t> rows;
     std::vector<float> vs;
-    uint64_t nnz_factor = 0, dropped = 0;
+    uint64_t nnz_factor = 0, dropped = 0, dropped_flush = 0, flushed = 0;
     for (uint32_t j = 0; j < m; ++j) {
         rows.clear(); vs.clear();
         for (uint32_t p = colptr[j]; p < colptr[j + 1]; ++p) {
@@ -430,14 +446,26 @@ std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* r
             rows.push_back(rowidx[p]); vs.push_back(vals[p]);
         }
         nnz_factor += rows.size();
+        const size_t first = ci.size();
+        float s = 1.0f;   // the column's scale, taken before the drop
+        if (rel > 0.0 || fp16) {
+            s = column_scale(vs.data(), 0, static_cast<uint32_t>(vs.size()));
+            // fp16 storage: a scale whose 1/s or diagonal/s overflows fp32 falls
+            // back to 1, before the drop (cuda.h:287-301)
+            if (fp16 && (!std::isfinite(1.0f / s) || !std::isfinite(vs[0] / s))) s = 1.0f;
+        }
         if (rel > 0.0) {
-            const float s = column_scale(vs.data(), 0, static_cast<uint32_t>(vs.size()));
             double dropped_sum = 0.0, kept_abs = 0.0;
-            const size_t first = ci.size();
             for (size_t t = 0; t < rows.size(); ++t) {
                 const float v = vs[t];
                 if (rows[t] != j) {
-                    if (!keep_offdiag(v, s, rel)) { dropped_sum += static_cast<double>(v); ++dropped; continue; }
+                    // fp16 storage also drops what it would flush (cuda_host.h:135-139)
+                    if (!keep_offdiag(v, s, rel) || (fp16 && fp16_flushes(v / s))) {
+                        if (std::fabs(static_cast<double>(v)) >= rel * static_cast<double>(s)) ++dropped_flush;
+                        dropped_sum += static_cast<double>(v);
+                        ++dropped;
+                        continue;
+                    }
                     kept_abs += std::fabs(static_cast<double>(v));
                 }
                 ci.push_back(rows[t]); cv.push_back(v);
@@ -454,11 +482,31 @@ std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* r
             ci.insert(ci.end(), rows.begin(), rows.end());
             cv.insert(cv.end(), vs.begin(), vs.end());
         }
+        if (fp16) {
+            // off-diagonals as binary16(v / s); the diagonal (first in the
+            // column) as fp32 d / s plus the column's rounding residual, so the
+            // stored column sums to what the fp32 column sums to
+            const float d = cv[first] / s;
+            double resid = 0.0;
+            for (size_t q = first; q < ci.size(); ++q) {
+                const float v = cv[q];
+                const uint16_t h = fp16_narrow(v, s);
+                ch.push_back(h);                  // the diagonal's slot too (never read)
+                if (ci[q] == j) continue;
+                const float w = fp16_value(h);
+                if (v != 0.0f && w == 0.0f) ++flushed;
+                resid += static_cast<double>(v) / static_cast<double>(s) - static_cast<double>(w);
+            }
+            out.diag16[j] = static_cast<float>(static_cast<double>(d) + resid);
+            out.inv_scale[j] = 1.0f / s;
+        }
         cp[j + 1] = static_cast<uint32_t>(ci.size());
     }
     out.nnz_factor = nnz_factor;
     out.nnz_stored = ci.size();
     out.dropped = dropped;
+    out.dropped_flush = dropped_flush;
+    out.flushed = flushed;
 
     clk.mark("L11 + drop");
     // CSR by the column-order scatter: columns ascend within each row. On T
@@ -469,6 +517,7 @@ std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* r
     out.csr_ptr.assign(static_cast<size_t>(m) + 1, 0);
     out.csr_idx.resize(nnz);
     out.csr_val.resize(nnz);
+    if (fp16) out.csr_h.resize(nnz);
     {
         const unsigned T = prep_threads(nnz);
         const std::vector<uint32_t> jb = column_ranges(cp.data(), m, T);
@@ -493,6 +542,7 @@ std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* r
                     const uint32_t slot = cur[ci[p]]++;
                     out.csr_idx[slot] = j;
                     out.csr_val[slot] = cv[p];
+                    if (fp16) out.csr_h[slot] = ch[p];
                 }
         });
     }
@@ -555,11 +605,12 @@ std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* r
     std::string bad[2];
     {
         std::thread bck([&] {
-            build_plan(m, bl, out.bck_levels, out.bck_thin_bits, cp, ci, cv, false, done, out.bck_plan);
+            build_plan(m, bl, out.bck_levels, out.bck_thin_bits, cp, ci, cv, false, done, out.bck_plan,
+                       fp16 ? &ch : nullptr);
             bad[1] = check_plan(m, bl, out.bck_plan);
         });
         build_plan(m, fl, out.fwd_levels, out.fwd_thin_bits, out.csr_ptr, out.csr_idx, out.csr_val, true, done,
-                   out.fwd_plan);
+                   out.fwd_plan, fp16 ? &out.csr_h : nullptr);
         bad[0] = check_plan(m, fl, out.fwd_plan);
         bck.join();
     }

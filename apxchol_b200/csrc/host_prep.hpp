@@ -17,6 +17,7 @@
 // With these the fp64 sweep kernels reproduce the reference's bytes.
 #pragma once
 #include <cstdint>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -24,6 +25,59 @@ namespace apxb {
 
 constexpr uint32_t kThinLevelRows = 1024;   // kSpTRSVOMPThreshold, omp.h:32
 constexpr double kDropRelDefault = 1e-4;    // kFactorDropRelDefault, factor_drop.h:70
+
+// IEEE binary16 bit pattern of x, rounded to nearest even (overflow to
+// infinity, subnormal results kept as subnormals).
+inline uint16_t fp16_bits(float x) {
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    const uint16_t sign = static_cast<uint16_t>((u >> 16) & 0x8000u);
+    const uint32_t ax = u & 0x7fffffffu;
+    if (ax >= 0x7f800000u)                                   // infinity, NaN (quiet, payload kept)
+        return static_cast<uint16_t>(sign | 0x7c00u | (ax > 0x7f800000u ? 0x200u | ((ax >> 13) & 0x3ffu) : 0u));
+    if (ax >= 0x477ff000u) return static_cast<uint16_t>(sign | 0x7c00u);   // >= 65520: rounds past 65504
+    if (ax >= 0x38800000u) {                                 // >= 2^-14: a normal half
+        const uint32_t v = ax - 0x38000000u;                 // exponent rebiased 127 -> 15
+        return static_cast<uint16_t>(sign | ((v + 0xfffu + ((v >> 13) & 1u)) >> 13));
+    }
+    if (ax < 0x33000000u) return sign;                       // < 2^-25: rounds to zero
+    // subnormal half: x / 2^-24 rounded to nearest even
+    const uint32_t e = ax >> 23, mant = (ax & 0x7fffffu) | 0x800000u;
+    const uint32_t shift = 126u - e;                          // 14 .. 24
+    uint32_t q = mant >> shift;
+    const uint32_t rem = mant & ((1u << shift) - 1u), half = 1u << (shift - 1u);
+    if (rem > half || (rem == half && (q & 1u))) ++q;
+    return static_cast<uint16_t>(sign | q);
+}
+
+// The value of a binary16 bit pattern (exact in fp32).
+inline float fp16_value(uint16_t h) {
+    const uint32_t sign = static_cast<uint32_t>(h & 0x8000u) << 16, e = (h >> 10) & 0x1fu, m = h & 0x3ffu;
+    uint32_t u;
+    if (e == 0) {
+        const float v = static_cast<float>(m) * 5.9604644775390625e-8f;   // m * 2^-24, exact
+        std::memcpy(&u, &v, 4);
+        u |= sign;
+    } else if (e == 31) {
+        u = sign | 0x7f800000u | (m << 13);
+    } else {
+        u = sign | ((e + 112u) << 23) | (m << 13);
+    }
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+
+// fp16 storage flushes x: it rounds to zero or to a subnormal (stored as zero).
+inline bool fp16_flushes(float x) { return (fp16_bits(x) & 0x7c00u) == 0; }
+
+// What the fp16 storage keeps for an entry v of a column with scale s:
+// binary16(fp32(v) / s), subnormals flushed to signed zero
+// (cuda_host.h:195-201).
+inline uint16_t fp16_narrow(float v, float s) {
+    const uint16_t h = fp16_bits(v / s);
+    return (h & 0x7c00u) == 0 ? static_cast<uint16_t>(h & 0x8000u) : h;
+}
 
 // Execution plan of one sweep direction, in the layout the dataflow kernels
 // read.
@@ -58,6 +112,7 @@ struct sweep_plan {
     std::vector<uint32_t> ptr;
     std::vector<uint32_t> idx;
     std::vector<float> val;
+    std::vector<uint16_t> val16;       // fp16 storage: the binary16 values, same layout as val
     uint32_t seg_first = 0, seg_rows = 0, seg_levels = 0;
     std::vector<uint32_t> seg_row, seg_lvl, seg_ptr, seg_idx;
     std::vector<float> seg_val;
@@ -89,6 +144,18 @@ struct prepared_factor {
     std::vector<uint32_t> perm;  // perm[original] = position
     std::vector<int32_t> fwd_level, bck_level;   // level of every row per direction
     sweep_plan fwd_plan, bck_plan;
+    // fp16 storage (the reference's cuda_sptrsv default, cuda.h:131-163;
+    // cuda_host.h:16-34): column j is stored scaled by 1 / s_j (s_j the
+    // pre-drop max |off-diagonal|; 1 when 1/s_j or L_jj/s_j overflows fp32),
+    // off-diagonals as binary16, the diagonal as fp32 L_jj / s_j plus the
+    // column's rounding residual. The forward sweep on the scaled factor
+    // returns D y; the backward reads its input times inv_scale^2 (in fp64).
+    bool fp16 = false;
+    uint64_t dropped_flush = 0;                // off-diagonals dropped only because fp16 flushes them
+    uint64_t flushed = 0;                      // stored off-diagonals v != 0 whose binary16 is zero
+    std::vector<uint16_t> csr_h, csc_h;        // binary16 values, same layout as csr_val / csc_val
+    std::vector<float> diag16;                 // per row j: fp32(L_jj) / s_j + rounding residual
+    std::vector<float> inv_scale;              // per row j: fp32(1 / s_j)
 };
 
 // Lane-group width for a row with `len` off-diagonals (see sweep_plan).
@@ -121,9 +188,11 @@ void chunk_plan(sweep_plan& p);
 std::string check_batch_plan(uint32_t m, const std::vector<int32_t>& level, const sweep_plan& p, uint32_t col_lanes);
 
 // Returns an empty string on success, else the reason the factor was rejected.
+// fp16: also build the fp16 storage (prepared_factor::fp16); its drop then
+// also removes the off-diagonals fp16 flushes (cuda_host.h:128-139).
 std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* rowidx, const float* vals,
                            const uint32_t* perm, bool sddm, const uint64_t* rounds, uint32_t n_rounds,
-                           double drop_rel, prepared_factor& out);
+                           double drop_rel, prepared_factor& out, bool fp16 = false);
 
 // Full symmetric CSR of P A P^T (rows sorted) from A's full symmetric CSC and
 // perm (what cuda_pcg::setup builds, include/apxchol/solver/pcg_cuda.h:304-404).

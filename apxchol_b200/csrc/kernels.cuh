@@ -49,11 +49,20 @@ struct sweep_args {
     // batch plans (host_prep.hpp, build_batch_plan): claim units over the items
     const uint32_t* chunk;            // chunk c = items [chunk[c], chunk[c + 1])
     uint32_t n_chunks;
+    // fp16 factor storage (fp32 sweeps only; prepared_factor::fp16): entry
+    // weights are the binary16 values val16 (val is not read), a row's
+    // diagonal is diag16[row] (its plan slot is not read), and, when
+    // in_scale2 is given, the fp32 right-hand side is multiplied by
+    // in_scale2[row] in fp64 and rounded once (the backward sweep's D^-2).
+    const uint16_t* val16;
+    const float* diag16;
+    const double* in_scale2;
 };
 
 // fp64 sweep reproducing the reference CPU arithmetic (exact sum order).
 void launch_sweep64(int dir, const sweep_args<double>& a, int grid, cudaStream_t s);
-// fp32 sweep, fp32 accumulation, k in {1, 2, 4, 8, 16} right-hand sides.
+// fp32 sweep, fp32 accumulation, k in {1, 2, 4, 8, 16} right-hand sides
+// (fp16-stored factors when a.val16 is set).
 void launch_sweep32(int dir, const sweep_args<float>& a, int grid, cudaStream_t s);
 // The same with the right-hand side read from fp64 (minus rhs_sub[s] when given).
 void launch_sweep32_from64(int dir, const sweep_args<float>& a, const double* in64, int grid, cudaStream_t s);

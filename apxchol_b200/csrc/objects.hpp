@@ -128,7 +128,10 @@ struct apxb_factor {
     uint32_t* ord[2] = {nullptr, nullptr};
     uint32_t* ptr[2] = {nullptr, nullptr};
     uint32_t* idx[2] = {nullptr, nullptr};
-    float* val[2] = {nullptr, nullptr};
+    float* val[2] = {nullptr, nullptr};                // fp32 values (not on fp16 factors)
+    uint16_t* val16[2] = {nullptr, nullptr};           // fp16 factors: binary16 values
+    float* diag16 = nullptr;                           // fp16 factors: per-row diagonal
+    double* inv_scale2 = nullptr;                      // fp16 factors: per-row (1 / s)^2, fp64
     uint32_t* chunk[2] = {nullptr, nullptr};           // claim units (host_prep.hpp, chunk_plan)
     uint32_t n_chunks[2] = {0, 0};
     uint32_t *seg_row[2] = {nullptr, nullptr}, *seg_lvl[2] = {nullptr, nullptr};

@@ -385,6 +385,12 @@ __global__ void k_cast32to64(const float* in, double* out, size_t n) {
         out[i] = static_cast<double>(in[i]);
 }
 
+__global__ void k_cast64to32(const double* in, float* out, size_t n) {
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x)
+        out[i] = static_cast<float>(in[i]);
+}
+
 __global__ void k_perm_in(const uint32_t* perm, const double* src, double* dst, unsigned n) {
     for (unsigned v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) dst[perm[v]] = src[v];
 }
@@ -419,6 +425,9 @@ int grid_for(size_t n) {
 
 void launch_cast32to64(const float* in, double* out, size_t n, cudaStream_t s) {
     if (n) k_cast32to64<<<grid_for(n), 256, 0, s>>>(in, out, n);
+}
+void launch_cast64to32(const double* in, float* out, size_t n, cudaStream_t s) {
+    if (n) k_cast64to32<<<grid_for(n), 256, 0, s>>>(in, out, n);
 }
 void launch_perm_in(const uint32_t* perm, const double* src, double* dst, unsigned n, int grid, cudaStream_t s) {
     k_perm_in<<<grid, 256, 0, s>>>(perm, src, dst, n);

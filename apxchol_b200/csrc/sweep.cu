@@ -40,7 +40,13 @@
 //  * Rows are consumed progressively: in the fp64 sweep the reference's sum
 //    order is advanced step by step as operands arrive, so most of a row's
 //    arithmetic is done before its last dependency lands.
+//  * fp16 factor storage (the reference's GPU default, cuda.h:131-163): the
+//    fp32 sweep reads binary16 weights of the column-scaled factor, widened
+//    exactly to fp32, a per-row fp32 diagonal, and (backward) its right-hand
+//    side times the fp64 inv_scale^2 (cuda_dataflow.cu:395), 6 instead of 8
+//    bytes per stored entry.
 #include <cstdlib>
+#include <cuda_fp16.h>
 
 #include "kernels.cuh"
 
@@ -488,7 +494,14 @@ struct stage_data32 {
     float ww[batch_of<K>::value];
 };
 
-template <int K>
+// Weight of plan entry e: fp32, or the binary16 value widened (exact).
+template <bool H>
+__device__ __forceinline__ float weight32(const sweep_args<float>& a, uint32_t e) {
+    if constexpr (H) return __half2float(__ushort_as_half(__ldg(a.val16 + e)));
+    else return __ldg(a.val + e);
+}
+
+template <int K, bool H>
 __device__ __forceinline__ void load_data32(const sweep_args<float>& a, const double* in64, const stage_desc& ds,
                                             stage_data32<K>& s) {
     constexpr int B = batch_of<K>::value;
@@ -501,7 +514,7 @@ __device__ __forceinline__ void load_data32(const sweep_args<float>& a, const do
 #pragma unroll
     for (int k = 0; k < B; ++k) {
         const uint32_t t = (static_cast<uint32_t>(k) << v.lg) + v.u;
-        if (t < v.len) { s.jj[k] = __ldg(a.idx + v.q + t); s.ww[k] = __ldg(a.val + v.q + t); }
+        if (t < v.len) { s.jj[k] = __ldg(a.idx + v.q + t); s.ww[k] = weight32<H>(a, v.q + t); }
     }
     if (v.valid && v.u == 0) {
         const size_t base = static_cast<size_t>(v.row) * K;
@@ -512,15 +525,19 @@ __device__ __forceinline__ void load_data32(const sweep_args<float>& a, const do
                 if (a.rhs_sub) x -= a.rhs_sub[r];
                 s.rhs[r] = static_cast<float>(x);
             }
+        } else if (H && a.in_scale2) {
+            const double sc = a.in_scale2[v.row];
+#pragma unroll
+            for (int r = 0; r < K; ++r) s.rhs[r] = static_cast<float>(static_cast<double>(a.in[base + r]) * sc);
         } else {
 #pragma unroll
             for (int r = 0; r < K; ++r) s.rhs[r] = a.in[base + r];
         }
-        s.d = __ldg(a.val + v.q + v.len);
+        s.d = H ? __ldg(a.diag16 + v.row) : __ldg(a.val + v.q + v.len);
     }
 }
 
-template <int DIR, int K>
+template <int DIR, int K, bool H>
 __device__ __forceinline__ bool run32(const sweep_args<float>& a, stage_data32<K>& s) {
     constexpr int B = batch_of<K>::value;
     const lane_view& v = s.v;
@@ -536,7 +553,7 @@ __device__ __forceinline__ bool run32(const sweep_args<float>& a, stage_data32<K
 #pragma unroll
             for (int k = 0; k < B; ++k) {
                 const uint32_t t = ((jb + k) << v.lg) + v.u;
-                if (t < v.len) { s.jj[k] = __ldg(a.idx + v.q + t); s.ww[k] = __ldg(a.val + v.q + t); }
+                if (t < v.len) { s.jj[k] = __ldg(a.idx + v.q + t); s.ww[k] = weight32<H>(a, v.q + t); }
             }
         }
         // this lane's entries in the batch: steps 0 .. nk-1
@@ -590,7 +607,7 @@ __device__ __forceinline__ bool run32(const sweep_args<float>& a, stage_data32<K
     return true;
 }
 
-template <int DIR, int K>
+template <int DIR, int K, bool H>
 __global__ void __launch_bounds__(kSweepThreads, 2) k_df32(const sweep_args<float> a, const double* in64) {
     if (a.skip && *a.skip) return;
     const unsigned lane = threadIdx.x & 31u;
@@ -599,16 +616,16 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_df32(const sweep_args<floa
     stage_desc dD;
     load_desc(a, cc.next(a), dD);
     stage_data32<K> sL;
-    load_data32<K>(a, in64, dD, sL);
+    load_data32<K, H>(a, in64, dD, sL);
     load_desc(a, cc.next(a), dD);
     int bad = 0;   // the error word, read one item late
     while (sL.v.c < a.n_items) {
         stage_data32<K> sR = sL;
-        load_data32<K>(a, in64, dD, sL);
+        load_data32<K, H>(a, in64, dD, sL);
         load_desc(a, cc.next(a), dD);
         if (__shfl_sync(kFull, bad, 0)) break;
         if (lane == 0) bad = ld_relaxed_int(&a.err->code);
-        if (!run32<DIR, K>(a, sR)) break;
+        if (!run32<DIR, K, H>(a, sR)) break;
     }
     leave(a.ctl);
 }
@@ -940,8 +957,8 @@ int fill_grid(size_t n) {
 template <int K>
 int occ32() {
     int b0 = 0, b1 = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_df32<0, K>, kSweepThreads, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_df32<1, K>, kSweepThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_df32<0, K, false>, kSweepThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_df32<1, K, false>, kSweepThreads, 0);
     return b0 < b1 ? b0 : b1;
 }
 
@@ -962,8 +979,13 @@ template <int K>
 void sweep32_dir(int dir, const sweep_args<float>& a, const double* in64, int grid, cudaStream_t s) {
     if (dir == 1 && a.seg_rows) seg32<K>(a, in64, s);
     if (a.n_items) {
-        if (dir == 0) k_df32<0, K><<<grid, kSweepThreads, 0, s>>>(a, in64);
-        else          k_df32<1, K><<<grid, kSweepThreads, 0, s>>>(a, in64);
+        if (a.val16) {
+            if (dir == 0) k_df32<0, K, true><<<grid, kSweepThreads, 0, s>>>(a, in64);
+            else          k_df32<1, K, true><<<grid, kSweepThreads, 0, s>>>(a, in64);
+        } else {
+            if (dir == 0) k_df32<0, K, false><<<grid, kSweepThreads, 0, s>>>(a, in64);
+            else          k_df32<1, K, false><<<grid, kSweepThreads, 0, s>>>(a, in64);
+        }
     }
     if (dir == 0 && a.seg_rows) seg32<K>(a, in64, s);
 }

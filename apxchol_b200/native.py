@@ -19,7 +19,7 @@ HEADER = os.path.join(os.path.dirname(_HERE), "include", "apxb200.h")
 TRUE_RESIDUAL = 8
 OK = 0
 ERR_INVALID, ERR_CUDA, ERR_OOM, ERR_TIMEOUT, ERR_BAD_FACTOR, ERR_NONFINITE, ERR_BUDGET, ERR_BUSY = range(-1, -9, -1)
-PREC_FP64, PREC_FP32 = 0, 1
+PREC_FP64, PREC_FP32, PREC_FP16 = 0, 1, 2
 DEVICE_PTRS, CENTER_SCHEDULE, CENTER_ALWAYS, CENTER_NEVER = 1, 0, 2, 4
 
 c_p = ctypes.c_void_p
@@ -65,6 +65,8 @@ _SIGS = {
     "apxb_factor_reset_apply_count": (ctypes.c_int, [c_p]),
     "apxb_prepare_host": (ctypes.c_int, [ctypes.c_uint32, c_p, c_p, c_p, c_p, ctypes.c_int, c_p, ctypes.c_uint32,
                                          ctypes.c_double, c_p, c_p, c_p] + [c_p] * 8),
+    "apxb_prepare_host_fp16": (ctypes.c_int, [ctypes.c_uint32, c_p, c_p, c_p, c_p, ctypes.c_int, c_p, ctypes.c_uint32,
+                                              ctypes.c_double, c_p, c_p] + [c_p] * 9),
     "apxb_sweep": (ctypes.c_int, [c_p, c_p, ctypes.c_int, c_p, c_p]),
     "apxb_sweep_pair": (ctypes.c_int, [c_p, c_p, c_p, c_p]),
     "apxb_sweep_pair_host": (ctypes.c_int, [c_p, c_p, c_p, c_p]),
@@ -312,6 +314,30 @@ def prepare_host(fac, drop_rel: float = -1.0):
     check(lib.apxb_prepare_host(*args, *[ptr(out[k]) for k in ("csr_ptr", "csr_idx", "csr_val", "csc_ptr", "csc_idx",
                                                                 "csc_val", "fwd_thin", "bck_thin")]))
     out["m"], out["nnz"], out["levels"] = M, N, (int(lv[0]), int(lv[1]))
+    return out
+
+
+def prepare_host_fp16(fac, drop_rel: float = -1.0):
+    """Host-only fp16 factor storage through the C ABI (no GPU): the arrays an
+    APXB_PREC_FP16 factor uploads (binary16 values as uint16 bit patterns)."""
+    lib = load()
+    cp_ = np.ascontiguousarray(fac.colptr, np.uint32)
+    ri = np.ascontiguousarray(fac.rowidx, np.uint32)
+    va = np.ascontiguousarray(fac.vals, np.float32)
+    pe = np.ascontiguousarray(fac.perm, np.uint32)
+    ro = np.ascontiguousarray(fac.rounds, np.uint64)
+    m = ctypes.c_uint32(); nnz = ctypes.c_uint64()
+    args = (fac.n, ptr(cp_), ptr(ri), ptr(va), ptr(pe), int(fac.sddm), ptr(ro) if ro.size else None, ro.size,
+            drop_rel, ctypes.byref(m), ctypes.byref(nnz))
+    check(lib.apxb_prepare_host_fp16(*args, *([None] * 9)))
+    M, N = m.value, nnz.value
+    out = dict(csc_ptr=np.empty(M + 1, np.uint32), csc_idx=np.empty(N, np.uint32), csc_val16=np.empty(N, np.uint16),
+               csr_ptr=np.empty(M + 1, np.uint32), csr_idx=np.empty(N, np.uint32), csr_val16=np.empty(N, np.uint16),
+               diag=np.empty(M, np.float32), inv_scale=np.empty(M, np.float32), stats=np.zeros(3, np.uint64))
+    check(lib.apxb_prepare_host_fp16(*args, *[ptr(out[k]) for k in ("csc_ptr", "csc_idx", "csc_val16", "csr_ptr",
+                                                                     "csr_idx", "csr_val16", "diag", "inv_scale",
+                                                                     "stats")]))
+    out["m"], out["nnz"] = M, N
     return out
 
 

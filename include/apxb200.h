@@ -43,6 +43,9 @@ extern "C" {
 /* ---- sweep precisions ---- */
 #define APXB_PREC_FP64  0  /* fp32-stored factor, fp64 sweeps: the reference's CPU arithmetic */
 #define APXB_PREC_FP32  1  /* fp32 factor and sweeps, fp32 accumulation (mixed precision) */
+#define APXB_PREC_FP16  2  /* fp16 per-column-scaled factor storage, fp32 sweeps: the reference GPU
+                            * backend's default storage (cuda_sptrsv with APXCHOL_SPTRSV_FP16,
+                            * cuda.h:131-163); 6 instead of 8 bytes per stored entry */
 
 /* ---- apply flags ---- */
 #define APXB_DEVICE_PTRS      1  /* b / z are device pointers */
@@ -130,8 +133,29 @@ int apxb_prepare_host(uint32_t n, const uint32_t* colptr, const uint32_t* rowidx
                       uint32_t* csc_ptr, uint32_t* csc_idx, float* csc_val,
                       uint8_t* fwd_thin, uint8_t* bck_thin);
 
+/* Host-only fp16 storage (no GPU): what apxb_factor_create(..., APXB_PREC_FP16)
+ * uploads. Replaces the reference GPU backend's host preparation with fp16
+ * storage: cuda_host::apply_factor_drop with the fp16 keep predicate and
+ * cuda_host::narrow_fp16_scaled (cuda_host.h:120-232), after the scale
+ * fallback of cuda_sptrsv::setup (cuda.h:287-301). Call once with NULL arrays
+ * for *m and *nnz_stored. csc_*: CSC(L11) = CSR(L11^T) with binary16 values;
+ * csr_*: CSR(L11) carrying the same bit patterns; diag[m] = fp32 L_jj / s_j
+ * plus the column's rounding residual; inv_scale[m] = fp32 1 / s_j;
+ * stats[3] = {dropped, dropped only because fp16 flushes them, stored
+ * off-diagonals flushed to zero}. */
+int apxb_prepare_host_fp16(uint32_t n, const uint32_t* colptr, const uint32_t* rowidx, const float* vals,
+                           const uint32_t* perm, int sddm, const uint64_t* rounds, uint32_t n_rounds,
+                           double drop_rel, uint32_t* m, uint64_t* nnz_stored,
+                           uint32_t* csc_ptr, uint32_t* csc_idx, uint16_t* csc_val16,
+                           uint32_t* csr_ptr, uint32_t* csr_idx, uint16_t* csr_val16,
+                           float* diag, float* inv_scale, uint64_t* stats);
+
 /* ---- sweeps, permuted space, m entries (cuda_sptrsv::solve_LLt_dev, cuda.h:480-487) ---- */
-/* dir 0: forward L y = x; dir 1: backward L^T z = y. Device pointers; fp64. */
+/* dir 0: forward L y = x; dir 1: backward L^T z = y. Device pointers; fp64.
+ * fp32 / fp16 factors sweep in fp32 (input narrowed, output widened); an fp16
+ * factor's sweeps are those of the stored, column-scaled factor: the forward
+ * returns D y and the backward reads its input times D^-2 (D = diag(s_j)), so
+ * only the pair applies (L L^T)^-1. */
 int apxb_sweep(apxb_engine* e, apxb_factor* f, int dir, const double* d_in, double* d_out);
 /* Both sweeps: out = (L L^T)^-1 in. Device pointers (in and out may alias). */
 int apxb_sweep_pair(apxb_engine* e, apxb_factor* f, const double* d_in, double* d_out);

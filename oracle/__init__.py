@@ -62,6 +62,8 @@ def _load_ref():
         lib.apxref_sptrsv_info.argtypes = [c_p, c_p, c_p, c_p, c_p]
         lib.apxref_sptrsv_arrays.argtypes = [c_p] * 7
         lib.apxref_level_sizes.argtypes = [c_p, ctypes.c_int, c_p]
+        lib.apxref_fp16_prep.argtypes = [ctypes.c_uint32, c_p, c_p, c_p, ctypes.c_int, ctypes.c_double,
+                                         c_p, c_p] + [c_p] * 9
         _ref = lib
     return _ref
 
@@ -72,6 +74,31 @@ def ref_available() -> bool:
 
 def set_threads(t: int) -> int:
     return _load_ref().apxref_set_threads(t)
+
+
+def fp16_prep(fac, rel=-1.0):
+    """The reference GPU backend's fp16 factor storage, from its own host code
+    (cuda_host.h:120-258 with the scale fallback of cuda.h:295-301): CSR(L^T)
+    = CSC(L11) and CSR(L11) with binary16 values, diag, inv_scale and the drop
+    and flush counts. rel < 0 means the default 1e-4."""
+    lib = _load_ref()
+    rel = DROP_REL if rel < 0 else rel
+    cp_ = np.ascontiguousarray(fac.colptr, np.uint32)
+    ri = np.ascontiguousarray(fac.rowidx, np.uint32)
+    va = np.ascontiguousarray(fac.vals, np.float32)
+    m = ctypes.c_uint32(); nnz = ctypes.c_uint64()
+    args = (fac.n, _ptr(cp_), _ptr(ri), _ptr(va), int(fac.sddm), rel, ctypes.byref(m), ctypes.byref(nnz))
+    if lib.apxref_fp16_prep(*args, *([None] * 9)):
+        raise RuntimeError(lib.apxref_last_error().decode())
+    M, N = m.value, nnz.value
+    out = dict(csc_ptr=np.empty(M + 1, np.int32), csc_idx=np.empty(N, np.int32), csc_val16=np.empty(N, np.uint16),
+               csr_ptr=np.empty(M + 1, np.int32), csr_idx=np.empty(N, np.int32), csr_val16=np.empty(N, np.uint16),
+               diag=np.empty(M, np.float32), inv_scale=np.empty(M, np.float32), stats=np.zeros(3, np.uint64))
+    if lib.apxref_fp16_prep(*args, *[_ptr(out[k]) for k in ("csc_ptr", "csc_idx", "csc_val16", "csr_ptr", "csr_idx",
+                                                            "csr_val16", "diag", "inv_scale", "stats")]):
+        raise RuntimeError(lib.apxref_last_error().decode())
+    out["m"], out["nnz"] = M, N
+    return out
 
 
 class Ref:

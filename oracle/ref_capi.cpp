@@ -8,7 +8,10 @@
 //   cpu_solver(L, F, opts) / solve / apply    src/solve.cpp:295-318, 478-679
 //   apx_cholesky::apply_fused / reset_apply_count   preconditioner.h:317, 370-377
 //   omp_sptrsv forward_solve / transpose_solve / csr_* / csc_*   sptrsv/omp.h:1048-1058, 1176-1189
+//   cuda_host:: build_L11_csc_int / column_scales / apply_factor_drop /
+//     narrow_fp16_scaled / transpose_csr   sptrsv/cuda_host.h:66-258 (CUDA-free)
 #include "apxchol/solver/solve.h"
+#include "apxchol/solver/sptrsv/cuda_host.h"
 
 #include <chrono>
 #include <cstdint>
@@ -179,6 +182,56 @@ void apxref_level_sizes(void* hv, int fwd, int* sizes) {
     std::vector<long long> w;
     t.level_stats(fwd != 0, s, w);
     std::memcpy(sizes, s.data(), sizeof(int) * s.size());
+}
+
+// The reference GPU backend's host preparation with fp16 storage: what
+// cuda_sptrsv::setup computes before its upload (cuda.h:276-372): L11 as int
+// CSC, the pre-drop column scales, the drop with the fp16 keep predicate, the
+// narrowing and the transpose carrying the 16-bit values. The scale fallback
+// (cuda.h:295-301) sits inside the CUDA class, so its five lines are restated
+// here. Call once with NULL arrays for *m_out / *nnz_out.
+// stats[3] = {dropped, dropped_flush, flushed}.
+int apxref_fp16_prep(uint32_t n, const uint32_t* colptr, const uint32_t* rowidx, const float* vals, int sddm,
+                     double rel, uint32_t* m_out, uint64_t* nnz_out, int* lt_ptr, int* lt_idx, uint16_t* lt_val16,
+                     int* l_ptr, int* l_idx, uint16_t* l_val16, float* diag, float* inv_scale, uint64_t* stats) {
+    try {
+        namespace ch = apxchol::cuda_host;
+        std::vector<uint32_t> perm(n);
+        for (uint32_t v = 0; v < n; ++v) perm[v] = v;
+        const apxchol::factorization F = make_factor(n, colptr, rowidx, vals, perm.data(), sddm, nullptr, 0);
+        const int64_t m = sddm ? n : n - 1;
+        ch::csr_int<float> LT = ch::build_L11_csc_int<float>(F.L, m);
+        std::vector<float> col_scale = ch::column_scales(LT);
+        for (int64_t j = 0; j < m; ++j) {
+            const float s = col_scale[static_cast<size_t>(j)];
+            const float d = LT.vals[LT.ptr[static_cast<size_t>(j)]];
+            if (!std::isfinite(1.0f / s) || !std::isfinite(d / s)) col_scale[static_cast<size_t>(j)] = 1.0f;
+        }
+        const apxchol::factor_drop_stats st = ch::apply_factor_drop(LT, col_scale, rel, true);
+        ch::fp16_scaled_arrays h16 = ch::narrow_fp16_scaled(LT, col_scale);
+        *m_out = static_cast<uint32_t>(m);
+        *nnz_out = static_cast<uint64_t>(LT.nnz);
+        if (!lt_ptr) return 0;
+        const size_t nnz = static_cast<size_t>(LT.nnz);
+        std::memcpy(lt_ptr, LT.ptr.data(), sizeof(int) * (static_cast<size_t>(m) + 1));
+        std::memcpy(lt_idx, LT.idx.get(), sizeof(int) * nnz);
+        std::memcpy(lt_val16, h16.vals.get(), 2 * nnz);
+        std::memcpy(diag, h16.diag.data(), 4 * static_cast<size_t>(m));
+        std::memcpy(inv_scale, h16.inv_scale.data(), 4 * static_cast<size_t>(m));
+        ch::csr_int<uint16_t> LT16;
+        LT16.m = LT.m; LT16.nnz = LT.nnz; LT16.ptr = LT.ptr;
+        LT16.idx = std::move(LT.idx);
+        LT16.vals = std::move(h16.vals);
+        const ch::csr_int<uint16_t> L16 = ch::transpose_csr(LT16);
+        std::memcpy(l_ptr, L16.ptr.data(), sizeof(int) * (static_cast<size_t>(m) + 1));
+        std::memcpy(l_idx, L16.idx.get(), sizeof(int) * nnz);
+        std::memcpy(l_val16, L16.vals.get(), 2 * nnz);
+        stats[0] = st.dropped; stats[1] = st.dropped_flush; stats[2] = h16.flushed;
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
 }
 
 }  // extern "C"
