@@ -14,6 +14,7 @@
 #define APXB200_HPP
 
 #include <cstdint>
+#include <cstdlib>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -64,11 +65,25 @@ public:
         for (size_t i = 1; i < bounds.size(); ++i) rounds_.push_back(bounds[i] - bounds[i - 1]);
     }
 
+    // APXCHOL_SPTRSV_FP16, the reference's storage switch (cuda.h:186-205):
+    // 1 = fp16 storage, 0 = not, anything else / unset = -1 (the default).
+    static int fp16_env_tristate() {
+        const char* e = std::getenv("APXCHOL_SPTRSV_FP16");
+        if (!e) return -1;
+        return std::string(e) == "1" ? 1 : (std::string(e) == "0" ? 0 : -1);
+    }
+    static bool fp16_from_env() { return fp16_env_tristate() == 1; }
+    // The storage setup() picks by default. Unlike the reference (fp16 by
+    // default on its own kernels), the default here is the fp64 sweep, which
+    // reproduces the reference CPU backend bit for bit; =1 selects fp16.
+    static bool fp16_resolved() { return fp16_env_tristate() == 1; }
+    static int default_precision() { return fp16_resolved() ? APXB_PREC_FP16 : APXB_PREC_FP64; }
+
     // cuda_sptrsv::setup(const sparse_csc& L, node_index m) (cuda.h:233).
     // The sweeps run in the factor's permuted space, so no permutation is
     // needed here (identity); apply_perm() installs one for apply().
     template <class Csc>
-    void setup(const Csc& L, uint32_t m, int precision = APXB_PREC_FP64) {
+    void setup(const Csc& L, uint32_t m, int precision = default_precision()) {
         const uint32_t n = static_cast<uint32_t>(L.rows());
         if (m != n && m + 1 != n) throw std::runtime_error("cuda_sptrsv::setup: m must be n or n-1");
         if (perm_.size() != n) {
@@ -109,9 +124,9 @@ public:
     const char* backend_name() const { return "dataflow"; }
     const char* backend_reason() const { return "apxb200 sync-free dataflow sweeps (sm_100a)"; }
     bool backend_forced() const { return false; }
-    bool fp16() const { return false; }
+    bool fp16() const { return info_.precision == APXB_PREC_FP16; }
     static constexpr std::size_t value_bytes = 4;
-    std::size_t value_bytes_effective() const { return value_bytes; }
+    std::size_t value_bytes_effective() const { return fp16() ? 2 : value_bytes; }
     std::uint64_t factor_device_bytes() const { return info_.device_bytes; }
     apxb_factor* handle() const { return f_; }
     apxb_engine* engine_handle() const { return eng_ ? eng_->get() : nullptr; }
