@@ -26,6 +26,41 @@ bool keep_offdiag(float v, float s, double rel) {
     return std::fabs(static_cast<double>(v)) >= rel * static_cast<double>(s) && v != 0.0f;
 }
 
+// Threads for a pass over `work` items: 1 below a million, else up to 8.
+// APXB_PREP_THREADS=T (1..64) sets T whatever the size, so that tests can
+// compare the threaded passes with the serial ones on small inputs.
+unsigned prep_threads(uint64_t work) {
+    if (const char* e = std::getenv("APXB_PREP_THREADS")) {
+        const long t = std::strtol(e, nullptr, 10);
+        if (t >= 1 && t <= 64) return static_cast<unsigned>(t);
+    }
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    return work < (1u << 20) ? 1u : std::min(8u, hw);
+}
+
+// body(t) for t in [0, T), t = 0 on the calling thread.
+template <class F>
+void run_threads(unsigned T, F&& body) {
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < T; ++t) th.emplace_back(body, t);
+    body(0u);
+    for (auto& x : th) x.join();
+}
+
+// Column ranges of T threads with about equal entry counts: [jb[t], jb[t+1]).
+template <class P>
+std::vector<uint32_t> column_ranges(const P* ptr, uint32_t cols, unsigned T) {
+    std::vector<uint32_t> jb(T + 1, cols);
+    jb[0] = 0;
+    const uint64_t total = ptr[cols] - ptr[0];
+    for (unsigned t = 1; t < T; ++t) {
+        const uint64_t target = ptr[0] + total * t / T;
+        jb[t] = static_cast<uint32_t>(std::lower_bound(ptr, ptr + cols, target) - ptr);
+        jb[t] = std::max(jb[t], jb[t - 1]);
+    }
+    return jb;
+}
+
 // Plan of one direction (see sweep_plan). level[r] = level of row r in this
 // direction; (ptr, idx, val) = the canonical arrays of the direction (forward:
 // CSR(L11), diagonal last; backward: CSC(L11), diagonal first).
@@ -48,20 +83,36 @@ void relay_row(uint32_t r, bool forward, const std::vector<uint32_t>& ptr, const
     oi.push_back(idx[d]); ov.push_back(val[d]);
 }
 
+// Rows grouped by (level, class): levels ascending, classes 0..n_cls-1, rows
+// ascending inside a group -- one stable counting sort. cls[r] == n_cls leaves
+// row r out. start[l * n_cls + c] is where group (l, c) begins in rows.
+void group_rows(uint32_t m, const std::vector<int32_t>& level, int32_t n_levels, const std::vector<uint8_t>& cls,
+                uint32_t n_cls, std::vector<uint32_t>& rows, std::vector<uint32_t>& start) {
+    const size_t nk = static_cast<size_t>(n_levels) * n_cls;
+    start.assign(nk + 1, 0);
+    for (uint32_t r = 0; r < m; ++r)
+        if (cls[r] < n_cls) start[static_cast<size_t>(level[r]) * n_cls + cls[r] + 1]++;
+    for (size_t k = 0; k < nk; ++k) start[k + 1] += start[k];
+    rows.resize(start[nk]);
+    std::vector<uint32_t> cur(start.begin(), start.end() - 1);
+    for (uint32_t r = 0; r < m; ++r)
+        if (cls[r] < n_cls) rows[cur[static_cast<size_t>(level[r]) * n_cls + cls[r]]++] = r;
+}
+
 // val16 (fp16 storage, nullable): binary16 values beside val, re-laid the
 // same way into plan.val16; such plans have no serial segment.
 void build_plan(uint32_t m, const std::vector<int32_t>& level, int32_t n_levels, const std::vector<uint32_t>& bits,
                 const std::vector<uint32_t>& ptr, const std::vector<uint32_t>& idx, const std::vector<float>& val,
                 bool forward, bool contiguous, sweep_plan& plan, const std::vector<uint16_t>* val16 = nullptr) {
     if (val16) contiguous = false;
-    std::vector<std::vector<uint32_t>> by_level(static_cast<size_t>(n_levels));
-    for (uint32_t r = 0; r < m; ++r) by_level[level[r]].push_back(r);
     plan = sweep_plan{};
     // Serial segment: the trailing run (forward order) of small levels.
     int32_t seg_from = n_levels;   // in this direction's level numbering: forward [seg_from, n), backward [0, seg_to)
     int32_t seg_to = 0;
     const uint32_t seg_rows_max = seg_level_rows_setting();
     if (contiguous && seg_rows_max > 0) {
+        std::vector<std::vector<uint32_t>> by_level(static_cast<size_t>(n_levels));
+        for (uint32_t r = 0; r < m; ++r) by_level[level[r]].push_back(r);
         uint32_t rows = 0;
         int32_t nseg = 0;
         for (int32_t k = 0; k < n_levels; ++k) {            // k-th level from the forward end
@@ -75,70 +126,77 @@ void build_plan(uint32_t m, const std::vector<int32_t>& level, int32_t n_levels,
             if (forward) seg_from = n_levels - nseg;
             else seg_to = nseg;
         }
-    }
-    auto in_seg = [&](int32_t l) { return forward ? l >= seg_from : l < seg_to; };
-    if (seg_from < n_levels || seg_to > 0) {
-        plan.seg_first = m;
-        plan.seg_ptr.push_back(0);
-        for (int32_t l = 0; l < n_levels; ++l) {
-            if (!in_seg(l)) continue;
-            const auto& rows = by_level[l];
-            const uint32_t thin = rows.empty() ? 0u : (bits[rows[0] >> 5] >> (rows[0] & 31)) & 1u;
-            plan.seg_lvl.push_back(static_cast<uint32_t>(plan.seg_row.size()) | (thin << 31));
-            for (uint32_t r : rows) {
-                plan.seg_row.push_back(r);
-                plan.seg_first = std::min(plan.seg_first, r);
-                relay_row(r, forward, ptr, idx, val, plan.seg_idx, plan.seg_val);
-                plan.seg_ptr.push_back(static_cast<uint32_t>(plan.seg_idx.size()));
-            }
-        }
-        plan.seg_levels = static_cast<uint32_t>(plan.seg_lvl.size());
-        plan.seg_lvl.push_back(static_cast<uint32_t>(plan.seg_row.size()));
-        plan.seg_rows = static_cast<uint32_t>(plan.seg_row.size());
-        for (int32_t l = 0; l < n_levels; ++l)
-            if (in_seg(l)) std::vector<uint32_t>().swap(by_level[l]);
-    }
-    // items first: (level, G) groups cut into 32/G rows
-    std::vector<uint32_t> item_rows;   // rows, item by item (count from info)
-    item_rows.reserve(m);
-    for (int32_t l = 0; l < n_levels; ++l) {
-        auto& rows = by_level[l];
-        if (rows.empty()) continue;
-        const uint32_t thin = (bits[rows[0] >> 5] >> (rows[0] & 31)) & 1u;
-        for (uint32_t g : {32u, 16u, 8u, 4u, 1u}) {
-            const uint32_t cap = 32 / g;
-            uint32_t lg = 0;
-            while ((1u << lg) < g) ++lg;
-            uint32_t in_item = 0;
-            for (uint32_t r : rows) {
-                if (group_width(ptr[r + 1] - ptr[r] - 1) != g) continue;
-                item_rows.push_back(r);
-                if (++in_item == cap) {
-                    plan.info.push_back(in_item | (lg << 8) | (thin << 16));
-                    plan.item_level.push_back(l);
-                    in_item = 0;
+        auto in_seg = [&](int32_t l) { return forward ? l >= seg_from : l < seg_to; };
+        if (seg_from < n_levels || seg_to > 0) {
+            plan.seg_first = m;
+            plan.seg_ptr.push_back(0);
+            for (int32_t l = 0; l < n_levels; ++l) {
+                if (!in_seg(l)) continue;
+                const auto& lr = by_level[l];
+                const uint32_t thin = lr.empty() ? 0u : (bits[lr[0] >> 5] >> (lr[0] & 31)) & 1u;
+                plan.seg_lvl.push_back(static_cast<uint32_t>(plan.seg_row.size()) | (thin << 31));
+                for (uint32_t r : lr) {
+                    plan.seg_row.push_back(r);
+                    plan.seg_first = std::min(plan.seg_first, r);
+                    relay_row(r, forward, ptr, idx, val, plan.seg_idx, plan.seg_val);
+                    plan.seg_ptr.push_back(static_cast<uint32_t>(plan.seg_idx.size()));
                 }
             }
-            if (in_item) { plan.info.push_back(in_item | (lg << 8) | (thin << 16)); plan.item_level.push_back(l); }
+            plan.seg_levels = static_cast<uint32_t>(plan.seg_lvl.size());
+            plan.seg_lvl.push_back(static_cast<uint32_t>(plan.seg_row.size()));
+            plan.seg_rows = static_cast<uint32_t>(plan.seg_row.size());
         }
-        std::vector<uint32_t>().swap(rows);
+    }
+    auto in_seg = [&](int32_t l) { return forward ? l >= seg_from : l < seg_to; };
+    // items: (level, G) groups, G = 32, 16, 8, 4, 1 (classes 0..4), cut into 32/G rows
+    constexpr uint32_t kCls = 5;
+    std::vector<uint8_t> cls(m);
+    std::vector<uint32_t> first_row(static_cast<size_t>(n_levels), kNoRow);   // a level's smallest row (its thin bit)
+    for (uint32_t r = 0; r < m; ++r) {
+        const uint32_t g = group_width(ptr[r + 1] - ptr[r] - 1);
+        cls[r] = in_seg(level[r]) ? kCls : static_cast<uint8_t>(g == 1 ? 4 : 5 - __builtin_ctz(g));
+        if (first_row[level[r]] == kNoRow) first_row[level[r]] = r;
+    }
+    std::vector<uint32_t> item_rows, start;
+    group_rows(m, level, n_levels, cls, kCls, item_rows, start);
+    for (int32_t l = 0; l < n_levels; ++l) {
+        if (in_seg(l) || first_row[l] == kNoRow) continue;
+        const uint32_t thin = (bits[first_row[l] >> 5] >> (first_row[l] & 31)) & 1u;
+        for (uint32_t c = 0; c < kCls; ++c) {
+            const size_t key = static_cast<size_t>(l) * kCls + c;
+            const uint32_t lg = c == 4 ? 0u : 5u - c, cap = 32u >> lg;
+            for (uint32_t q = start[key]; q < start[key + 1]; q += cap) {
+                plan.info.push_back(std::min(cap, start[key + 1] - q) | (lg << 8) | (thin << 16));
+                plan.item_level.push_back(l);
+            }
+        }
     }
     plan.n_items = static_cast<uint32_t>(plan.info.size());
     const size_t npos = static_cast<size_t>(plan.n_items) * 32;
-    plan.ord.assign(npos, kNoRow);
-    plan.ptr.assign(npos + 1, 0);
-    plan.idx.resize(idx.size());
-    plan.val.resize(val.size());
-    if (val16) plan.val16.resize(val16->size());
-    size_t k = 0;      // index into item_rows
-    uint32_t e = 0;    // entry cursor
-    for (uint32_t c = 0; c < plan.n_items; ++c) {
-        const uint32_t cnt = plan.info[c] & 0xffu;
-        for (uint32_t s = 0; s < 32; ++s) {
-            const size_t pos = static_cast<size_t>(c) * 32 + s;
-            plan.ptr[pos] = e;
-            if (s < cnt) {
-                const uint32_t r = item_rows[k++];
+    plan.ord.resize(npos);      // uninitialized: every position is written below
+    plan.ptr.resize(npos + 1);
+    // entry offsets, then the items filled on T threads (see build_batch_plan)
+    std::vector<uint32_t> item_k(static_cast<size_t>(plan.n_items) + 1, 0);
+    for (uint32_t c = 0; c < plan.n_items; ++c) item_k[c + 1] = item_k[c] + (plan.info[c] & 0xffu);
+    std::vector<uint32_t> row_e(item_rows.size() + 1, 0);
+    for (size_t k = 0; k < item_rows.size(); ++k) row_e[k + 1] = row_e[k] + (ptr[item_rows[k] + 1] - ptr[item_rows[k]]);
+    const uint32_t total = row_e.back();
+    plan.idx.resize(total);
+    plan.val.resize(total);
+    if (val16) plan.val16.resize(total);
+    std::vector<uint32_t> item_e(static_cast<size_t>(plan.n_items) + 1);
+    for (uint32_t c = 0; c <= plan.n_items; ++c) item_e[c] = row_e[item_k[c]];
+    const unsigned T = prep_threads(total);
+    const std::vector<uint32_t> cb = column_ranges(item_e.data(), plan.n_items, T);
+    run_threads(T, [&](unsigned t) {
+        for (uint32_t c = cb[t]; c < cb[t + 1]; ++c) {
+            const uint32_t cnt = plan.info[c] & 0xffu;
+            for (uint32_t sl = 0; sl < 32; ++sl) {
+                const size_t pos = static_cast<size_t>(c) * 32 + sl;
+                if (sl >= cnt) { plan.ord[pos] = kNoRow; plan.ptr[pos] = row_e[item_k[c] + cnt]; continue; }
+                const uint32_t k = item_k[c] + sl, r = item_rows[k];
+                uint32_t e = row_e[k];
+                plan.ptr[pos] = e;
                 plan.ord[pos] = r;
                 const uint32_t b = ptr[r], en = ptr[r + 1];
                 const uint32_t d = forward ? en - 1 : b;                 // diagonal slot
@@ -150,14 +208,10 @@ void build_plan(uint32_t m, const std::vector<int32_t>& level, int32_t n_levels,
                 }
                 plan.idx[e] = idx[d]; plan.val[e] = val[d];             // diagonal last
                 if (val16) plan.val16[e] = (*val16)[d];
-                ++e;
             }
         }
-    }
-    plan.ptr[npos] = e;
-    plan.idx.resize(e);
-    plan.val.resize(e);
-    if (val16) plan.val16.resize(e);
+    });
+    plan.ptr[npos] = total;
     chunk_plan(plan);
 }
 
@@ -211,41 +265,6 @@ std::string check_plan(uint32_t m, const std::vector<int32_t>& level, const swee
     return {};
 }
 
-// Threads for a pass over `work` items: 1 below a million, else up to 8.
-// APXB_PREP_THREADS=T (1..64) sets T whatever the size, so that tests can
-// compare the threaded passes with the serial ones on small inputs.
-unsigned prep_threads(uint64_t work) {
-    if (const char* e = std::getenv("APXB_PREP_THREADS")) {
-        const long t = std::strtol(e, nullptr, 10);
-        if (t >= 1 && t <= 64) return static_cast<unsigned>(t);
-    }
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    return work < (1u << 20) ? 1u : std::min(8u, hw);
-}
-
-// body(t) for t in [0, T), t = 0 on the calling thread.
-template <class F>
-void run_threads(unsigned T, F&& body) {
-    std::vector<std::thread> th;
-    for (unsigned t = 1; t < T; ++t) th.emplace_back(body, t);
-    body(0u);
-    for (auto& x : th) x.join();
-}
-
-// Column ranges of T threads with about equal entry counts: [jb[t], jb[t+1]).
-template <class P>
-std::vector<uint32_t> column_ranges(const P* ptr, uint32_t cols, unsigned T) {
-    std::vector<uint32_t> jb(T + 1, cols);
-    jb[0] = 0;
-    const uint64_t total = ptr[cols] - ptr[0];
-    for (unsigned t = 1; t < T; ++t) {
-        const uint64_t target = ptr[0] + total * t / T;
-        jb[t] = static_cast<uint32_t>(std::lower_bound(ptr, ptr + cols, target) - ptr);
-        jb[t] = std::max(jb[t], jb[t - 1]);
-    }
-    return jb;
-}
-
 // APXB_PREP_TRACE=1: the time of each preparation stage on stderr.
 struct stage_clock {
     bool on = false;
@@ -287,64 +306,67 @@ void build_batch_plan(const prepared_factor& h, int dir, uint32_t col_lanes, swe
         while (ge * col_lanes < 32 && ge * 8 < len) ge *= 2;
         return ge * col_lanes;
     };
-    std::vector<std::vector<uint32_t>> by_level(static_cast<size_t>(n_levels));
-    for (uint32_t r = 0; r < m; ++r) by_level[level[r]].push_back(r);
+    // items: (level, G) groups, G = 32, 16, ..., col_lanes (class c: G = 32 >> c),
+    // cut into 32/G rows; rows ascending inside a group
+    uint32_t n_cls = 1;
+    while ((32u >> (n_cls - 1)) > col_lanes) ++n_cls;
+    std::vector<uint8_t> cls(m);
+    for (uint32_t r = 0; r < m; ++r) cls[r] = static_cast<uint8_t>(5 - __builtin_ctz(width(r)));
+    std::vector<uint32_t> item_rows, start;
+    group_rows(m, level, n_levels, cls, n_cls, item_rows, start);
     plan = sweep_plan{};
-    std::vector<uint32_t> item_rows;
-    item_rows.reserve(m);
-    for (int32_t l = 0; l < n_levels; ++l) {
-        auto& rows = by_level[l];
-        for (uint32_t g = 32; g >= col_lanes && g >= 1; g /= 2) {
-            const uint32_t cap = 32 / g;
-            uint32_t lg = 0;
-            while ((1u << lg) < g) ++lg;
-            uint32_t in_item = 0;
-            for (uint32_t r : rows) {
-                if (width(r) != g) continue;
-                item_rows.push_back(r);
-                if (++in_item == cap) {
-                    plan.info.push_back(in_item | (lg << 8));
-                    plan.item_level.push_back(l);
-                    in_item = 0;
-                }
+    for (int32_t l = 0; l < n_levels; ++l)
+        for (uint32_t c = 0; c < n_cls; ++c) {
+            const size_t key = static_cast<size_t>(l) * n_cls + c;
+            const uint32_t lg = 5u - c, cap = 32u >> lg;
+            for (uint32_t q = start[key]; q < start[key + 1]; q += cap) {
+                plan.info.push_back(std::min(cap, start[key + 1] - q) | (lg << 8));
+                plan.item_level.push_back(l);
             }
-            if (in_item) { plan.info.push_back(in_item | (lg << 8)); plan.item_level.push_back(l); }
-            if (g == 1) break;
         }
-        std::vector<uint32_t>().swap(rows);
-    }
     plan.n_items = static_cast<uint32_t>(plan.info.size());
     const size_t npos = static_cast<size_t>(plan.n_items) * 32;
-    plan.ord.assign(npos, kNoRow);
-    plan.ptr.assign(npos + 1, 0);
-    plan.idx.resize(idx.size());
-    plan.val.resize(val.size());
-    size_t k = 0;
-    uint32_t e = 0;
-    std::vector<std::pair<int32_t, uint32_t>> order;   // (dependency level, position in the row)
-    for (uint32_t c = 0; c < plan.n_items; ++c) {
-        const uint32_t cnt = plan.info[c] & 0xffu;
-        for (uint32_t sl = 0; sl < 32; ++sl) {
-            const size_t pos = static_cast<size_t>(c) * 32 + sl;
-            plan.ptr[pos] = e;
-            if (sl >= cnt) continue;
-            const uint32_t r = item_rows[k++];
-            plan.ord[pos] = r;
-            const uint32_t b = ptr[r], en = ptr[r + 1];
-            const uint32_t d = forward ? en - 1 : b;
-            order.clear();
-            for (uint32_t p = b; p < en; ++p)
-                if (p != d) order.emplace_back(level[idx[p]], p);
-            std::sort(order.begin(), order.end(), [&](const auto& x, const auto& y) {
-                return x.first != y.first ? x.first < y.first : idx[x.second] < idx[y.second];
-            });
-            for (const auto& o : order) { plan.idx[e] = idx[o.second]; plan.val[e] = val[o.second]; ++e; }
-            plan.idx[e] = idx[d]; plan.val[e] = val[d]; ++e;
+    plan.ord.resize(npos);      // uninitialized: every position is written below
+    plan.ptr.resize(npos + 1);
+    // Entry offsets first (row k of item_rows starts at row_e[k], item c's rows
+    // at item_k[c]), then the items are filled on T threads, each over a range
+    // of items with about equal entry counts: the same arrays as one pass.
+    std::vector<uint32_t> item_k(static_cast<size_t>(plan.n_items) + 1, 0);
+    for (uint32_t c = 0; c < plan.n_items; ++c) item_k[c + 1] = item_k[c] + (plan.info[c] & 0xffu);
+    std::vector<uint32_t> row_e(item_rows.size() + 1, 0);
+    for (size_t k = 0; k < item_rows.size(); ++k) row_e[k + 1] = row_e[k] + (ptr[item_rows[k] + 1] - ptr[item_rows[k]]);
+    const uint32_t total = row_e.back();
+    plan.idx.resize(total);
+    plan.val.resize(total);
+    std::vector<uint32_t> item_e(static_cast<size_t>(plan.n_items) + 1);
+    for (uint32_t c = 0; c <= plan.n_items; ++c) item_e[c] = row_e[item_k[c]];
+    const unsigned T = prep_threads(total);
+    const std::vector<uint32_t> cb = column_ranges(item_e.data(), plan.n_items, T);
+    run_threads(T, [&](unsigned t) {
+        std::vector<std::pair<int32_t, uint32_t>> order;   // (dependency level, position in the row)
+        for (uint32_t c = cb[t]; c < cb[t + 1]; ++c) {
+            const uint32_t cnt = plan.info[c] & 0xffu;
+            for (uint32_t sl = 0; sl < 32; ++sl) {
+                const size_t pos = static_cast<size_t>(c) * 32 + sl;
+                if (sl >= cnt) { plan.ord[pos] = kNoRow; plan.ptr[pos] = row_e[item_k[c] + cnt]; continue; }
+                const uint32_t k = item_k[c] + sl, r = item_rows[k];
+                uint32_t e = row_e[k];
+                plan.ptr[pos] = e;
+                plan.ord[pos] = r;
+                const uint32_t b = ptr[r], en = ptr[r + 1];
+                const uint32_t d = forward ? en - 1 : b;
+                order.clear();
+                for (uint32_t p = b; p < en; ++p)
+                    if (p != d) order.emplace_back(level[idx[p]], p);
+                std::sort(order.begin(), order.end(), [&](const auto& x, const auto& y) {
+                    return x.first != y.first ? x.first < y.first : idx[x.second] < idx[y.second];
+                });
+                for (const auto& o : order) { plan.idx[e] = idx[o.second]; plan.val[e] = val[o.second]; ++e; }
+                plan.idx[e] = idx[d]; plan.val[e] = val[d];
+            }
         }
-    }
-    plan.ptr[npos] = e;
-    plan.idx.resize(e);
-    plan.val.resize(e);
+    });
+    plan.ptr[npos] = total;
     chunk_plan(plan);
 }
 
@@ -638,6 +660,13 @@ std::string permute_operator(uint32_t n, const int32_t* colptr, const int32_t* r
     if (colptr[0] != 0) return "operator colptr[0] != 0";
     const int64_t nnz = colptr[n];
     if (nnz < 0 || nnz > INT32_MAX) return "operator nnz out of the int32 range";
+    {
+        std::vector<uint8_t> seen(n, 0);
+        for (uint32_t v = 0; v < n; ++v) {
+            if (perm[v] >= n || seen[perm[v]]) return "perm is not a permutation of [0, n)";
+            seen[perm[v]] = 1;
+        }
+    }
     // A is symmetric, so its CSC column j is its CSR row j. Row perm[j] of
     // P A P^T holds the entries of row j with columns mapped through perm.
     ptr.assign(static_cast<size_t>(n) + 1, 0);
@@ -648,18 +677,26 @@ std::string permute_operator(uint32_t n, const int32_t* colptr, const int32_t* r
     for (uint32_t i = 0; i < n; ++i) ptr[i + 1] += ptr[i];
     idx.resize(nnz);
     val.resize(nnz);
-    std::vector<std::pair<int32_t, double>> row;
-    for (uint32_t j = 0; j < n; ++j) {
-        row.clear();
-        for (int32_t p = colptr[j]; p < colptr[j + 1]; ++p) {
-            const int32_t r = rowidx[p];
-            if (r < 0 || static_cast<uint32_t>(r) >= n) return "operator row index out of range";
-            row.emplace_back(static_cast<int32_t>(perm[r]), vals[p]);
+    // Rows are independent: T threads over column ranges of equal entry counts.
+    const unsigned T = prep_threads(static_cast<uint64_t>(nnz));
+    const std::vector<uint32_t> jb = column_ranges(colptr, n, T);
+    std::vector<uint8_t> bad(T, 0);
+    run_threads(T, [&](unsigned t) {
+        std::vector<std::pair<int32_t, double>> row;
+        for (uint32_t j = jb[t]; j < jb[t + 1]; ++j) {
+            row.clear();
+            for (int32_t p = colptr[j]; p < colptr[j + 1]; ++p) {
+                const int32_t r = rowidx[p];
+                if (r < 0 || static_cast<uint32_t>(r) >= n) { bad[t] = 1; return; }
+                row.emplace_back(static_cast<int32_t>(perm[r]), vals[p]);
+            }
+            std::sort(row.begin(), row.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+            int32_t o = ptr[perm[j]];
+            for (const auto& [c, v] : row) { idx[o] = c; val[o] = v; ++o; }
         }
-        std::sort(row.begin(), row.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
-        int32_t o = ptr[perm[j]];
-        for (const auto& [c, v] : row) { idx[o] = c; val[o] = v; ++o; }
-    }
+    });
+    for (unsigned t = 0; t < T; ++t)
+        if (bad[t]) return "operator row index out of range";
     return {};
 }
 

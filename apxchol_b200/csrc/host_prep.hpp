@@ -18,7 +18,10 @@
 #pragma once
 #include <cstdint>
 #include <cstring>
+#include <memory>
+#include <new>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace apxb {
@@ -79,6 +82,24 @@ inline uint16_t fp16_narrow(float v, float s) {
     return (h & 0x7c00u) == 0 ? static_cast<uint16_t>(h & 0x8000u) : h;
 }
 
+// std::allocator whose value-less construct leaves the element uninitialized:
+// resize() then costs no serial zero-fill, and the threads that write the
+// array (every element) touch its pages first.
+template <class T>
+struct uninit_alloc : std::allocator<T> {
+    template <class U>
+    struct rebind { using other = uninit_alloc<U>; };
+    uninit_alloc() = default;
+    template <class U>
+    uninit_alloc(const uninit_alloc<U>&) noexcept {}
+    template <class U>
+    void construct(U* p) noexcept { ::new (static_cast<void*>(p)) U; }
+    template <class U, class... A>
+    void construct(U* p, A&&... a) { ::new (static_cast<void*>(p)) U(std::forward<A>(a)...); }
+};
+template <class T>
+using plan_vec = std::vector<T, uninit_alloc<T>>;
+
 // Execution plan of one sweep direction, in the layout the dataflow kernels
 // read.
 //  * Rows are scheduled level by level; inside a level by lane-group width G
@@ -108,11 +129,11 @@ struct sweep_plan {
     std::vector<int32_t> item_level;   // level of each item (host side; batch plans)
     std::vector<uint32_t> chunk;       // claim units of batch plans: chunk c = items [chunk[c], chunk[c+1])
     std::vector<uint32_t> info;
-    std::vector<uint32_t> ord;
-    std::vector<uint32_t> ptr;
-    std::vector<uint32_t> idx;
-    std::vector<float> val;
-    std::vector<uint16_t> val16;       // fp16 storage: the binary16 values, same layout as val
+    plan_vec<uint32_t> ord;
+    plan_vec<uint32_t> ptr;
+    plan_vec<uint32_t> idx;
+    plan_vec<float> val;
+    plan_vec<uint16_t> val16;          // fp16 storage: the binary16 values, same layout as val
     uint32_t seg_first = 0, seg_rows = 0, seg_levels = 0;
     std::vector<uint32_t> seg_row, seg_lvl, seg_ptr, seg_idx;
     std::vector<float> seg_val;
