@@ -445,84 +445,111 @@ std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* r
     clk.mark("validate");
     // L11 (drop row n-1 for a Laplacian), then the compacting drop, written
     // straight into the CSC arrays; with fp16 storage each column is then
-    // narrowed (cuda_host.h:202-232).
+    // narrowed (cuda_host.h:202-232). Columns are independent: pass 1 counts
+    // what each keeps, a prefix sum places them, pass 2 writes them -- on T
+    // threads over column ranges (factor_drop.h:131-211 has the same shape).
     std::vector<uint32_t>& cp = out.csc_ptr;
     std::vector<uint32_t>& ci = out.csc_idx;
     std::vector<float>& cv = out.csc_val;
     std::vector<uint16_t>& ch = out.csc_h;
     cp.assign(static_cast<size_t>(m) + 1, 0);
-    ci.reserve(colptr[m]);
-    cv.reserve(colptr[m]);
+    // a Laplacian's L11 leaves out row n-1: the column's last row when present
+    auto col_end = [&](uint32_t j) {
+        uint32_t e = colptr[j + 1];
+        if (!sddm && e > colptr[j] + 1 && rowidx[e - 1] == n - 1) --e;
+        return e;
+    };
+    // fp16 storage also drops what it would flush (cuda_host.h:135-139)
+    auto kept = [&](float v, float s) { return keep_offdiag(v, s, rel) && !(fp16 && fp16_flushes(v / s)); };
+    std::vector<float> col_s(m);
+    const unsigned TD = prep_threads(colptr[m]);
+    const std::vector<uint32_t> jd = column_ranges(colptr, m, TD);
+    std::vector<uint64_t> nf_t(TD), dr_t(TD), df_t(TD), fl_t(TD);
+    run_threads(TD, [&](unsigned t) {
+        uint64_t nf = 0;
+        for (uint32_t j = jd[t]; j < jd[t + 1]; ++j) {
+            const uint32_t b = colptr[j], e = col_end(j);
+            nf += e - b;
+            float s = 1.0f;   // the column's scale, taken before the drop
+            if (rel > 0.0 || fp16) {
+                s = column_scale(vals, b, e);
+                // fp16 storage: a scale whose 1/s or diagonal/s overflows fp32
+                // falls back to 1, before the drop (cuda.h:287-301)
+                if (fp16 && (!std::isfinite(1.0f / s) || !std::isfinite(vals[b] / s))) s = 1.0f;
+            }
+            col_s[j] = s;
+            uint32_t k = e - b;
+            if (rel > 0.0) {
+                k = 1;                                     // the diagonal, first in the column
+                for (uint32_t p = b + 1; p < e; ++p) k += kept(vals[p], s) ? 1u : 0u;
+            }
+            cp[j + 1] = k;
+        }
+        nf_t[t] = nf;
+    });
+    for (uint32_t j = 0; j < m; ++j) cp[j + 1] += cp[j];
+    ci.resize(cp[m]);
+    cv.resize(cp[m]);
     if (fp16) {
-        ch.reserve(colptr[m]);
+        ch.resize(cp[m]);
         out.diag16.resize(m);
         out.inv_scale.resize(m);
     }
-    std::vector<uint32_t> rows;
-    std::vector<float> vs;
-    uint64_t nnz_factor = 0, dropped = 0, dropped_flush = 0, flushed = 0;
-    for (uint32_t j = 0; j < m; ++j) {
-        rows.clear(); vs.clear();
-        for (uint32_t p = colptr[j]; p < colptr[j + 1]; ++p) {
-            if (!sddm && rowidx[p] == n - 1) continue;
-            rows.push_back(rowidx[p]); vs.push_back(vals[p]);
-        }
-        nnz_factor += rows.size();
-        const size_t first = ci.size();
-        float s = 1.0f;   // the column's scale, taken before the drop
-        if (rel > 0.0 || fp16) {
-            s = column_scale(vs.data(), 0, static_cast<uint32_t>(vs.size()));
-            // fp16 storage: a scale whose 1/s or diagonal/s overflows fp32 falls
-            // back to 1, before the drop (cuda.h:287-301)
-            if (fp16 && (!std::isfinite(1.0f / s) || !std::isfinite(vs[0] / s))) s = 1.0f;
-        }
-        if (rel > 0.0) {
-            double dropped_sum = 0.0, kept_abs = 0.0;
-            for (size_t t = 0; t < rows.size(); ++t) {
-                const float v = vs[t];
-                if (rows[t] != j) {
-                    // fp16 storage also drops what it would flush (cuda_host.h:135-139)
-                    if (!keep_offdiag(v, s, rel) || (fp16 && fp16_flushes(v / s))) {
-                        if (std::fabs(static_cast<double>(v)) >= rel * static_cast<double>(s)) ++dropped_flush;
-                        dropped_sum += static_cast<double>(v);
-                        ++dropped;
-                        continue;
+    run_threads(TD, [&](unsigned t) {
+        uint64_t dr = 0, df = 0, fl = 0;
+        for (uint32_t j = jd[t]; j < jd[t + 1]; ++j) {
+            const uint32_t b = colptr[j], e = col_end(j), first = cp[j];
+            const float s = col_s[j];
+            uint32_t o = first;
+            if (rel > 0.0) {
+                double dropped_sum = 0.0, kept_abs = 0.0;
+                for (uint32_t p = b; p < e; ++p) {
+                    const float v = vals[p];
+                    if (p != b) {
+                        if (!kept(v, s)) {
+                            if (std::fabs(static_cast<double>(v)) >= rel * static_cast<double>(s)) ++df;
+                            dropped_sum += static_cast<double>(v);
+                            ++dr;
+                            continue;
+                        }
+                        kept_abs += std::fabs(static_cast<double>(v));
                     }
-                    kept_abs += std::fabs(static_cast<double>(v));
+                    ci[o] = rowidx[p]; cv[o] = v; ++o;
                 }
-                ci.push_back(rows[t]); cv.push_back(v);
-            }
-            if (dropped_sum != 0.0 && kept_abs > 0.0) {
-                const double per_abs = dropped_sum / kept_abs;
-                for (size_t q = first; q < ci.size(); ++q) {
-                    if (ci[q] == j) continue;
-                    const double v = static_cast<double>(cv[q]);
-                    cv[q] = static_cast<float>(v + per_abs * std::fabs(v));
+                if (dropped_sum != 0.0 && kept_abs > 0.0) {
+                    const double per_abs = dropped_sum / kept_abs;
+                    for (uint32_t q = first + 1; q < o; ++q) {
+                        const double v = static_cast<double>(cv[q]);
+                        cv[q] = static_cast<float>(v + per_abs * std::fabs(v));
+                    }
                 }
+            } else {
+                for (uint32_t p = b; p < e; ++p) { ci[o] = rowidx[p]; cv[o] = vals[p]; ++o; }
             }
-        } else {
-            ci.insert(ci.end(), rows.begin(), rows.end());
-            cv.insert(cv.end(), vs.begin(), vs.end());
-        }
-        if (fp16) {
-            // off-diagonals as binary16(v / s); the diagonal (first in the
-            // column) as fp32 d / s plus the column's rounding residual, so the
-            // stored column sums to what the fp32 column sums to
-            const float d = cv[first] / s;
-            double resid = 0.0;
-            for (size_t q = first; q < ci.size(); ++q) {
-                const float v = cv[q];
-                const uint16_t h = fp16_narrow(v, s);
-                ch.push_back(h);                  // the diagonal's slot too (never read)
-                if (ci[q] == j) continue;
-                const float w = fp16_value(h);
-                if (v != 0.0f && w == 0.0f) ++flushed;
-                resid += static_cast<double>(v) / static_cast<double>(s) - static_cast<double>(w);
+            if (fp16) {
+                // off-diagonals as binary16(v / s); the diagonal as fp32 d / s
+                // plus the column's rounding residual, so the stored column sums
+                // to what the fp32 column sums to
+                const float d = cv[first] / s;
+                ch[first] = fp16_narrow(cv[first], s);      // the diagonal's slot (never read)
+                double resid = 0.0;
+                for (uint32_t q = first + 1; q < o; ++q) {
+                    const float v = cv[q];
+                    const uint16_t h = fp16_narrow(v, s);
+                    ch[q] = h;
+                    const float w = fp16_value(h);
+                    if (v != 0.0f && w == 0.0f) ++fl;
+                    resid += static_cast<double>(v) / static_cast<double>(s) - static_cast<double>(w);
+                }
+                out.diag16[j] = static_cast<float>(static_cast<double>(d) + resid);
+                out.inv_scale[j] = 1.0f / s;
             }
-            out.diag16[j] = static_cast<float>(static_cast<double>(d) + resid);
-            out.inv_scale[j] = 1.0f / s;
         }
-        cp[j + 1] = static_cast<uint32_t>(ci.size());
+        dr_t[t] = dr; df_t[t] = df; fl_t[t] = fl;
+    });
+    uint64_t nnz_factor = 0, dropped = 0, dropped_flush = 0, flushed = 0;
+    for (unsigned t = 0; t < TD; ++t) {
+        nnz_factor += nf_t[t]; dropped += dr_t[t]; dropped_flush += df_t[t]; flushed += fl_t[t];
     }
     out.nnz_factor = nnz_factor;
     out.nnz_stored = ci.size();
@@ -543,20 +570,34 @@ std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* r
     {
         const unsigned T = prep_threads(nnz);
         const std::vector<uint32_t> jb = column_ranges(cp.data(), m, T);
-        std::vector<std::vector<uint32_t>> cnt(T, std::vector<uint32_t>(m, 0));
+        std::vector<std::vector<uint32_t>> cnt(T);
         run_threads(T, [&](unsigned t) {
+            cnt[t].assign(m, 0);
             for (uint32_t p = cp[jb[t]]; p < cp[jb[t + 1]]; ++p) cnt[t][ci[p]]++;
         });
-        // row starts, then each thread's offset inside every row
-        for (uint32_t i = 0; i < m; ++i) {
-            uint32_t acc = out.csr_ptr[i];
-            for (unsigned t = 0; t < T; ++t) {
-                const uint32_t c = cnt[t][i];
-                cnt[t][i] = acc;
-                acc += c;
+        // row lengths, row starts, then each thread's offset inside every row
+        // (threads over row ranges)
+        std::vector<uint32_t> len(m);
+        run_threads(T, [&](unsigned t) {
+            const uint32_t i1 = static_cast<uint32_t>(static_cast<uint64_t>(m) * (t + 1) / T);
+            for (uint32_t i = static_cast<uint32_t>(static_cast<uint64_t>(m) * t / T); i < i1; ++i) {
+                uint32_t c = 0;
+                for (unsigned u = 0; u < T; ++u) c += cnt[u][i];
+                len[i] = c;
             }
-            out.csr_ptr[i + 1] = acc;
-        }
+        });
+        for (uint32_t i = 0; i < m; ++i) out.csr_ptr[i + 1] = out.csr_ptr[i] + len[i];
+        run_threads(T, [&](unsigned t) {
+            const uint32_t i1 = static_cast<uint32_t>(static_cast<uint64_t>(m) * (t + 1) / T);
+            for (uint32_t i = static_cast<uint32_t>(static_cast<uint64_t>(m) * t / T); i < i1; ++i) {
+                uint32_t acc = out.csr_ptr[i];
+                for (unsigned u = 0; u < T; ++u) {
+                    const uint32_t c = cnt[u][i];
+                    cnt[u][i] = acc;
+                    acc += c;
+                }
+            }
+        });
         run_threads(T, [&](unsigned t) {
             std::vector<uint32_t>& cur = cnt[t];
             for (uint32_t j = jb[t]; j < jb[t + 1]; ++j)
