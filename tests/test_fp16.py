@@ -76,6 +76,26 @@ def test_fp16_storage_wide_magnitudes(sddm, rel):
         assert ours["stats"][1] > 0          # the fp16 keep clause drops what fp16 flushes
 
 
+@needs_ref
+@pytest.mark.parametrize("rel", [-1.0, 0.0])
+def test_fp16_scale_fallback(rel):
+    """Columns whose off-diagonals are ~1e-39 (fp32 subnormals): 1/s overflows
+    fp32, so s falls back to 1 (cuda.h:287-301) and their off-diagonals flush
+    to zero, folded into the diagonal."""
+    F = _wide_factor(2000, 21, True)
+    tiny = np.array([1e-39, 5e-40, 1e-40], np.float32)   # 1/s >= 1e39 overflows fp32
+    hit = []
+    for j in range(0, 1900, 37):
+        lo, hi = int(F.colptr[j]), int(F.colptr[j + 1])
+        if hi - lo > 1:
+            F.vals[lo + 1:hi] = -tiny[np.arange(hi - lo - 1) % 3]
+            hit.append(j)
+    ours = native.prepare_host_fp16(F, rel)
+    _same(ours, oracle.fp16_prep(F, rel))
+    assert len(hit) > 10
+    assert all(ours["inv_scale"][j] == 1.0 for j in hit)
+
+
 def test_fp16_values_and_folded_diagonal():
     """Self-checks of the contract without the reference: each stored
     off-diagonal is binary16(v / s) of the fp32 column (numpy's IEEE
