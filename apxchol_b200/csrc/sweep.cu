@@ -685,8 +685,25 @@ __device__ __forceinline__ void load_wide(const sweep_args<float>& a, const stag
     }
 }
 
+// L2 prefetch of the dependency rows the lane will gather for its next item
+// (whose indices arrived while the current item ran). A prefetch holds no
+// register and L2 is the point of coherence, so the later relaxed load still
+// sees whatever the row holds then, solved or not.
+template <int K>
+__device__ __forceinline__ void prefetch_wide(const sweep_args<float>& a, const stage_wide<K>& s) {
+    using W = wide_cfg<K>;
+    const lane_view& v = s.v;
+    if (v.c >= a.n_items) return;
+    const size_t col = static_cast<size_t>(s.cl) * W::KC;
+#pragma unroll
+    for (int k = 0; k < W::B; ++k) {
+        const uint32_t t = (static_cast<uint32_t>(k) << s.glg) + s.ue;
+        if (t < v.len) asm volatile("prefetch.global.L2 [%0];" ::"l"(a.out + static_cast<size_t>(s.jj[k]) * K + col));
+    }
+}
+
 template <int DIR, int K>
-__device__ __forceinline__ bool run_wide(const sweep_args<float>& a, stage_wide<K>& s) {
+__device__ __forceinline__ bool run_wide(const sweep_args<float>& a, stage_wide<K>& s, const stage_wide<K>& next) {
     using W = wide_cfg<K>;
     constexpr int B = W::B, KC = W::KC;
     const lane_view& v = s.v;
@@ -713,6 +730,7 @@ __device__ __forceinline__ bool run_wide(const sweep_args<float>& a, stage_wide<
 #pragma unroll
         for (int k = 0; k < B; ++k)
             if (static_cast<uint32_t>(k) < nk) ld_row<KC>(a.out + static_cast<size_t>(s.jj[k]) * K + col, yv[k]);
+        if (jb == 0) prefetch_wide<K>(a, next);   // the next item's gathers start while these are in flight
         uint32_t kpos = 0;
         for (;;) {
             const uint32_t before = kpos;
@@ -774,7 +792,7 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_dw32(const sweep_args<floa
         load_desc(a, cc.next(a), dD);
         if (__shfl_sync(kFull, bad, 0)) break;
         if (lane == 0) bad = ld_relaxed_int(&a.err->code);
-        if (!run_wide<DIR, K>(a, sR)) break;
+        if (!run_wide<DIR, K>(a, sR, sL)) break;
     }
     leave(a.ctl);
 }
