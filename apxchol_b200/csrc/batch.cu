@@ -19,7 +19,6 @@
 //  * The iteration is a CUDA graph; a full solve runs it under a conditional
 //    WHILE node until every slot is done.
 #include <algorithm>
-#include <thread>
 
 #include "objects.hpp"
 
@@ -1085,196 +1084,195 @@ extern "C" {
 
 int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, apxb_operator* const* ops, int k,
                       apxb_batch** out) {
-    if (!e || n_inst < 1 || !factors || !ops || !out) return fail(APXB_ERR_INVALID, "bad argument");
-    if (k != 1 && k != 2 && k != 4 && k != 8 && k != 16) return fail(APXB_ERR_INVALID, "k must be 1, 2, 4, 8 or 16");
-    *out = nullptr;
-    APXB_CK(cudaSetDevice(e->device));
-    std::unique_ptr<apxb_batch> bt(new (std::nothrow) apxb_batch);
-    if (!bt) return fail(APXB_ERR_INVALID, "host allocation failed");
-    bt->e = e; bt->S = n_inst; bt->K = k;
-    std::vector<const apxb_factor*> fs;
-    uint64_t nnz_a = 0;
-    for (int i = 0; i < n_inst; ++i) {
-        const apxb_factor* f = factors[i];
-        const apxb_operator* a = ops[i];
-        if (!f || !a || f->e != e || a->e != e) return fail(APXB_ERR_INVALID, "instance objects missing or on another engine");
-        if (a->n != f->h.n) return fail(APXB_ERR_INVALID, "instance operator / factor dimensions differ");
-        bt->off.push_back(bt->n_tot);
-        bt->n.push_back(f->h.n);
-        bt->lap.push_back(f->h.sddm ? 0 : 1);
-        bt->n_tot += f->h.n;
-        nnz_a += a->nnz;
-        fs.push_back(f);
-    }
-    if (nnz_a >= 0x7fffffffull) return fail(APXB_ERR_INVALID, "combined operator exceeds the int32 range");
-    cudaStream_t s = e->stream;
-    const size_t nk = static_cast<size_t>(bt->n_tot) * k, ns = bt->slots();
-    int rc;
-    // ---- sweep plans (batch plans for this k; the two directions on two threads) ----
-    {
-        const uint32_t col_lanes = k >= 8 ? static_cast<uint32_t>(k / 4) : 1u;
-        apxb::sweep_plan plans[2];
-        std::string bad[2];
-        {
-            auto make = [&](int dir) {
-                batch_plan(fs, bt->off, dir, col_lanes, plans[dir]);
-                if (n_inst == 1)
-                    bad[dir] = apxb::check_batch_plan(fs[0]->h.m, dir == 0 ? fs[0]->h.fwd_level : fs[0]->h.bck_level,
-                                                      plans[dir], col_lanes);
-            };
-            std::thread bck(make, 1);
-            make(0);
-            bck.join();
-        }
-        for (int dir = 0; dir < 2; ++dir) {
-            const apxb::sweep_plan& pl = plans[dir];
-            if (!bad[dir].empty()) return fail(APXB_ERR_INVALID, "internal batch plan error: " + bad[dir]);
-            uint32_t *info, *ord, *ptr, *idx, *chunk;
-            float* val;
-            if ((rc = bt->dalloc(&info, pl.info.size())) || (rc = bt->dalloc(&ord, pl.ord.size())) ||
-                (rc = bt->dalloc(&ptr, pl.ptr.size())) || (rc = bt->dalloc(&idx, pl.idx.size())) ||
-                (rc = bt->dalloc(&val, pl.val.size())) || (rc = bt->dalloc(&chunk, pl.chunk.size())))
-                return rc;
-            APXB_CK(cudaMemcpyAsync(info, pl.info.data(), 4 * pl.info.size(), cudaMemcpyHostToDevice, s));
-            APXB_CK(cudaMemcpyAsync(ord, pl.ord.data(), 4 * pl.ord.size(), cudaMemcpyHostToDevice, s));
-            APXB_CK(cudaMemcpyAsync(ptr, pl.ptr.data(), 4 * pl.ptr.size(), cudaMemcpyHostToDevice, s));
-            APXB_CK(cudaMemcpyAsync(idx, pl.idx.data(), 4 * pl.idx.size(), cudaMemcpyHostToDevice, s));
-            APXB_CK(cudaMemcpyAsync(val, pl.val.data(), 4 * pl.val.size(), cudaMemcpyHostToDevice, s));
-            APXB_CK(cudaMemcpyAsync(chunk, pl.chunk.data(), 4 * pl.chunk.size(), cudaMemcpyHostToDevice, s));
-            APXB_CK(cudaStreamSynchronize(s));
-            bt->n_items[dir] = pl.n_items;
-            bt->info[dir] = info; bt->ord[dir] = ord; bt->ptr[dir] = ptr; bt->idx[dir] = idx; bt->val[dir] = val;
-            bt->chunk[dir] = chunk; bt->n_chunks[dir] = static_cast<uint32_t>(pl.chunk.size() - 1);
-        }
-    }
-    if ((rc = bt->dalloc(&bt->ctl, 2))) return rc;
-    APXB_CK(cudaMemsetAsync(bt->ctl, 0, sizeof(apxb::sweep_ctl) * 2, s));
-    bt->grid32 = e->sweep_grid > 0 ? e->sweep_grid : apxb::sweep_grid32_batch(k, e->num_sms);
-    // ---- operator ----
-    if (n_inst == 1) {
-        bt->a_ptr = ops[0]->ptr; bt->a_idx = ops[0]->idx; bt->a_val = ops[0]->val;
-    } else {
-        int32_t *ap, *ai;
-        double* av;
-        if ((rc = bt->dalloc(&ap, bt->n_tot + 1)) || (rc = bt->dalloc(&ai, nnz_a)) || (rc = bt->dalloc(&av, nnz_a)))
-            return rc;
-        std::vector<int32_t> hp(bt->n_tot + 1, 0);
-        uint64_t base = 0;
+    return guarded([&]() -> int {
+        if (!e || n_inst < 1 || !factors || !ops || !out) return fail(APXB_ERR_INVALID, "bad argument");
+        if (k != 1 && k != 2 && k != 4 && k != 8 && k != 16) return fail(APXB_ERR_INVALID, "k must be 1, 2, 4, 8 or 16");
+        *out = nullptr;
+        APXB_CK(cudaSetDevice(e->device));
+        std::unique_ptr<apxb_batch> bt(new (std::nothrow) apxb_batch);
+        if (!bt) return fail(APXB_ERR_INVALID, "host allocation failed");
+        bt->e = e; bt->S = n_inst; bt->K = k;
+        std::vector<const apxb_factor*> fs;
+        uint64_t nnz_a = 0;
         for (int i = 0; i < n_inst; ++i) {
+            const apxb_factor* f = factors[i];
             const apxb_operator* a = ops[i];
-            std::vector<int32_t> p(a->n + 1), ix(a->nnz);
-            APXB_CK(cudaMemcpy(p.data(), a->ptr, 4 * (static_cast<size_t>(a->n) + 1), cudaMemcpyDeviceToHost));
-            APXB_CK(cudaMemcpy(ix.data(), a->idx, 4 * a->nnz, cudaMemcpyDeviceToHost));
-            for (uint32_t r = 0; r <= a->n; ++r) hp[bt->off[i] + r] = static_cast<int32_t>(base + p[r]);
-            for (auto& c : ix) c += static_cast<int32_t>(bt->off[i]);
-            APXB_CK(cudaMemcpy(ai + base, ix.data(), 4 * a->nnz, cudaMemcpyHostToDevice));
-            APXB_CK(cudaMemcpy(av + base, a->val, 8 * a->nnz, cudaMemcpyDeviceToDevice));
-            base += a->nnz;
+            if (!f || !a || f->e != e || a->e != e) return fail(APXB_ERR_INVALID, "instance objects missing or on another engine");
+            if (a->n != f->h.n) return fail(APXB_ERR_INVALID, "instance operator / factor dimensions differ");
+            bt->off.push_back(bt->n_tot);
+            bt->n.push_back(f->h.n);
+            bt->lap.push_back(f->h.sddm ? 0 : 1);
+            bt->n_tot += f->h.n;
+            nnz_a += a->nnz;
+            fs.push_back(f);
         }
-        APXB_CK(cudaMemcpy(ap, hp.data(), 4 * hp.size(), cudaMemcpyHostToDevice));
-        bt->a_ptr = ap; bt->a_idx = ai; bt->a_val = av;
-    }
-    // ---- long SpMV rows ----
-    {
-        std::vector<int32_t> hp(bt->n_tot + 1);
-        APXB_CK(cudaMemcpy(hp.data(), bt->a_ptr, 4 * hp.size(), cudaMemcpyDeviceToHost));
-        std::vector<uint32_t> lrow, lfirst, clo, chi;
-        for (uint32_t r = 0; r < bt->n_tot; ++r) {
-            const uint32_t b0 = static_cast<uint32_t>(hp[r]), e0 = static_cast<uint32_t>(hp[r + 1]);
-            if (e0 - b0 <= kLongRow) continue;
-            lrow.push_back(r);
-            lfirst.push_back(static_cast<uint32_t>(clo.size()));
-            for (uint32_t q = b0; q < e0; q += kChunkNnz) { clo.push_back(q); chi.push_back(std::min(e0, q + kChunkNnz)); }
-        }
-        if (!lrow.empty()) {
-            lfirst.push_back(static_cast<uint32_t>(clo.size()));
-            bt->n_long = static_cast<uint32_t>(lrow.size());
-            bt->n_sp_chunks = static_cast<uint32_t>(clo.size());
-            if ((rc = bt->dalloc(&bt->lr_row, lrow.size())) || (rc = bt->dalloc(&bt->lr_first, lfirst.size())) ||
-                (rc = bt->dalloc(&bt->ch_lo, clo.size())) || (rc = bt->dalloc(&bt->ch_hi, chi.size())) ||
-                (rc = bt->dalloc(&bt->ch_part, static_cast<size_t>(clo.size()) * k)))
-                return rc;
-            APXB_CK(cudaMemcpy(bt->lr_row, lrow.data(), 4 * lrow.size(), cudaMemcpyHostToDevice));
-            APXB_CK(cudaMemcpy(bt->lr_first, lfirst.data(), 4 * lfirst.size(), cudaMemcpyHostToDevice));
-            APXB_CK(cudaMemcpy(bt->ch_lo, clo.data(), 4 * clo.size(), cudaMemcpyHostToDevice));
-            APXB_CK(cudaMemcpy(bt->ch_hi, chi.data(), 4 * chi.size(), cudaMemcpyHostToDevice));
-        }
-    }
-    // ---- permutation (permuted position -> original global index), tiles ----
-    {
-        std::vector<uint32_t> gp(bt->n_tot), io(bt->n_tot);
-        std::vector<uint32_t> ti, tl, th, t0(n_inst), t1(n_inst);
-        for (int i = 0; i < n_inst; ++i) {
-            const auto& perm = fs[i]->h.perm;
-            for (uint32_t v = 0; v < bt->n[i]; ++v) { gp[bt->off[i] + v] = bt->off[i] + perm[v]; io[bt->off[i] + v] = i; }
-            t0[i] = static_cast<uint32_t>(ti.size());
-            for (uint32_t lo = 0; lo < bt->n[i]; lo += kTile) {
-                ti.push_back(static_cast<uint32_t>(i));
-                tl.push_back(bt->off[i] + lo);
-                th.push_back(bt->off[i] + std::min(bt->n[i], lo + kTile));
+        if (nnz_a >= 0x7fffffffull) return fail(APXB_ERR_INVALID, "combined operator exceeds the int32 range");
+        cudaStream_t s = e->stream;
+        const size_t nk = static_cast<size_t>(bt->n_tot) * k, ns = bt->slots();
+        int rc;
+        // ---- sweep plans (batch plans for this k; the two directions on two threads) ----
+        {
+            const uint32_t col_lanes = k >= 8 ? static_cast<uint32_t>(k / 4) : 1u;
+            apxb::sweep_plan plans[2];
+            std::string bad[2];
+            {
+                apxb::run_threads(2, [&](unsigned dir) {
+                    batch_plan(fs, bt->off, static_cast<int>(dir), col_lanes, plans[dir]);
+                    if (n_inst == 1)
+                        bad[dir] = apxb::check_batch_plan(fs[0]->h.m, dir == 0 ? fs[0]->h.fwd_level : fs[0]->h.bck_level,
+                                                          plans[dir], col_lanes);
+                });
             }
-            t1[i] = static_cast<uint32_t>(ti.size());
+            for (int dir = 0; dir < 2; ++dir) {
+                const apxb::sweep_plan& pl = plans[dir];
+                if (!bad[dir].empty()) return fail(APXB_ERR_INVALID, "internal batch plan error: " + bad[dir]);
+                uint32_t *info, *ord, *ptr, *idx, *chunk;
+                float* val;
+                if ((rc = bt->dalloc(&info, pl.info.size())) || (rc = bt->dalloc(&ord, pl.ord.size())) ||
+                    (rc = bt->dalloc(&ptr, pl.ptr.size())) || (rc = bt->dalloc(&idx, pl.idx.size())) ||
+                    (rc = bt->dalloc(&val, pl.val.size())) || (rc = bt->dalloc(&chunk, pl.chunk.size())))
+                    return rc;
+                APXB_CK(cudaMemcpyAsync(info, pl.info.data(), 4 * pl.info.size(), cudaMemcpyHostToDevice, s));
+                APXB_CK(cudaMemcpyAsync(ord, pl.ord.data(), 4 * pl.ord.size(), cudaMemcpyHostToDevice, s));
+                APXB_CK(cudaMemcpyAsync(ptr, pl.ptr.data(), 4 * pl.ptr.size(), cudaMemcpyHostToDevice, s));
+                APXB_CK(cudaMemcpyAsync(idx, pl.idx.data(), 4 * pl.idx.size(), cudaMemcpyHostToDevice, s));
+                APXB_CK(cudaMemcpyAsync(val, pl.val.data(), 4 * pl.val.size(), cudaMemcpyHostToDevice, s));
+                APXB_CK(cudaMemcpyAsync(chunk, pl.chunk.data(), 4 * pl.chunk.size(), cudaMemcpyHostToDevice, s));
+                APXB_CK(cudaStreamSynchronize(s));
+                bt->n_items[dir] = pl.n_items;
+                bt->info[dir] = info; bt->ord[dir] = ord; bt->ptr[dir] = ptr; bt->idx[dir] = idx; bt->val[dir] = val;
+                bt->chunk[dir] = chunk; bt->n_chunks[dir] = static_cast<uint32_t>(pl.chunk.size() - 1);
+            }
         }
-        bt->n_tiles = static_cast<uint32_t>(ti.size());
-        if ((rc = bt->dalloc(&bt->gperm, bt->n_tot)) || (rc = bt->dalloc(&bt->inst_of, bt->n_tot)) ||
-            (rc = bt->dalloc(&bt->tile_inst, ti.size())) ||
-            (rc = bt->dalloc(&bt->tile_lo, ti.size())) || (rc = bt->dalloc(&bt->tile_hi, ti.size())) ||
-            (rc = bt->dalloc(&bt->inst_t0, n_inst)) || (rc = bt->dalloc(&bt->inst_t1, n_inst)) ||
-            (rc = bt->dalloc(&bt->inst_off, n_inst)) || (rc = bt->dalloc(&bt->inst_n, n_inst)) ||
-            (rc = bt->dalloc(&bt->inst_lap, n_inst)) || (rc = bt->dalloc(&bt->nrhs, n_inst)))
+        if ((rc = bt->dalloc(&bt->ctl, 2))) return rc;
+        APXB_CK(cudaMemsetAsync(bt->ctl, 0, sizeof(apxb::sweep_ctl) * 2, s));
+        bt->grid32 = e->sweep_grid > 0 ? e->sweep_grid : apxb::sweep_grid32_batch(k, e->num_sms);
+        // ---- operator ----
+        if (n_inst == 1) {
+            bt->a_ptr = ops[0]->ptr; bt->a_idx = ops[0]->idx; bt->a_val = ops[0]->val;
+        } else {
+            int32_t *ap, *ai;
+            double* av;
+            if ((rc = bt->dalloc(&ap, bt->n_tot + 1)) || (rc = bt->dalloc(&ai, nnz_a)) || (rc = bt->dalloc(&av, nnz_a)))
+                return rc;
+            std::vector<int32_t> hp(bt->n_tot + 1, 0);
+            uint64_t base = 0;
+            for (int i = 0; i < n_inst; ++i) {
+                const apxb_operator* a = ops[i];
+                std::vector<int32_t> p(a->n + 1), ix(a->nnz);
+                APXB_CK(cudaMemcpy(p.data(), a->ptr, 4 * (static_cast<size_t>(a->n) + 1), cudaMemcpyDeviceToHost));
+                APXB_CK(cudaMemcpy(ix.data(), a->idx, 4 * a->nnz, cudaMemcpyDeviceToHost));
+                for (uint32_t r = 0; r <= a->n; ++r) hp[bt->off[i] + r] = static_cast<int32_t>(base + p[r]);
+                for (auto& c : ix) c += static_cast<int32_t>(bt->off[i]);
+                APXB_CK(cudaMemcpy(ai + base, ix.data(), 4 * a->nnz, cudaMemcpyHostToDevice));
+                APXB_CK(cudaMemcpy(av + base, a->val, 8 * a->nnz, cudaMemcpyDeviceToDevice));
+                base += a->nnz;
+            }
+            APXB_CK(cudaMemcpy(ap, hp.data(), 4 * hp.size(), cudaMemcpyHostToDevice));
+            bt->a_ptr = ap; bt->a_idx = ai; bt->a_val = av;
+        }
+        // ---- long SpMV rows ----
+        {
+            std::vector<int32_t> hp(bt->n_tot + 1);
+            APXB_CK(cudaMemcpy(hp.data(), bt->a_ptr, 4 * hp.size(), cudaMemcpyDeviceToHost));
+            std::vector<uint32_t> lrow, lfirst, clo, chi;
+            for (uint32_t r = 0; r < bt->n_tot; ++r) {
+                const uint32_t b0 = static_cast<uint32_t>(hp[r]), e0 = static_cast<uint32_t>(hp[r + 1]);
+                if (e0 - b0 <= kLongRow) continue;
+                lrow.push_back(r);
+                lfirst.push_back(static_cast<uint32_t>(clo.size()));
+                for (uint32_t q = b0; q < e0; q += kChunkNnz) { clo.push_back(q); chi.push_back(std::min(e0, q + kChunkNnz)); }
+            }
+            if (!lrow.empty()) {
+                lfirst.push_back(static_cast<uint32_t>(clo.size()));
+                bt->n_long = static_cast<uint32_t>(lrow.size());
+                bt->n_sp_chunks = static_cast<uint32_t>(clo.size());
+                if ((rc = bt->dalloc(&bt->lr_row, lrow.size())) || (rc = bt->dalloc(&bt->lr_first, lfirst.size())) ||
+                    (rc = bt->dalloc(&bt->ch_lo, clo.size())) || (rc = bt->dalloc(&bt->ch_hi, chi.size())) ||
+                    (rc = bt->dalloc(&bt->ch_part, static_cast<size_t>(clo.size()) * k)))
+                    return rc;
+                APXB_CK(cudaMemcpy(bt->lr_row, lrow.data(), 4 * lrow.size(), cudaMemcpyHostToDevice));
+                APXB_CK(cudaMemcpy(bt->lr_first, lfirst.data(), 4 * lfirst.size(), cudaMemcpyHostToDevice));
+                APXB_CK(cudaMemcpy(bt->ch_lo, clo.data(), 4 * clo.size(), cudaMemcpyHostToDevice));
+                APXB_CK(cudaMemcpy(bt->ch_hi, chi.data(), 4 * chi.size(), cudaMemcpyHostToDevice));
+            }
+        }
+        // ---- permutation (permuted position -> original global index), tiles ----
+        {
+            std::vector<uint32_t> gp(bt->n_tot), io(bt->n_tot);
+            std::vector<uint32_t> ti, tl, th, t0(n_inst), t1(n_inst);
+            for (int i = 0; i < n_inst; ++i) {
+                const auto& perm = fs[i]->h.perm;
+                for (uint32_t v = 0; v < bt->n[i]; ++v) { gp[bt->off[i] + v] = bt->off[i] + perm[v]; io[bt->off[i] + v] = i; }
+                t0[i] = static_cast<uint32_t>(ti.size());
+                for (uint32_t lo = 0; lo < bt->n[i]; lo += kTile) {
+                    ti.push_back(static_cast<uint32_t>(i));
+                    tl.push_back(bt->off[i] + lo);
+                    th.push_back(bt->off[i] + std::min(bt->n[i], lo + kTile));
+                }
+                t1[i] = static_cast<uint32_t>(ti.size());
+            }
+            bt->n_tiles = static_cast<uint32_t>(ti.size());
+            if ((rc = bt->dalloc(&bt->gperm, bt->n_tot)) || (rc = bt->dalloc(&bt->inst_of, bt->n_tot)) ||
+                (rc = bt->dalloc(&bt->tile_inst, ti.size())) ||
+                (rc = bt->dalloc(&bt->tile_lo, ti.size())) || (rc = bt->dalloc(&bt->tile_hi, ti.size())) ||
+                (rc = bt->dalloc(&bt->inst_t0, n_inst)) || (rc = bt->dalloc(&bt->inst_t1, n_inst)) ||
+                (rc = bt->dalloc(&bt->inst_off, n_inst)) || (rc = bt->dalloc(&bt->inst_n, n_inst)) ||
+                (rc = bt->dalloc(&bt->inst_lap, n_inst)) || (rc = bt->dalloc(&bt->nrhs, n_inst)))
+                return rc;
+            APXB_CK(cudaMemcpy(bt->gperm, gp.data(), 4 * gp.size(), cudaMemcpyHostToDevice));
+            APXB_CK(cudaMemcpy(bt->inst_of, io.data(), 4 * io.size(), cudaMemcpyHostToDevice));
+            APXB_CK(cudaMemcpy(bt->tile_inst, ti.data(), 4 * ti.size(), cudaMemcpyHostToDevice));
+            APXB_CK(cudaMemcpy(bt->tile_lo, tl.data(), 4 * tl.size(), cudaMemcpyHostToDevice));
+            APXB_CK(cudaMemcpy(bt->tile_hi, th.data(), 4 * th.size(), cudaMemcpyHostToDevice));
+            APXB_CK(cudaMemcpy(bt->inst_t0, t0.data(), 4 * t0.size(), cudaMemcpyHostToDevice));
+            APXB_CK(cudaMemcpy(bt->inst_t1, t1.data(), 4 * t1.size(), cudaMemcpyHostToDevice));
+            APXB_CK(cudaMemcpy(bt->inst_off, bt->off.data(), 4 * bt->off.size(), cudaMemcpyHostToDevice));
+            APXB_CK(cudaMemcpy(bt->inst_n, bt->n.data(), 4 * bt->n.size(), cudaMemcpyHostToDevice));
+            APXB_CK(cudaMemcpy(bt->inst_lap, bt->lap.data(), 4 * bt->lap.size(), cudaMemcpyHostToDevice));
+        }
+        // ---- vectors, state ----
+        if ((rc = bt->dalloc(&bt->x, nk)) || (rc = bt->dalloc(&bt->r, nk)) || (rc = bt->dalloc(&bt->p, nk)) ||
+            (rc = bt->dalloc(&bt->Ap, nk)) || (rc = bt->dalloc(&bt->b, nk)) || (rc = bt->dalloc(&bt->rhs32, nk)) ||
+            (rc = bt->dalloc(&bt->Yf, nk)) || (rc = bt->dalloc(&bt->Zf, nk)) || (rc = bt->dalloc(&bt->sd, kSd * ns)) ||
+            (rc = bt->dalloc(&bt->si, 6 * ns + 3)) || (rc = bt->dalloc(&bt->applies, ns)) ||
+            (rc = bt->dalloc(&bt->partials, static_cast<size_t>(bt->n_tiles) * k * 2)) || (rc = bt->dalloc(&bt->d_B, nk)))
             return rc;
-        APXB_CK(cudaMemcpy(bt->gperm, gp.data(), 4 * gp.size(), cudaMemcpyHostToDevice));
-        APXB_CK(cudaMemcpy(bt->inst_of, io.data(), 4 * io.size(), cudaMemcpyHostToDevice));
-        APXB_CK(cudaMemcpy(bt->tile_inst, ti.data(), 4 * ti.size(), cudaMemcpyHostToDevice));
-        APXB_CK(cudaMemcpy(bt->tile_lo, tl.data(), 4 * tl.size(), cudaMemcpyHostToDevice));
-        APXB_CK(cudaMemcpy(bt->tile_hi, th.data(), 4 * th.size(), cudaMemcpyHostToDevice));
-        APXB_CK(cudaMemcpy(bt->inst_t0, t0.data(), 4 * t0.size(), cudaMemcpyHostToDevice));
-        APXB_CK(cudaMemcpy(bt->inst_t1, t1.data(), 4 * t1.size(), cudaMemcpyHostToDevice));
-        APXB_CK(cudaMemcpy(bt->inst_off, bt->off.data(), 4 * bt->off.size(), cudaMemcpyHostToDevice));
-        APXB_CK(cudaMemcpy(bt->inst_n, bt->n.data(), 4 * bt->n.size(), cudaMemcpyHostToDevice));
-        APXB_CK(cudaMemcpy(bt->inst_lap, bt->lap.data(), 4 * bt->lap.size(), cudaMemcpyHostToDevice));
-    }
-    // ---- vectors, state ----
-    if ((rc = bt->dalloc(&bt->x, nk)) || (rc = bt->dalloc(&bt->r, nk)) || (rc = bt->dalloc(&bt->p, nk)) ||
-        (rc = bt->dalloc(&bt->Ap, nk)) || (rc = bt->dalloc(&bt->b, nk)) || (rc = bt->dalloc(&bt->rhs32, nk)) ||
-        (rc = bt->dalloc(&bt->Yf, nk)) || (rc = bt->dalloc(&bt->Zf, nk)) || (rc = bt->dalloc(&bt->sd, kSd * ns)) ||
-        (rc = bt->dalloc(&bt->si, 6 * ns + 3)) || (rc = bt->dalloc(&bt->applies, ns)) ||
-        (rc = bt->dalloc(&bt->partials, static_cast<size_t>(bt->n_tiles) * k * 2)) || (rc = bt->dalloc(&bt->d_B, nk)))
-        return rc;
-    APXB_CK(cudaMallocHost(&bt->h_sd, sizeof(double) * kSd * ns));
-    APXB_CK(cudaMallocHost(&bt->h_si, sizeof(int) * (6 * ns + 1)));
-    std::fill(bt->h_sd, bt->h_sd + kSd * ns, 0.0);
-    std::fill(bt->h_si, bt->h_si + 6 * ns + 1, 0);
-    std::fill(bt->h_si + ns, bt->h_si + 2 * ns, 1);   // host mirror of the idle state below
-    APXB_CK(cudaMemsetAsync(bt->sd, 0, sizeof(double) * kSd * ns, s));
-    APXB_CK(cudaMemsetAsync(bt->si, 0, sizeof(int) * (6 * ns + 3), s));
-    {   // every slot starts idle: done, and the batch all done
-        std::vector<int> idle(ns + 1, 1);
-        APXB_CK(cudaMemcpyAsync(bt->si + ns, idle.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, s));
-        APXB_CK(cudaMemcpyAsync(bt->si + 6 * ns, idle.data(), sizeof(int), cudaMemcpyHostToDevice, s));
-    }
-    APXB_CK(cudaMemsetAsync(bt->applies, 0, sizeof(unsigned long long) * ns, s));
-    APXB_CK(cudaMemsetAsync(bt->p, 0, sizeof(double) * nk, s));
-    // Zf: markers on factor rows, 0 on each Laplacian instance's grounded row
-    apxb::launch_fill_sent32(bt->Yf, nk, s);
-    apxb::launch_fill_sent32(bt->Zf, nk, s);
-    {
-        std::vector<uint32_t> grounded;
-        for (int i = 0; i < n_inst; ++i)
-            if (bt->lap[i]) grounded.push_back(bt->off[i] + bt->n[i] - 1);
-        if (!grounded.empty()) {
-            uint32_t* gr;
-            if ((rc = bt->dalloc(&gr, grounded.size()))) return rc;
-            APXB_CK(cudaMemcpy(gr, grounded.data(), 4 * grounded.size(), cudaMemcpyHostToDevice));
-            k_b_zero_rows<<<1, 256, 0, s>>>(bt->Zf, gr, static_cast<unsigned>(grounded.size()), k);
+        APXB_CK(cudaMallocHost(&bt->h_sd, sizeof(double) * kSd * ns));
+        APXB_CK(cudaMallocHost(&bt->h_si, sizeof(int) * (6 * ns + 1)));
+        std::fill(bt->h_sd, bt->h_sd + kSd * ns, 0.0);
+        std::fill(bt->h_si, bt->h_si + 6 * ns + 1, 0);
+        std::fill(bt->h_si + ns, bt->h_si + 2 * ns, 1);   // host mirror of the idle state below
+        APXB_CK(cudaMemsetAsync(bt->sd, 0, sizeof(double) * kSd * ns, s));
+        APXB_CK(cudaMemsetAsync(bt->si, 0, sizeof(int) * (6 * ns + 3), s));
+        {   // every slot starts idle: done, and the batch all done
+            std::vector<int> idle(ns + 1, 1);
+            APXB_CK(cudaMemcpyAsync(bt->si + ns, idle.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, s));
+            APXB_CK(cudaMemcpyAsync(bt->si + 6 * ns, idle.data(), sizeof(int), cudaMemcpyHostToDevice, s));
         }
-    }
-    bt->y_armed = true;
-    APXB_CK(cudaGetLastError());
-    APXB_CK(cudaStreamSynchronize(s));
-    e->children++;
-    *out = bt.release();
-    return APXB_OK;
+        APXB_CK(cudaMemsetAsync(bt->applies, 0, sizeof(unsigned long long) * ns, s));
+        APXB_CK(cudaMemsetAsync(bt->p, 0, sizeof(double) * nk, s));
+        // Zf: markers on factor rows, 0 on each Laplacian instance's grounded row
+        apxb::launch_fill_sent32(bt->Yf, nk, s);
+        apxb::launch_fill_sent32(bt->Zf, nk, s);
+        {
+            std::vector<uint32_t> grounded;
+            for (int i = 0; i < n_inst; ++i)
+                if (bt->lap[i]) grounded.push_back(bt->off[i] + bt->n[i] - 1);
+            if (!grounded.empty()) {
+                uint32_t* gr;
+                if ((rc = bt->dalloc(&gr, grounded.size()))) return rc;
+                APXB_CK(cudaMemcpy(gr, grounded.data(), 4 * grounded.size(), cudaMemcpyHostToDevice));
+                k_b_zero_rows<<<1, 256, 0, s>>>(bt->Zf, gr, static_cast<unsigned>(grounded.size()), k);
+            }
+        }
+        bt->y_armed = true;
+        APXB_CK(cudaGetLastError());
+        APXB_CK(cudaStreamSynchronize(s));
+        e->children++;
+        *out = bt.release();
+        return APXB_OK;
+    });
 }
 
 int apxb_batch_destroy(apxb_batch* bt) {
@@ -1385,22 +1383,24 @@ int apxb_batch_solve(apxb_batch* bt, const double* B, double* X, const int* nrhs
 int apxb_batch_plan_host(uint32_t n, const uint32_t* colptr, const uint32_t* rowidx, const float* vals,
                          const uint32_t* perm, int sddm, const uint64_t* rounds, uint32_t n_rounds, double drop_rel,
                          int k, uint32_t* n_items, uint32_t* n_chunks) {
-    if (!colptr || !rowidx || !vals || !perm || !n_items || !n_chunks) return fail(APXB_ERR_INVALID, "NULL argument");
-    if (k != 1 && k != 2 && k != 4 && k != 8 && k != 16) return fail(APXB_ERR_INVALID, "k must be 1, 2, 4, 8 or 16");
-    apxb_factor f;
-    const std::string why = apxb::prepare_factor(n, colptr, rowidx, vals, perm, sddm != 0, rounds, n_rounds,
-                                                 drop_rel < 0.0 ? apxb::kDropRelDefault : drop_rel, f.h);
-    if (!why.empty()) return fail(APXB_ERR_BAD_FACTOR, why);
-    const uint32_t col_lanes = k >= 8 ? static_cast<uint32_t>(k / 4) : 1u;
-    for (int dir = 0; dir < 2; ++dir) {
-        apxb::sweep_plan pl;
-        batch_plan({&f}, {0u}, dir, col_lanes, pl);
-        const std::string bad = apxb::check_batch_plan(f.h.m, dir == 0 ? f.h.fwd_level : f.h.bck_level, pl, col_lanes);
-        if (!bad.empty()) return fail(APXB_ERR_INVALID, "batch plan: " + bad);
-        n_items[dir] = pl.n_items;
-        n_chunks[dir] = static_cast<uint32_t>(pl.chunk.size() - 1);
-    }
-    return APXB_OK;
+    return guarded([&]() -> int {
+        if (!colptr || !rowidx || !vals || !perm || !n_items || !n_chunks) return fail(APXB_ERR_INVALID, "NULL argument");
+        if (k != 1 && k != 2 && k != 4 && k != 8 && k != 16) return fail(APXB_ERR_INVALID, "k must be 1, 2, 4, 8 or 16");
+        apxb_factor f;
+        const std::string why = apxb::prepare_factor(n, colptr, rowidx, vals, perm, sddm != 0, rounds, n_rounds,
+                                                     drop_rel < 0.0 ? apxb::kDropRelDefault : drop_rel, f.h);
+        if (!why.empty()) return fail(APXB_ERR_BAD_FACTOR, why);
+        const uint32_t col_lanes = k >= 8 ? static_cast<uint32_t>(k / 4) : 1u;
+        for (int dir = 0; dir < 2; ++dir) {
+            apxb::sweep_plan pl;
+            batch_plan({&f}, {0u}, dir, col_lanes, pl);
+            const std::string bad = apxb::check_batch_plan(f.h.m, dir == 0 ? f.h.fwd_level : f.h.bck_level, pl, col_lanes);
+            if (!bad.empty()) return fail(APXB_ERR_INVALID, "batch plan: " + bad);
+            n_items[dir] = pl.n_items;
+            n_chunks[dir] = static_cast<uint32_t>(pl.chunk.size() - 1);
+        }
+        return APXB_OK;
+    });
 }
 
 int apxb_batch_set_refresh(apxb_batch* bt, int every) {

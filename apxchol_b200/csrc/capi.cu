@@ -152,26 +152,28 @@ int apxb_prepare_host(uint32_t n, const uint32_t* colptr, const uint32_t* rowidx
                       uint32_t* csr_ptr, uint32_t* csr_idx, float* csr_val,
                       uint32_t* csc_ptr, uint32_t* csc_idx, float* csc_val,
                       uint8_t* fwd_thin, uint8_t* bck_thin) {
-    if (!colptr || !rowidx || !vals || !perm || !m || !nnz_stored) return fail(APXB_ERR_INVALID, "NULL argument");
-    if (n_rounds && !rounds) return fail(APXB_ERR_INVALID, "rounds is NULL");
-    apxb::prepared_factor h;
-    const std::string why = apxb::prepare_factor(n, colptr, rowidx, vals, perm, sddm != 0, rounds, n_rounds,
-                                                 drop_rel, h);
-    if (!why.empty()) return fail(APXB_ERR_BAD_FACTOR, why);
-    *m = h.m;
-    *nnz_stored = h.nnz_stored;
-    if (levels) { levels[0] = h.fwd_levels; levels[1] = h.bck_levels; }
-    if (csr_ptr) std::memcpy(csr_ptr, h.csr_ptr.data(), 4 * h.csr_ptr.size());
-    if (csr_idx) std::memcpy(csr_idx, h.csr_idx.data(), 4 * h.csr_idx.size());
-    if (csr_val) std::memcpy(csr_val, h.csr_val.data(), 4 * h.csr_val.size());
-    if (csc_ptr) std::memcpy(csc_ptr, h.csc_ptr.data(), 4 * h.csc_ptr.size());
-    if (csc_idx) std::memcpy(csc_idx, h.csc_idx.data(), 4 * h.csc_idx.size());
-    if (csc_val) std::memcpy(csc_val, h.csc_val.data(), 4 * h.csc_val.size());
-    for (uint32_t r = 0; r < h.m; ++r) {
-        if (fwd_thin) fwd_thin[r] = (h.fwd_thin_bits[r >> 5] >> (r & 31)) & 1u;
-        if (bck_thin) bck_thin[r] = (h.bck_thin_bits[r >> 5] >> (r & 31)) & 1u;
-    }
-    return APXB_OK;
+    return guarded([&]() -> int {
+        if (!colptr || !rowidx || !vals || !perm || !m || !nnz_stored) return fail(APXB_ERR_INVALID, "NULL argument");
+        if (n_rounds && !rounds) return fail(APXB_ERR_INVALID, "rounds is NULL");
+        apxb::prepared_factor h;
+        const std::string why = apxb::prepare_factor(n, colptr, rowidx, vals, perm, sddm != 0, rounds, n_rounds,
+                                                     drop_rel, h);
+        if (!why.empty()) return fail(APXB_ERR_BAD_FACTOR, why);
+        *m = h.m;
+        *nnz_stored = h.nnz_stored;
+        if (levels) { levels[0] = h.fwd_levels; levels[1] = h.bck_levels; }
+        if (csr_ptr) std::memcpy(csr_ptr, h.csr_ptr.data(), 4 * h.csr_ptr.size());
+        if (csr_idx) std::memcpy(csr_idx, h.csr_idx.data(), 4 * h.csr_idx.size());
+        if (csr_val) std::memcpy(csr_val, h.csr_val.data(), 4 * h.csr_val.size());
+        if (csc_ptr) std::memcpy(csc_ptr, h.csc_ptr.data(), 4 * h.csc_ptr.size());
+        if (csc_idx) std::memcpy(csc_idx, h.csc_idx.data(), 4 * h.csc_idx.size());
+        if (csc_val) std::memcpy(csc_val, h.csc_val.data(), 4 * h.csc_val.size());
+        for (uint32_t r = 0; r < h.m; ++r) {
+            if (fwd_thin) fwd_thin[r] = (h.fwd_thin_bits[r >> 5] >> (r & 31)) & 1u;
+            if (bck_thin) bck_thin[r] = (h.bck_thin_bits[r >> 5] >> (r & 31)) & 1u;
+        }
+        return APXB_OK;
+    });
 }
 
 int apxb_prepare_host_fp16(uint32_t n, const uint32_t* colptr, const uint32_t* rowidx, const float* vals,
@@ -180,24 +182,26 @@ int apxb_prepare_host_fp16(uint32_t n, const uint32_t* colptr, const uint32_t* r
                            uint32_t* csc_ptr, uint32_t* csc_idx, uint16_t* csc_val16,
                            uint32_t* csr_ptr, uint32_t* csr_idx, uint16_t* csr_val16,
                            float* diag, float* inv_scale, uint64_t* stats) {
-    if (!colptr || !rowidx || !vals || !perm || !m || !nnz_stored) return fail(APXB_ERR_INVALID, "NULL argument");
-    if (n_rounds && !rounds) return fail(APXB_ERR_INVALID, "rounds is NULL");
-    apxb::prepared_factor h;
-    const std::string why = apxb::prepare_factor(n, colptr, rowidx, vals, perm, sddm != 0, rounds, n_rounds,
-                                                 drop_rel, h, true);
-    if (!why.empty()) return fail(APXB_ERR_BAD_FACTOR, why);
-    *m = h.m;
-    *nnz_stored = h.nnz_stored;
-    if (csc_ptr) std::memcpy(csc_ptr, h.csc_ptr.data(), 4 * h.csc_ptr.size());
-    if (csc_idx) std::memcpy(csc_idx, h.csc_idx.data(), 4 * h.csc_idx.size());
-    if (csc_val16) std::memcpy(csc_val16, h.csc_h.data(), 2 * h.csc_h.size());
-    if (csr_ptr) std::memcpy(csr_ptr, h.csr_ptr.data(), 4 * h.csr_ptr.size());
-    if (csr_idx) std::memcpy(csr_idx, h.csr_idx.data(), 4 * h.csr_idx.size());
-    if (csr_val16) std::memcpy(csr_val16, h.csr_h.data(), 2 * h.csr_h.size());
-    if (diag) std::memcpy(diag, h.diag16.data(), 4 * h.diag16.size());
-    if (inv_scale) std::memcpy(inv_scale, h.inv_scale.data(), 4 * h.inv_scale.size());
-    if (stats) { stats[0] = h.dropped; stats[1] = h.dropped_flush; stats[2] = h.flushed; }
-    return APXB_OK;
+    return guarded([&]() -> int {
+        if (!colptr || !rowidx || !vals || !perm || !m || !nnz_stored) return fail(APXB_ERR_INVALID, "NULL argument");
+        if (n_rounds && !rounds) return fail(APXB_ERR_INVALID, "rounds is NULL");
+        apxb::prepared_factor h;
+        const std::string why = apxb::prepare_factor(n, colptr, rowidx, vals, perm, sddm != 0, rounds, n_rounds,
+                                                     drop_rel, h, true);
+        if (!why.empty()) return fail(APXB_ERR_BAD_FACTOR, why);
+        *m = h.m;
+        *nnz_stored = h.nnz_stored;
+        if (csc_ptr) std::memcpy(csc_ptr, h.csc_ptr.data(), 4 * h.csc_ptr.size());
+        if (csc_idx) std::memcpy(csc_idx, h.csc_idx.data(), 4 * h.csc_idx.size());
+        if (csc_val16) std::memcpy(csc_val16, h.csc_h.data(), 2 * h.csc_h.size());
+        if (csr_ptr) std::memcpy(csr_ptr, h.csr_ptr.data(), 4 * h.csr_ptr.size());
+        if (csr_idx) std::memcpy(csr_idx, h.csr_idx.data(), 4 * h.csr_idx.size());
+        if (csr_val16) std::memcpy(csr_val16, h.csr_h.data(), 2 * h.csr_h.size());
+        if (diag) std::memcpy(diag, h.diag16.data(), 4 * h.diag16.size());
+        if (inv_scale) std::memcpy(inv_scale, h.inv_scale.data(), 4 * h.inv_scale.size());
+        if (stats) { stats[0] = h.dropped; stats[1] = h.dropped_flush; stats[2] = h.flushed; }
+        return APXB_OK;
+    });
 }
 
 // ---------------------------------------------------------------- factor
@@ -205,91 +209,93 @@ int apxb_prepare_host_fp16(uint32_t n, const uint32_t* colptr, const uint32_t* r
 int apxb_factor_create(apxb_engine* e, uint32_t n, const uint32_t* colptr, const uint32_t* rowidx,
                        const float* vals, const uint32_t* perm, int sddm, const uint64_t* rounds,
                        uint32_t n_rounds, double drop_rel, int precision, apxb_factor** out) {
-    if (!e || !out || !colptr || !rowidx || !vals || !perm) return fail(APXB_ERR_INVALID, "NULL argument");
-    if (precision != APXB_PREC_FP64 && precision != APXB_PREC_FP32 && precision != APXB_PREC_FP16)
-        return fail(APXB_ERR_INVALID, "bad precision");
-    if (n_rounds && !rounds) return fail(APXB_ERR_INVALID, "rounds is NULL");
-    *out = nullptr;
-    const bool fp16 = precision == APXB_PREC_FP16;
-    APXB_CK(cudaSetDevice(e->device));
-    std::unique_ptr<apxb_factor> f(new (std::nothrow) apxb_factor);
-    if (!f) return fail(APXB_ERR_INVALID, "host allocation failed");
-    f->e = e;
-    f->precision = precision;
-    const std::string why = apxb::prepare_factor(n, colptr, rowidx, vals, perm, sddm != 0, rounds, n_rounds,
-                                                 drop_rel, f->h, fp16);
-    if (!why.empty()) return fail(APXB_ERR_BAD_FACTOR, why);
-    const auto& h = f->h;
-    const size_t m = h.m, nnz = h.nnz_stored;
-    if (nnz >= 0xffffffffull) return fail(APXB_ERR_BAD_FACTOR, "factor nnz exceeds the 32-bit offset range");
-    // fp16 storage: (1 / s)^2 in fp64 (an fp32 square overflows for s below
-    // ~5e-20), and a column the storage cannot represent fails here, loudly
-    // (cuda.h:339-358)
-    std::vector<double> inv_scale2;
-    if (fp16) {
-        inv_scale2.resize(m);
-        for (size_t j = 0; j < m; ++j) {
-            const double r = static_cast<double>(h.inv_scale[j]);
-            inv_scale2[j] = r * r;
-            if (!(std::isfinite(h.diag16[j]) && h.diag16[j] != 0.0f && std::isfinite(inv_scale2[j])))
-                return fail(APXB_ERR_BAD_FACTOR, "fp16 factor storage cannot represent column " + std::to_string(j) +
-                                                     " (diag " + std::to_string(h.diag16[j]) + ", inv_scale^2 " +
-                                                     std::to_string(inv_scale2[j]) + ")");
+    return guarded([&]() -> int {
+        if (!e || !out || !colptr || !rowidx || !vals || !perm) return fail(APXB_ERR_INVALID, "NULL argument");
+        if (precision != APXB_PREC_FP64 && precision != APXB_PREC_FP32 && precision != APXB_PREC_FP16)
+            return fail(APXB_ERR_INVALID, "bad precision");
+        if (n_rounds && !rounds) return fail(APXB_ERR_INVALID, "rounds is NULL");
+        *out = nullptr;
+        const bool fp16 = precision == APXB_PREC_FP16;
+        APXB_CK(cudaSetDevice(e->device));
+        std::unique_ptr<apxb_factor> f(new (std::nothrow) apxb_factor);
+        if (!f) return fail(APXB_ERR_INVALID, "host allocation failed");
+        f->e = e;
+        f->precision = precision;
+        const std::string why = apxb::prepare_factor(n, colptr, rowidx, vals, perm, sddm != 0, rounds, n_rounds,
+                                                     drop_rel, f->h, fp16);
+        if (!why.empty()) return fail(APXB_ERR_BAD_FACTOR, why);
+        const auto& h = f->h;
+        const size_t m = h.m, nnz = h.nnz_stored;
+        if (nnz >= 0xffffffffull) return fail(APXB_ERR_BAD_FACTOR, "factor nnz exceeds the 32-bit offset range");
+        // fp16 storage: (1 / s)^2 in fp64 (an fp32 square overflows for s below
+        // ~5e-20), and a column the storage cannot represent fails here, loudly
+        // (cuda.h:339-358)
+        std::vector<double> inv_scale2;
+        if (fp16) {
+            inv_scale2.resize(m);
+            for (size_t j = 0; j < m; ++j) {
+                const double r = static_cast<double>(h.inv_scale[j]);
+                inv_scale2[j] = r * r;
+                if (!(std::isfinite(h.diag16[j]) && h.diag16[j] != 0.0f && std::isfinite(inv_scale2[j])))
+                    return fail(APXB_ERR_BAD_FACTOR, "fp16 factor storage cannot represent column " + std::to_string(j) +
+                                                         " (diag " + std::to_string(h.diag16[j]) + ", inv_scale^2 " +
+                                                         std::to_string(inv_scale2[j]) + ")");
+            }
         }
-    }
-    int rc;
-    if ((rc = f->dalloc(&f->perm, n)) || (rc = f->dalloc(&f->ctl, 2))) return rc;
-    cudaStream_t s = e->stream;
-    APXB_CK(cudaMemcpyAsync(f->perm, h.perm.data(), 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s));
-    APXB_CK(cudaMemsetAsync(f->ctl, 0, sizeof(apxb::sweep_ctl) * 2, s));
-    for (int dir = 0; dir < 2; ++dir) {
-        const apxb::sweep_plan& pl = dir == 0 ? h.fwd_plan : h.bck_plan;
-        if ((rc = f->dalloc(&f->info[dir], pl.info.size())) || (rc = f->dalloc(&f->ord[dir], pl.ord.size())) ||
-            (rc = f->dalloc(&f->ptr[dir], pl.ptr.size())) || (rc = f->dalloc(&f->idx[dir], pl.idx.size())) ||
-            (rc = fp16 ? f->dalloc(&f->val16[dir], pl.val16.size()) : f->dalloc(&f->val[dir], pl.val.size())) ||
-            (rc = f->dalloc(&f->chunk[dir], pl.chunk.size())))
-            return rc;
-        f->n_chunks[dir] = static_cast<uint32_t>(pl.chunk.size() - 1);
-        APXB_CK(cudaMemcpyAsync(f->chunk[dir], pl.chunk.data(), 4 * pl.chunk.size(), cudaMemcpyHostToDevice, s));
-        APXB_CK(cudaMemcpyAsync(f->info[dir], pl.info.data(), 4 * pl.info.size(), cudaMemcpyHostToDevice, s));
-        APXB_CK(cudaMemcpyAsync(f->ord[dir], pl.ord.data(), 4 * pl.ord.size(), cudaMemcpyHostToDevice, s));
-        APXB_CK(cudaMemcpyAsync(f->ptr[dir], pl.ptr.data(), 4 * pl.ptr.size(), cudaMemcpyHostToDevice, s));
-        APXB_CK(cudaMemcpyAsync(f->idx[dir], pl.idx.data(), 4 * pl.idx.size(), cudaMemcpyHostToDevice, s));
-        if (fp16)
-            APXB_CK(cudaMemcpyAsync(f->val16[dir], pl.val16.data(), 2 * pl.val16.size(), cudaMemcpyHostToDevice, s));
-        else
-            APXB_CK(cudaMemcpyAsync(f->val[dir], pl.val.data(), 4 * pl.val.size(), cudaMemcpyHostToDevice, s));
-        if (pl.seg_rows) {
-            if ((rc = f->dalloc(&f->seg_row[dir], pl.seg_row.size())) ||
-                (rc = f->dalloc(&f->seg_lvl[dir], pl.seg_lvl.size())) ||
-                (rc = f->dalloc(&f->seg_ptr[dir], pl.seg_ptr.size())) ||
-                (rc = f->dalloc(&f->seg_idx[dir], pl.seg_idx.size())) ||
-                (rc = f->dalloc(&f->seg_val[dir], pl.seg_val.size())))
+        int rc;
+        if ((rc = f->dalloc(&f->perm, n)) || (rc = f->dalloc(&f->ctl, 2))) return rc;
+        cudaStream_t s = e->stream;
+        APXB_CK(cudaMemcpyAsync(f->perm, h.perm.data(), 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s));
+        APXB_CK(cudaMemsetAsync(f->ctl, 0, sizeof(apxb::sweep_ctl) * 2, s));
+        for (int dir = 0; dir < 2; ++dir) {
+            const apxb::sweep_plan& pl = dir == 0 ? h.fwd_plan : h.bck_plan;
+            if ((rc = f->dalloc(&f->info[dir], pl.info.size())) || (rc = f->dalloc(&f->ord[dir], pl.ord.size())) ||
+                (rc = f->dalloc(&f->ptr[dir], pl.ptr.size())) || (rc = f->dalloc(&f->idx[dir], pl.idx.size())) ||
+                (rc = fp16 ? f->dalloc(&f->val16[dir], pl.val16.size()) : f->dalloc(&f->val[dir], pl.val.size())) ||
+                (rc = f->dalloc(&f->chunk[dir], pl.chunk.size())))
                 return rc;
-            APXB_CK(cudaMemcpyAsync(f->seg_row[dir], pl.seg_row.data(), 4 * pl.seg_row.size(), cudaMemcpyHostToDevice, s));
-            APXB_CK(cudaMemcpyAsync(f->seg_lvl[dir], pl.seg_lvl.data(), 4 * pl.seg_lvl.size(), cudaMemcpyHostToDevice, s));
-            APXB_CK(cudaMemcpyAsync(f->seg_ptr[dir], pl.seg_ptr.data(), 4 * pl.seg_ptr.size(), cudaMemcpyHostToDevice, s));
-            APXB_CK(cudaMemcpyAsync(f->seg_idx[dir], pl.seg_idx.data(), 4 * pl.seg_idx.size(), cudaMemcpyHostToDevice, s));
-            APXB_CK(cudaMemcpyAsync(f->seg_val[dir], pl.seg_val.data(), 4 * pl.seg_val.size(), cudaMemcpyHostToDevice, s));
+            f->n_chunks[dir] = static_cast<uint32_t>(pl.chunk.size() - 1);
+            APXB_CK(cudaMemcpyAsync(f->chunk[dir], pl.chunk.data(), 4 * pl.chunk.size(), cudaMemcpyHostToDevice, s));
+            APXB_CK(cudaMemcpyAsync(f->info[dir], pl.info.data(), 4 * pl.info.size(), cudaMemcpyHostToDevice, s));
+            APXB_CK(cudaMemcpyAsync(f->ord[dir], pl.ord.data(), 4 * pl.ord.size(), cudaMemcpyHostToDevice, s));
+            APXB_CK(cudaMemcpyAsync(f->ptr[dir], pl.ptr.data(), 4 * pl.ptr.size(), cudaMemcpyHostToDevice, s));
+            APXB_CK(cudaMemcpyAsync(f->idx[dir], pl.idx.data(), 4 * pl.idx.size(), cudaMemcpyHostToDevice, s));
+            if (fp16)
+                APXB_CK(cudaMemcpyAsync(f->val16[dir], pl.val16.data(), 2 * pl.val16.size(), cudaMemcpyHostToDevice, s));
+            else
+                APXB_CK(cudaMemcpyAsync(f->val[dir], pl.val.data(), 4 * pl.val.size(), cudaMemcpyHostToDevice, s));
+            if (pl.seg_rows) {
+                if ((rc = f->dalloc(&f->seg_row[dir], pl.seg_row.size())) ||
+                    (rc = f->dalloc(&f->seg_lvl[dir], pl.seg_lvl.size())) ||
+                    (rc = f->dalloc(&f->seg_ptr[dir], pl.seg_ptr.size())) ||
+                    (rc = f->dalloc(&f->seg_idx[dir], pl.seg_idx.size())) ||
+                    (rc = f->dalloc(&f->seg_val[dir], pl.seg_val.size())))
+                    return rc;
+                APXB_CK(cudaMemcpyAsync(f->seg_row[dir], pl.seg_row.data(), 4 * pl.seg_row.size(), cudaMemcpyHostToDevice, s));
+                APXB_CK(cudaMemcpyAsync(f->seg_lvl[dir], pl.seg_lvl.data(), 4 * pl.seg_lvl.size(), cudaMemcpyHostToDevice, s));
+                APXB_CK(cudaMemcpyAsync(f->seg_ptr[dir], pl.seg_ptr.data(), 4 * pl.seg_ptr.size(), cudaMemcpyHostToDevice, s));
+                APXB_CK(cudaMemcpyAsync(f->seg_idx[dir], pl.seg_idx.data(), 4 * pl.seg_idx.size(), cudaMemcpyHostToDevice, s));
+                APXB_CK(cudaMemcpyAsync(f->seg_val[dir], pl.seg_val.data(), 4 * pl.seg_val.size(), cudaMemcpyHostToDevice, s));
+            }
         }
-    }
-    if (fp16) {
-        if ((rc = f->dalloc(&f->diag16, m)) || (rc = f->dalloc(&f->inv_scale2, m))) return rc;
-        APXB_CK(cudaMemcpyAsync(f->diag16, h.diag16.data(), 4 * m, cudaMemcpyHostToDevice, s));
-        APXB_CK(cudaMemcpyAsync(f->inv_scale2, inv_scale2.data(), 8 * m, cudaMemcpyHostToDevice, s));
-    }
-    if ((rc = f->dalloc(&f->Y, n)) || (rc = f->dalloc(&f->Z, n)) || (rc = f->dalloc(&f->zp, n))) return rc;
-    // Z[m] (the grounded entry of a Laplacian) is 0 for good; rows < m start armed.
-    APXB_CK(cudaMemsetAsync(f->Z, 0, 8 * static_cast<size_t>(n), s));
-    apxb::launch_fill_sent64(f->Y, m, s);
-    apxb::launch_fill_sent64(f->Z, m, s);
-    f->y_armed = f->z_armed = true;
-    APXB_CK(cudaGetLastError());
-    f->grid64 = apxb::sweep_grid64(e->num_sms);
-    APXB_CK(cudaStreamSynchronize(s));
-    e->children++;
-    *out = f.release();
-    return APXB_OK;
+        if (fp16) {
+            if ((rc = f->dalloc(&f->diag16, m)) || (rc = f->dalloc(&f->inv_scale2, m))) return rc;
+            APXB_CK(cudaMemcpyAsync(f->diag16, h.diag16.data(), 4 * m, cudaMemcpyHostToDevice, s));
+            APXB_CK(cudaMemcpyAsync(f->inv_scale2, inv_scale2.data(), 8 * m, cudaMemcpyHostToDevice, s));
+        }
+        if ((rc = f->dalloc(&f->Y, n)) || (rc = f->dalloc(&f->Z, n)) || (rc = f->dalloc(&f->zp, n))) return rc;
+        // Z[m] (the grounded entry of a Laplacian) is 0 for good; rows < m start armed.
+        APXB_CK(cudaMemsetAsync(f->Z, 0, 8 * static_cast<size_t>(n), s));
+        apxb::launch_fill_sent64(f->Y, m, s);
+        apxb::launch_fill_sent64(f->Z, m, s);
+        f->y_armed = f->z_armed = true;
+        APXB_CK(cudaGetLastError());
+        f->grid64 = apxb::sweep_grid64(e->num_sms);
+        APXB_CK(cudaStreamSynchronize(s));
+        e->children++;
+        *out = f.release();
+        return APXB_OK;
+    });
 }
 
 int apxb_factor_destroy(apxb_factor* f) {
@@ -640,60 +646,62 @@ int apxb_apply(apxb_engine* e, apxb_factor* f, const double* b, double* z, int f
 
 int apxb_operator_create(apxb_engine* e, uint32_t n, const int32_t* colptr, const int32_t* rowidx,
                          const double* vals, const uint32_t* perm, apxb_operator** out) {
-    if (!e || !colptr || !rowidx || !vals || !perm || !out || n == 0) return fail(APXB_ERR_INVALID, "bad argument");
-    *out = nullptr;
-    APXB_CK(cudaSetDevice(e->device));
-    std::unique_ptr<apxb_operator> a(new (std::nothrow) apxb_operator);
-    if (!a) return fail(APXB_ERR_INVALID, "host allocation failed");
-    a->e = e;
-    a->n = n;
-    std::vector<int32_t> ptr, idx;
-    std::vector<double> val;
-    const std::string why = apxb::permute_operator(n, colptr, rowidx, vals, perm, ptr, idx, val);
-    if (!why.empty()) return fail(APXB_ERR_INVALID, why);
-    a->nnz = idx.size();
-    int rc;
-    if ((rc = a->dalloc(&a->ptr, n + 1)) || (rc = a->dalloc(&a->idx, a->nnz)) || (rc = a->dalloc(&a->val, a->nnz)) ||
-        (rc = a->dalloc(&a->perm, n)) || (rc = a->dalloc(&a->x, n)) || (rc = a->dalloc(&a->r, n)) ||
-        (rc = a->dalloc(&a->p, n)) || (rc = a->dalloc(&a->Ap, n)) || (rc = a->dalloc(&a->b_orig, n)) ||
-        (rc = a->dalloc(&a->x_orig, n)) || (rc = a->dalloc(&a->st, 1)))
-        return rc;
-    APXB_CK(cudaMallocHost(&a->h_st, sizeof(apxb::pcg_state)));
-    cudaStream_t s = e->stream;
-    APXB_CK(cudaMemcpyAsync(a->ptr, ptr.data(), 4 * (static_cast<size_t>(n) + 1), cudaMemcpyHostToDevice, s));
-    APXB_CK(cudaMemcpyAsync(a->idx, idx.data(), 4 * a->nnz, cudaMemcpyHostToDevice, s));
-    APXB_CK(cudaMemcpyAsync(a->val, val.data(), 8 * a->nnz, cudaMemcpyHostToDevice, s));
-    APXB_CK(cudaMemcpyAsync(a->perm, perm, 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s));
-    {   // long rows: cut into chunks summed by one block each (power-law hubs)
-        std::vector<uint32_t> lrow, lfirst, clo, chi;
-        for (uint32_t r = 0; r < n; ++r) {
-            const uint32_t b0 = static_cast<uint32_t>(ptr[r]), e0 = static_cast<uint32_t>(ptr[r + 1]);
-            if (e0 - b0 <= apxb::kLongRowPlain) continue;
-            lrow.push_back(r);
-            lfirst.push_back(static_cast<uint32_t>(clo.size()));
-            for (uint32_t q = b0; q < e0; q += apxb::kChunkNnzPlain) {
-                clo.push_back(q);
-                chi.push_back(std::min(e0, q + apxb::kChunkNnzPlain));
+    return guarded([&]() -> int {
+        if (!e || !colptr || !rowidx || !vals || !perm || !out || n == 0) return fail(APXB_ERR_INVALID, "bad argument");
+        *out = nullptr;
+        APXB_CK(cudaSetDevice(e->device));
+        std::unique_ptr<apxb_operator> a(new (std::nothrow) apxb_operator);
+        if (!a) return fail(APXB_ERR_INVALID, "host allocation failed");
+        a->e = e;
+        a->n = n;
+        std::vector<int32_t> ptr, idx;
+        std::vector<double> val;
+        const std::string why = apxb::permute_operator(n, colptr, rowidx, vals, perm, ptr, idx, val);
+        if (!why.empty()) return fail(APXB_ERR_INVALID, why);
+        a->nnz = idx.size();
+        int rc;
+        if ((rc = a->dalloc(&a->ptr, n + 1)) || (rc = a->dalloc(&a->idx, a->nnz)) || (rc = a->dalloc(&a->val, a->nnz)) ||
+            (rc = a->dalloc(&a->perm, n)) || (rc = a->dalloc(&a->x, n)) || (rc = a->dalloc(&a->r, n)) ||
+            (rc = a->dalloc(&a->p, n)) || (rc = a->dalloc(&a->Ap, n)) || (rc = a->dalloc(&a->b_orig, n)) ||
+            (rc = a->dalloc(&a->x_orig, n)) || (rc = a->dalloc(&a->st, 1)))
+            return rc;
+        APXB_CK(cudaMallocHost(&a->h_st, sizeof(apxb::pcg_state)));
+        cudaStream_t s = e->stream;
+        APXB_CK(cudaMemcpyAsync(a->ptr, ptr.data(), 4 * (static_cast<size_t>(n) + 1), cudaMemcpyHostToDevice, s));
+        APXB_CK(cudaMemcpyAsync(a->idx, idx.data(), 4 * a->nnz, cudaMemcpyHostToDevice, s));
+        APXB_CK(cudaMemcpyAsync(a->val, val.data(), 8 * a->nnz, cudaMemcpyHostToDevice, s));
+        APXB_CK(cudaMemcpyAsync(a->perm, perm, 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s));
+        {   // long rows: cut into chunks summed by one block each (power-law hubs)
+            std::vector<uint32_t> lrow, lfirst, clo, chi;
+            for (uint32_t r = 0; r < n; ++r) {
+                const uint32_t b0 = static_cast<uint32_t>(ptr[r]), e0 = static_cast<uint32_t>(ptr[r + 1]);
+                if (e0 - b0 <= apxb::kLongRowPlain) continue;
+                lrow.push_back(r);
+                lfirst.push_back(static_cast<uint32_t>(clo.size()));
+                for (uint32_t q = b0; q < e0; q += apxb::kChunkNnzPlain) {
+                    clo.push_back(q);
+                    chi.push_back(std::min(e0, q + apxb::kChunkNnzPlain));
+                }
+            }
+            if (!lrow.empty()) {
+                lfirst.push_back(static_cast<uint32_t>(clo.size()));
+                a->n_long = static_cast<uint32_t>(lrow.size());
+                a->n_chunks = static_cast<uint32_t>(clo.size());
+                if ((rc = a->dalloc(&a->lr_row, lrow.size())) || (rc = a->dalloc(&a->lr_first, lfirst.size())) ||
+                    (rc = a->dalloc(&a->ch_lo, clo.size())) || (rc = a->dalloc(&a->ch_hi, chi.size())) ||
+                    (rc = a->dalloc(&a->ch_part, clo.size())))
+                    return rc;
+                APXB_CK(cudaMemcpyAsync(a->lr_row, lrow.data(), 4 * lrow.size(), cudaMemcpyHostToDevice, s));
+                APXB_CK(cudaMemcpyAsync(a->lr_first, lfirst.data(), 4 * lfirst.size(), cudaMemcpyHostToDevice, s));
+                APXB_CK(cudaMemcpyAsync(a->ch_lo, clo.data(), 4 * clo.size(), cudaMemcpyHostToDevice, s));
+                APXB_CK(cudaMemcpyAsync(a->ch_hi, chi.data(), 4 * chi.size(), cudaMemcpyHostToDevice, s));
             }
         }
-        if (!lrow.empty()) {
-            lfirst.push_back(static_cast<uint32_t>(clo.size()));
-            a->n_long = static_cast<uint32_t>(lrow.size());
-            a->n_chunks = static_cast<uint32_t>(clo.size());
-            if ((rc = a->dalloc(&a->lr_row, lrow.size())) || (rc = a->dalloc(&a->lr_first, lfirst.size())) ||
-                (rc = a->dalloc(&a->ch_lo, clo.size())) || (rc = a->dalloc(&a->ch_hi, chi.size())) ||
-                (rc = a->dalloc(&a->ch_part, clo.size())))
-                return rc;
-            APXB_CK(cudaMemcpyAsync(a->lr_row, lrow.data(), 4 * lrow.size(), cudaMemcpyHostToDevice, s));
-            APXB_CK(cudaMemcpyAsync(a->lr_first, lfirst.data(), 4 * lfirst.size(), cudaMemcpyHostToDevice, s));
-            APXB_CK(cudaMemcpyAsync(a->ch_lo, clo.data(), 4 * clo.size(), cudaMemcpyHostToDevice, s));
-            APXB_CK(cudaMemcpyAsync(a->ch_hi, chi.data(), 4 * chi.size(), cudaMemcpyHostToDevice, s));
-        }
-    }
-    APXB_CK(cudaStreamSynchronize(s));
-    e->children++;
-    *out = a.release();
-    return APXB_OK;
+        APXB_CK(cudaStreamSynchronize(s));
+        e->children++;
+        *out = a.release();
+        return APXB_OK;
+    });
 }
 
 int apxb_operator_destroy(apxb_operator* a) {

@@ -6,6 +6,7 @@
 #include <cstdlib>
 #include <chrono>
 #include <cstdio>
+#include <exception>
 #include <numeric>
 #include <thread>
 
@@ -36,15 +37,6 @@ unsigned prep_threads(uint64_t work) {
     }
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
     return work < (1u << 20) ? 1u : std::min(8u, hw);
-}
-
-// body(t) for t in [0, T), t = 0 on the calling thread.
-template <class F>
-void run_threads(unsigned T, F&& body) {
-    std::vector<std::thread> th;
-    for (unsigned t = 1; t < T; ++t) th.emplace_back(body, t);
-    body(0u);
-    for (auto& x : th) x.join();
 }
 
 // Column ranges of T threads with about equal entry counts: [jb[t], jb[t+1]).
@@ -666,17 +658,17 @@ std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* r
     // Sweep plans (the kernels' layout), checked before anything is uploaded;
     // the two directions are independent and built on two threads.
     std::string bad[2];
-    {
-        std::thread bck([&] {
+    run_threads(2, [&](unsigned dir) {
+        if (dir == 1) {
             build_plan(m, bl, out.bck_levels, out.bck_thin_bits, cp, ci, cv, false, done, out.bck_plan,
                        fp16 ? &ch : nullptr);
             bad[1] = check_plan(m, bl, out.bck_plan);
-        });
-        build_plan(m, fl, out.fwd_levels, out.fwd_thin_bits, out.csr_ptr, out.csr_idx, out.csr_val, true, done,
-                   out.fwd_plan, fp16 ? &out.csr_h : nullptr);
-        bad[0] = check_plan(m, fl, out.fwd_plan);
-        bck.join();
-    }
+        } else {
+            build_plan(m, fl, out.fwd_levels, out.fwd_thin_bits, out.csr_ptr, out.csr_idx, out.csr_val, true, done,
+                       out.fwd_plan, fp16 ? &out.csr_h : nullptr);
+            bad[0] = check_plan(m, fl, out.fwd_plan);
+        }
+    });
     for (int dir = 0; dir < 2; ++dir)
         if (!bad[dir].empty()) return "internal sweep plan error: " + bad[dir];
     out.fwd_level = std::move(fl);

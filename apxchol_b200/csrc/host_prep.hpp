@@ -18,9 +18,11 @@
 #pragma once
 #include <cstdint>
 #include <cstring>
+#include <exception>
 #include <memory>
 #include <new>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -80,6 +82,36 @@ inline bool fp16_flushes(float x) { return (fp16_bits(x) & 0x7c00u) == 0; }
 inline uint16_t fp16_narrow(float v, float s) {
     const uint16_t h = fp16_bits(v / s);
     return (h & 0x7c00u) == 0 ? static_cast<uint16_t>(h & 0x8000u) : h;
+}
+
+// body(t) for t in [0, T), t = 0 on the calling thread. An exception thrown
+// by any share is rethrown here after every thread has joined; when a thread
+// cannot be started, the shares left run on the calling thread.
+template <class F>
+inline void run_threads(unsigned T, F&& body) {
+    std::vector<std::exception_ptr> err(T);
+    auto guarded = [&](unsigned t) {
+        try {
+            body(t);
+        } catch (...) {
+            err[t] = std::current_exception();
+        }
+    };
+    std::vector<std::thread> th;
+    th.reserve(T);
+    unsigned started = 1;
+    for (; started < T; ++started) {
+        try {
+            th.emplace_back(guarded, started);
+        } catch (...) {
+            break;
+        }
+    }
+    guarded(0u);
+    for (unsigned t = started; t < T; ++t) guarded(t);
+    for (auto& x : th) x.join();
+    for (auto& e : err)
+        if (e) std::rethrow_exception(e);
 }
 
 // std::allocator whose value-less construct leaves the element uninitialized:

@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <exception>
 #include <memory>
 #include <new>
 #include <string>
@@ -16,11 +17,26 @@
 struct apxb_engine;
 namespace apxb_detail {
 int fail(int code, const std::string& msg);
+// Runs an entry point's body and turns a host exception (an allocation that
+// failed, a thread that could not start) into a status, so none crosses the C ABI.
+template <class F>
+int guarded(F&& body) noexcept {
+    try {
+        return body();
+    } catch (const std::bad_alloc&) {
+        return fail(APXB_ERR_INVALID, "host allocation failed");
+    } catch (const std::exception& ex) {
+        return fail(APXB_ERR_INVALID, std::string("host error: ") + ex.what());
+    } catch (...) {
+        return fail(APXB_ERR_INVALID, "host error");
+    }
+}
 int center_k_from_env();
 // A factor, operator or batch on engine e was destroyed.
 void release_child(apxb_engine* e);
 }  // namespace apxb_detail
 using apxb_detail::fail;
+using apxb_detail::guarded;
 
 #define APXB_CK(call)                                                                            \
     do {                                                                                         \

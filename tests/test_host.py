@@ -86,9 +86,9 @@ def test_factorization_is_deterministic_for_fixed_threads():
 
 @pytest.mark.parametrize("name", ["grid3d_24", "rmat_12", "path_200"])
 def test_threaded_preparation_matches_serial(name, monkeypatch):
-    """The threaded CSR transpose (per-thread column ranges scattered at
-    per-row offsets) gives the same arrays as the serial scatter, whatever
-    the thread count, including more threads than columns."""
+    """The threaded host preparation (the L11 drop, the CSR transpose, the
+    plans' fills) gives the same arrays as the serial passes, whatever the
+    thread count, including more threads than columns."""
     A, F = problem(name)
     outs = []
     for t in ("1", "3", "8", "64"):
@@ -131,3 +131,38 @@ def test_factor_file_round_trip(tmp_path):
     np.savez(tmp_path / "bad.npz", format=np.array("something else"))
     with pytest.raises(ValueError):
         load_factor(tmp_path / "bad.npz")
+
+
+_OOM_CHILD = r"""
+import resource, sys
+sys.path.insert(0, sys.argv[1])
+from apxchol_b200 import native
+from tests.problems import problem
+A, F = problem("grid3d_48")
+native.load()
+vm = int([l for l in open("/proc/self/status") if l.startswith("VmSize")][0].split()[1]) * 1024
+lim = vm + int(sys.argv[2]) * 2**20
+resource.setrlimit(resource.RLIMIT_AS, (lim, lim))
+try:
+    native.prepare_host(F)
+    print("ok")
+except Exception as e:
+    print("error:", e)
+"""
+
+
+@pytest.mark.parametrize("extra_mb", [4, 16])
+def test_host_allocation_failure_is_a_status(extra_mb):
+    """A host allocation that fails inside the threaded preparation (the
+    address space capped just above the process's current use, 8 threads
+    forced) comes back as an error status with its message; the process
+    survives. A thread that cannot start leaves its share to the caller."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, APXB_PREP_THREADS="8")
+    r = subprocess.run([sys.executable, "-c", _OOM_CHILD, root, str(extra_mb)], capture_output=True, text=True,
+                       env=env, cwd=root, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "host allocation failed" in r.stdout, (r.stdout, r.stderr[-2000:])
