@@ -224,23 +224,23 @@ class SolveServer:
         eng = native.Engine(self.device)
         eng.set_memory_budget(max(1, budget))   # the engine refuses what would overrun the budget
         eng.set_sweep_grid(grid)
-        f = op = None
+        f = op = bt = None
         try:
             f = native.DeviceFactor(eng, fac, precision=native.PREC_FP32)
             op = native.DeviceOperator(eng, mat, fac.perm)
             bt = native.Batch(eng, [f], [op], self.k)
             if self.refresh_every is not None:
                 bt.set_refresh(self.refresh_every)
-        except native.ApxbError as ex:
-            for o in (op, f, eng):
+            bbuf = [torch.empty(mat.n, dtype=torch.float64).pin_memory().numpy() for _ in range(self.k)]
+            xbuf = [torch.empty(mat.n, dtype=torch.float64).pin_memory().numpy() for _ in range(self.k)]
+        except Exception as ex:
+            for o in (bt, op, f, eng):
                 if o is not None:
                     o.close()
-            if ex.code == native.ERR_BUDGET:
+            if isinstance(ex, native.ApxbError) and ex.code == native.ERR_BUDGET:
                 raise BudgetError(str(ex)) from ex
             raise
         eng.set_sweep_grid(0)
-        bbuf = [torch.empty(mat.n, dtype=torch.float64).pin_memory().numpy() for _ in range(self.k)]
-        xbuf = [torch.empty(mat.n, dtype=torch.float64).pin_memory().numpy() for _ in range(self.k)]
         return _Lane(eng=eng, factor=f, op=op, batch=bt, bbuf=bbuf, xbuf=xbuf, slots=[None] * self.k,
                      first_step=[0] * self.k, staging=[None] * self.k)
 
