@@ -1295,87 +1295,89 @@ int apxb_batch_size(const apxb_batch* bt, int* n_inst, int* k, uint32_t* n_total
 
 int apxb_batch_solve(apxb_batch* bt, const double* B, double* X, const int* nrhs, double tol, int max_iter,
                      int flags, apxb_pcg_result* res) {
-    if (!bt || !B || !X || !res) return fail(APXB_ERR_INVALID, "bad argument");
-    if (!(tol >= 0.0) || max_iter < 0) return fail(APXB_ERR_INVALID, "bad tol / max_iter");
-    for (char busy : bt->slot_busy)
-        if (busy) return fail(APXB_ERR_BUSY, "slots are admitted for continuous batching");
-    apxb_engine* e = bt->e;
-    APXB_CK(cudaSetDevice(e->device));
-    cudaStream_t s = e->stream;
-    const size_t nk = static_cast<size_t>(bt->n_tot) * bt->K, ns = bt->slots();
-    const bool dev = flags & APXB_DEVICE_PTRS;
-    std::vector<int> nr(bt->S, bt->K);
-    if (nrhs)
-        for (int i = 0; i < bt->S; ++i) {
-            if (nrhs[i] < 0 || nrhs[i] > bt->K) return fail(APXB_ERR_INVALID, "nrhs out of range");
-            nr[i] = nrhs[i];
-        }
-    APXB_CK(cudaMemcpyAsync(bt->nrhs, nr.data(), sizeof(int) * nr.size(), cudaMemcpyHostToDevice, s));
-    const double* dB = B;
-    if (!dev) {
-        APXB_CK(cudaMemcpyAsync(bt->d_B, B, 8 * nk, cudaMemcpyHostToDevice, s));
-        dB = bt->d_B;
-    }
-    {
-        const int rc = ensure_graphs(bt, max_iter);
-        if (rc) return rc;
-    }
-    const bp P = bt->params(max_iter);
-    // every slot fresh with the call's tolerance, nothing done
-    std::vector<int> ones(ns, 1);
-    std::vector<double> tols(ns, tol);
-    APXB_CK(cudaMemcpyAsync(P.tol, tols.data(), sizeof(double) * ns, cudaMemcpyHostToDevice, s));
-    APXB_CK(cudaMemsetAsync(P.done, 0, sizeof(int) * ns, s));
-    APXB_CK(cudaMemcpyAsync(P.fresh, ones.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, s));
-    APXB_CK(cudaMemsetAsync(P.all_done, 0, sizeof(int), s));
-    APXB_CK(cudaMemsetAsync(P.refresh_due, 0, sizeof(int), s));
-    // Only the forward output needs its markers now: the forward sweep re-arms
-    // every factor row of Zf itself, and Zf's grounded rows must stay 0.
-    if (!bt->y_armed) apxb::launch_fill_sent32(bt->Yf, nk, s);
-    bt->y_armed = true;
-    APXB_CK(cudaEventRecord(e->ev0, s));
-    launch_admit(bt, P, dB, s);
-    if (no_graph()) {
-        for (int it = 0; it <= max_iter + 1; it += 4) {
-            for (int j = 0; j < 4; ++j) {
-                const int rc = launch_iteration(bt, P, s, 0, 0);
-                if (rc) return rc;
+    return guarded([&]() -> int {
+        if (!bt || !B || !X || !res) return fail(APXB_ERR_INVALID, "bad argument");
+        if (!(tol >= 0.0) || max_iter < 0) return fail(APXB_ERR_INVALID, "bad tol / max_iter");
+        for (char busy : bt->slot_busy)
+            if (busy) return fail(APXB_ERR_BUSY, "slots are admitted for continuous batching");
+        apxb_engine* e = bt->e;
+        APXB_CK(cudaSetDevice(e->device));
+        cudaStream_t s = e->stream;
+        const size_t nk = static_cast<size_t>(bt->n_tot) * bt->K, ns = bt->slots();
+        const bool dev = flags & APXB_DEVICE_PTRS;
+        std::vector<int> nr(bt->S, bt->K);
+        if (nrhs)
+            for (int i = 0; i < bt->S; ++i) {
+                if (nrhs[i] < 0 || nrhs[i] > bt->K) return fail(APXB_ERR_INVALID, "nrhs out of range");
+                nr[i] = nrhs[i];
             }
-            int ad = 0;
-            APXB_CK(cudaMemcpyAsync(&ad, P.all_done, sizeof(int), cudaMemcpyDeviceToHost, s));
-            APXB_CK(cudaStreamSynchronize(s));
-            if (ad) break;
+        APXB_CK(cudaMemcpyAsync(bt->nrhs, nr.data(), sizeof(int) * nr.size(), cudaMemcpyHostToDevice, s));
+        const double* dB = B;
+        if (!dev) {
+            APXB_CK(cudaMemcpyAsync(bt->d_B, B, 8 * nk, cudaMemcpyHostToDevice, s));
+            dB = bt->d_B;
         }
-    } else if (bt->loop_cond) {
-        APXB_CK(cudaGraphLaunch(bt->loop, s));
-    } else {
-        for (int it = 0; it <= max_iter + 1; it += 4) {
-            for (int j = 0; j < 4; ++j) APXB_CK(cudaGraphLaunch(bt->one, s));
-            int ad = 0;
-            APXB_CK(cudaMemcpyAsync(&ad, P.all_done, sizeof(int), cudaMemcpyDeviceToHost, s));
-            APXB_CK(cudaStreamSynchronize(s));
-            if (ad) break;
+        {
+            const int rc = ensure_graphs(bt, max_iter);
+            if (rc) return rc;
         }
-    }
-    double* dX = dev ? X : bt->d_B;
-    launch_finish(bt, P, dX, (flags & APXB_TRUE_RESIDUAL) != 0, s);
-    APXB_CK(cudaEventRecord(e->ev1, s));
-    APXB_CK(cudaGetLastError());
-    if (!dev) APXB_CK(cudaMemcpyAsync(X, bt->d_B, 8 * nk, cudaMemcpyDeviceToHost, s));
-    APXB_CK(cudaMemcpyAsync(bt->h_sd, bt->sd, sizeof(double) * kSd * ns, cudaMemcpyDeviceToHost, s));
-    APXB_CK(cudaMemcpyAsync(bt->h_si, bt->si, sizeof(int) * 6 * ns, cudaMemcpyDeviceToHost, s));
-    const int rc = e->take_error();
-    if (rc) { bt->y_armed = false; cudaMemsetAsync(bt->ctl, 0, 2 * sizeof(apxb::sweep_ctl), s); return rc; }
-    float ms = 0.0f;
-    cudaEventElapsedTime(&ms, e->ev0, e->ev1);
-    for (size_t sl = 0; sl < ns; ++sl) {
-        res[sl].iterations = bt->h_si[sl];
-        res[sl].status = bt->h_si[2 * ns + sl];
-        res[sl].residual = bt->h_sd[7 * ns + sl];
-        res[sl].true_residual = (flags & APXB_TRUE_RESIDUAL) ? bt->h_sd[12 * ns + sl] : -1.0;
-        res[sl].seconds = ms * 1e-3;
-    }
-    return APXB_OK;
+        const bp P = bt->params(max_iter);
+        // every slot fresh with the call's tolerance, nothing done
+        std::vector<int> ones(ns, 1);
+        std::vector<double> tols(ns, tol);
+        APXB_CK(cudaMemcpyAsync(P.tol, tols.data(), sizeof(double) * ns, cudaMemcpyHostToDevice, s));
+        APXB_CK(cudaMemsetAsync(P.done, 0, sizeof(int) * ns, s));
+        APXB_CK(cudaMemcpyAsync(P.fresh, ones.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, s));
+        APXB_CK(cudaMemsetAsync(P.all_done, 0, sizeof(int), s));
+        APXB_CK(cudaMemsetAsync(P.refresh_due, 0, sizeof(int), s));
+        // Only the forward output needs its markers now: the forward sweep re-arms
+        // every factor row of Zf itself, and Zf's grounded rows must stay 0.
+        if (!bt->y_armed) apxb::launch_fill_sent32(bt->Yf, nk, s);
+        bt->y_armed = true;
+        APXB_CK(cudaEventRecord(e->ev0, s));
+        launch_admit(bt, P, dB, s);
+        if (no_graph()) {
+            for (int it = 0; it <= max_iter + 1; it += 4) {
+                for (int j = 0; j < 4; ++j) {
+                    const int rc = launch_iteration(bt, P, s, 0, 0);
+                    if (rc) return rc;
+                }
+                int ad = 0;
+                APXB_CK(cudaMemcpyAsync(&ad, P.all_done, sizeof(int), cudaMemcpyDeviceToHost, s));
+                APXB_CK(cudaStreamSynchronize(s));
+                if (ad) break;
+            }
+        } else if (bt->loop_cond) {
+            APXB_CK(cudaGraphLaunch(bt->loop, s));
+        } else {
+            for (int it = 0; it <= max_iter + 1; it += 4) {
+                for (int j = 0; j < 4; ++j) APXB_CK(cudaGraphLaunch(bt->one, s));
+                int ad = 0;
+                APXB_CK(cudaMemcpyAsync(&ad, P.all_done, sizeof(int), cudaMemcpyDeviceToHost, s));
+                APXB_CK(cudaStreamSynchronize(s));
+                if (ad) break;
+            }
+        }
+        double* dX = dev ? X : bt->d_B;
+        launch_finish(bt, P, dX, (flags & APXB_TRUE_RESIDUAL) != 0, s);
+        APXB_CK(cudaEventRecord(e->ev1, s));
+        APXB_CK(cudaGetLastError());
+        if (!dev) APXB_CK(cudaMemcpyAsync(X, bt->d_B, 8 * nk, cudaMemcpyDeviceToHost, s));
+        APXB_CK(cudaMemcpyAsync(bt->h_sd, bt->sd, sizeof(double) * kSd * ns, cudaMemcpyDeviceToHost, s));
+        APXB_CK(cudaMemcpyAsync(bt->h_si, bt->si, sizeof(int) * 6 * ns, cudaMemcpyDeviceToHost, s));
+        const int rc = e->take_error();
+        if (rc) { bt->y_armed = false; cudaMemsetAsync(bt->ctl, 0, 2 * sizeof(apxb::sweep_ctl), s); return rc; }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e->ev0, e->ev1);
+        for (size_t sl = 0; sl < ns; ++sl) {
+            res[sl].iterations = bt->h_si[sl];
+            res[sl].status = bt->h_si[2 * ns + sl];
+            res[sl].residual = bt->h_sd[7 * ns + sl];
+            res[sl].true_residual = (flags & APXB_TRUE_RESIDUAL) ? bt->h_sd[12 * ns + sl] : -1.0;
+            res[sl].seconds = ms * 1e-3;
+        }
+        return APXB_OK;
+    });
 }
 
 // Host-only: the batch plans of one factor for k right-hand sides, built and
