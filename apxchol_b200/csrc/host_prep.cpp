@@ -64,8 +64,8 @@ uint32_t seg_level_rows_setting() {
 
 // Appends row r's entries re-laid (off-diagonals in the reference order, the
 // diagonal last) to (oi, ov).
-void relay_row(uint32_t r, bool forward, const std::vector<uint32_t>& ptr, const std::vector<uint32_t>& idx,
-               const std::vector<float>& val, std::vector<uint32_t>& oi, std::vector<float>& ov) {
+void relay_row(uint32_t r, bool forward, const std::vector<uint32_t>& ptr, const plan_vec<uint32_t>& idx,
+               const plan_vec<float>& val, std::vector<uint32_t>& oi, std::vector<float>& ov) {
     const uint32_t b = ptr[r], en = ptr[r + 1];
     const uint32_t d = forward ? en - 1 : b;
     for (uint32_t p = b; p < en; ++p) {
@@ -94,8 +94,8 @@ void group_rows(uint32_t m, const std::vector<int32_t>& level, int32_t n_levels,
 // val16 (fp16 storage, nullable): binary16 values beside val, re-laid the
 // same way into plan.val16; such plans have no serial segment.
 void build_plan(uint32_t m, const std::vector<int32_t>& level, int32_t n_levels, const std::vector<uint32_t>& bits,
-                const std::vector<uint32_t>& ptr, const std::vector<uint32_t>& idx, const std::vector<float>& val,
-                bool forward, bool contiguous, sweep_plan& plan, const std::vector<uint16_t>* val16 = nullptr) {
+                const std::vector<uint32_t>& ptr, const plan_vec<uint32_t>& idx, const plan_vec<float>& val,
+                bool forward, bool contiguous, sweep_plan& plan, const plan_vec<uint16_t>* val16 = nullptr) {
     if (val16) contiguous = false;
     plan = sweep_plan{};
     // Serial segment: the trailing run (forward order) of small levels.
@@ -290,8 +290,8 @@ void build_batch_plan(const prepared_factor& h, int dir, uint32_t col_lanes, swe
     const std::vector<int32_t>& level = forward ? h.fwd_level : h.bck_level;
     const int32_t n_levels = forward ? h.fwd_levels : h.bck_levels;
     const std::vector<uint32_t>& ptr = forward ? h.csr_ptr : h.csc_ptr;
-    const std::vector<uint32_t>& idx = forward ? h.csr_idx : h.csc_idx;
-    const std::vector<float>& val = forward ? h.csr_val : h.csc_val;
+    const plan_vec<uint32_t>& idx = forward ? h.csr_idx : h.csc_idx;
+    const plan_vec<float>& val = forward ? h.csr_val : h.csc_val;
     auto width = [&](uint32_t r) {
         const uint32_t len = ptr[r + 1] - ptr[r] - 1;
         uint32_t ge = 1;
@@ -441,9 +441,9 @@ std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* r
     // what each keeps, a prefix sum places them, pass 2 writes them -- on T
     // threads over column ranges (factor_drop.h:131-211 has the same shape).
     std::vector<uint32_t>& cp = out.csc_ptr;
-    std::vector<uint32_t>& ci = out.csc_idx;
-    std::vector<float>& cv = out.csc_val;
-    std::vector<uint16_t>& ch = out.csc_h;
+    plan_vec<uint32_t>& ci = out.csc_idx;     // uninitialized on resize: pass 2 writes every entry
+    plan_vec<float>& cv = out.csc_val;
+    plan_vec<uint16_t>& ch = out.csc_h;
     cp.assign(static_cast<size_t>(m) + 1, 0);
     // a Laplacian's L11 leaves out row n-1: the column's last row when present
     auto col_end = [&](uint32_t j) {

@@ -186,11 +186,13 @@ struct prepared_factor {
     uint64_t nnz_stored = 0;     // after the drop
     uint64_t dropped = 0;
     // forward: CSR(L11), diagonal last in each row
-    std::vector<uint32_t> csr_ptr, csr_idx;
-    std::vector<float> csr_val;
+    std::vector<uint32_t> csr_ptr;
+    plan_vec<uint32_t> csr_idx;
+    plan_vec<float> csr_val;
     // backward: CSC(L11), diagonal first in each column
-    std::vector<uint32_t> csc_ptr, csc_idx;
-    std::vector<float> csc_val;
+    std::vector<uint32_t> csc_ptr;
+    plan_vec<uint32_t> csc_idx;
+    plan_vec<float> csc_val;
     // per-row 4-way-sum flag, bit-packed (bit r&31 of word r>>5)
     std::vector<uint32_t> fwd_thin_bits, bck_thin_bits;
     int32_t fwd_levels = 0, bck_levels = 0;
@@ -206,7 +208,7 @@ struct prepared_factor {
     bool fp16 = false;
     uint64_t dropped_flush = 0;                // off-diagonals dropped only because fp16 flushes them
     uint64_t flushed = 0;                      // stored off-diagonals v != 0 whose binary16 is zero
-    std::vector<uint16_t> csr_h, csc_h;        // binary16 values, same layout as csr_val / csc_val
+    plan_vec<uint16_t> csr_h, csc_h;           // binary16 values, same layout as csr_val / csc_val
     std::vector<float> diag16;                 // per row j: fp32(L_jj) / s_j + rounding residual
     std::vector<float> inv_scale;              // per row j: fp32(1 / s_j)
 };
