@@ -22,14 +22,17 @@ from . import native
 
 class Lane:
     def __init__(self, mat, fac, k: int, grid: int, device: int):
+        self.batch = self.op = self.factor = None
         self.eng = native.Engine(device)
         self.eng.set_sweep_grid(grid)
         try:
             self.factor = native.DeviceFactor(self.eng, fac, precision=native.PREC_FP32)
             self.op = native.DeviceOperator(self.eng, mat, fac.perm)
             self.batch = native.Batch(self.eng, [self.factor], [self.op], k)
-        finally:
-            self.eng.set_sweep_grid(0)
+        except Exception:
+            self.close()          # what was made so far, the engine included
+            raise
+        self.eng.set_sweep_grid(0)
 
     def close(self):
         for o in ("batch", "op", "factor", "eng"):
@@ -114,17 +117,7 @@ class Lanes:
     def sweep_timed(self, reps: int = 10):
         """Every lane's forward and backward sweeps timed (CUDA events on its own
         stream) while all lanes run them concurrently: [(fwd s, bck s)] per lane."""
-        out = [None] * len(self.lanes)
-
-        def run(i):
-            out[i] = self.lanes[i].batch.sweep_timed(reps)
-
-        threads = [threading.Thread(target=run, args=(i,)) for i in range(len(self.lanes))]
-        for t in threads:
-            t.start()
-        for t in threads:
-            t.join()
-        return out
+        return self.each(lambda i, ln: ln.batch.sweep_timed(reps))
 
     def memory_used(self) -> int:
         return sum(ln.eng.memory_used() for ln in self.lanes)
