@@ -79,11 +79,20 @@ def build_problem(grid_n: int):
     return A, F
 
 
+L2_BYTES = 126 * 2**20   # B200 L2
+
+
 def workload_config(grid_n, A, F, form: str, extra=None):
+    # bytes an iteration streams: both factor directions (4 B index + 4 B value) and the operator
+    # (4 B index + 8 B value)
+    it_bytes = 2 * int(F.nnz) * 8 + int(A.nnz) * 12
+    l2 = (f"inputs larger than L2 (factor + operator {it_bytes / 1e6:.0f} MB per iteration), no flush"
+          if it_bytes > L2_BYTES else
+          f"inputs fit in L2 ({it_bytes / 1e6:.1f} MB per iteration): a small test size, not a bench workload")
     cfg = {"workload": f"grid3d_{grid_n} 7-point, weights 10^U[-3,3] (seed 1), boundary +1 (SDDM); {form}",
            "n": int(A.n), "nnz_A": int(A.nnz), "nnz_factor": int(F.nnz), "tol": TOL, "max_iter": MAX_ITER,
            "factor": f"apxchol factorize seed {FACTOR_SEED}, {FACTOR_THREADS} threads, block_greedy/vec_pool",
-           "l2": "inputs larger than L2 (factor + operator > 400 MB per iteration), no flush"}
+           "l2": l2}
     if extra:
         cfg.update(extra)
     return cfg

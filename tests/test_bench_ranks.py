@@ -48,3 +48,28 @@ def test_rank_reductions_gloo():
 def test_single_rank_identity():
     assert bench.max_over_ranks([3, 4.5], 1, "cpu") == [3.0, 4.5]
     assert bench.from_rank0([16, 0], 1, "cpu") == [16.0, 0.0]
+
+
+def test_reference_arm_json_contract():
+    """`bench.py --impl reference` (the reference's own cpu_solver on the host
+    cores) prints one JSON line with the contract's keys, on a small grid."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    import oracle
+    if not oracle.ref_available():
+        pytest.skip("reference library not built")
+    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--grid", "16", "--steps", "1",
+                        "--warmup", "3"], capture_output=True, text=True, cwd=root, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+                "scaling", "vs_baseline", "dtype", "data", "config", "impl", "cpu_baseline", "e2e"):
+        assert key in d, key
+    assert d["impl"] == "reference" and d["unit"] == "solves/s" and d["value"] > 0
+    assert d["steps"] == 1 and d["warmup"] == 3 and d["n_gpus"] == 1
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    assert "fit in L2" in d["config"]["l2"]
