@@ -654,8 +654,9 @@ int apxb_operator_create(apxb_engine* e, uint32_t n, const int32_t* colptr, cons
         if (!a) return fail(APXB_ERR_INVALID, "host allocation failed");
         a->e = e;
         a->n = n;
-        std::vector<int32_t> ptr, idx;
-        std::vector<double> val;
+        std::vector<int32_t> ptr;
+        apxb::plan_vec<int32_t> idx;
+        apxb::plan_vec<double> val;
         const std::string why = apxb::permute_operator(n, colptr, rowidx, vals, perm, ptr, idx, val);
         if (!why.empty()) return fail(APXB_ERR_INVALID, why);
         a->nnz = idx.size();

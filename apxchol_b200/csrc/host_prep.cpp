@@ -688,8 +688,8 @@ std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* r
 }
 
 std::string permute_operator(uint32_t n, const int32_t* colptr, const int32_t* rowidx, const double* vals,
-                             const uint32_t* perm, std::vector<int32_t>& ptr, std::vector<int32_t>& idx,
-                             std::vector<double>& val) {
+                             const uint32_t* perm, std::vector<int32_t>& ptr, plan_vec<int32_t>& idx,
+                             plan_vec<double>& val) {
     if (colptr[0] != 0) return "operator colptr[0] != 0";
     const int64_t nnz = colptr[n];
     if (nnz < 0 || nnz > INT32_MAX) return "operator nnz out of the int32 range";
@@ -708,7 +708,7 @@ std::string permute_operator(uint32_t n, const int32_t* colptr, const int32_t* r
         ptr[perm[j] + 1] = colptr[j + 1] - colptr[j];
     }
     for (uint32_t i = 0; i < n; ++i) ptr[i + 1] += ptr[i];
-    idx.resize(nnz);
+    idx.resize(nnz);     // uninitialized: every entry is written below
     val.resize(nnz);
     // Rows are independent: T threads over column ranges of equal entry counts.
     const unsigned T = prep_threads(static_cast<uint64_t>(nnz));

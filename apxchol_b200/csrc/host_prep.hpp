@@ -252,7 +252,7 @@ std::string prepare_factor(uint32_t n, const uint32_t* colptr, const uint32_t* r
 // Full symmetric CSR of P A P^T (rows sorted) from A's full symmetric CSC and
 // perm (what cuda_pcg::setup builds, include/apxchol/solver/pcg_cuda.h:304-404).
 std::string permute_operator(uint32_t n, const int32_t* colptr, const int32_t* rowidx, const double* vals,
-                             const uint32_t* perm, std::vector<int32_t>& ptr, std::vector<int32_t>& idx,
-                             std::vector<double>& val);
+                             const uint32_t* perm, std::vector<int32_t>& ptr, plan_vec<int32_t>& idx,
+                             plan_vec<double>& val);
 
 }  // namespace apxb
