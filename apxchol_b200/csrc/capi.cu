@@ -565,6 +565,7 @@ int apxb_sweep_pair(apxb_engine* e, apxb_factor* f, const double* d_in, double* 
 
 int apxb_sweep_pair_multi(apxb_engine* e, apxb_factor* f, int k, const double* d_in, double* d_out) {
     if (!e || !f || !d_in || !d_out) return fail(APXB_ERR_INVALID, "bad argument");
+    if (f->e != e) return fail(APXB_ERR_INVALID, "factor belongs to another engine");
     if (k != 1 && k != 2 && k != 4 && k != 8 && k != 16) return fail(APXB_ERR_INVALID, "k must be 1, 2, 4, 8 or 16");
     APXB_CK(cudaSetDevice(e->device));
     const int rc = pair_fp32(f, k, d_in, d_out);
@@ -574,6 +575,7 @@ int apxb_sweep_pair_multi(apxb_engine* e, apxb_factor* f, int k, const double* d
 
 int apxb_sweep_pair_host(apxb_engine* e, apxb_factor* f, const double* in, double* out) {
     if (!e || !f || !in || !out) return fail(APXB_ERR_INVALID, "bad argument");
+    if (f->e != e) return fail(APXB_ERR_INVALID, "factor belongs to another engine");
     APXB_CK(cudaSetDevice(e->device));
     const size_t m = f->h.m;
     int rc = e->ensure_stage(f->h.n);
@@ -965,6 +967,7 @@ extern "C" int apxb_test_stalled_sweep(apxb_engine* e, apxb_factor* f, uint64_t 
 extern "C" int apxb_sweep_pair_timed(apxb_engine* e, apxb_factor* f, const double* d_in, double* d_out, int reps,
                                      double* seconds) {
     if (!e || !f || !d_in || !d_out || reps < 1 || !seconds) return fail(APXB_ERR_INVALID, "bad argument");
+    if (f->e != e) return fail(APXB_ERR_INVALID, "factor belongs to another engine");
     APXB_CK(cudaSetDevice(e->device));
     APXB_CK(cudaEventRecord(e->ev0, e->stream));
     for (int i = 0; i < reps; ++i) {

@@ -180,7 +180,9 @@ int apxb_sweep_pair_host(apxb_engine* e, apxb_factor* f, const double* in, doubl
 /* reps back-to-back pairs on the engine stream, timed with CUDA events; *seconds = per pair. */
 int apxb_sweep_pair_timed(apxb_engine* e, apxb_factor* f, const double* d_in, double* d_out, int reps,
                           double* seconds);
-/* k right-hand sides at once, row-interleaved in[i*k + s] (device pointers). */
+/* k right-hand sides at once, row-interleaved in[i*k + s] (device pointers).
+ * The sweeps are fp32 (fp16-stored factors: over their binary16 values)
+ * whatever the factor's precision; k in {1, 2, 4, 8, 16}. */
 int apxb_sweep_pair_multi(apxb_engine* e, apxb_factor* f, int k, const double* d_in, double* d_out);
 
 /* ---- preconditioner application in the original ordering (apply_core) ----
