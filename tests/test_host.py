@@ -1,6 +1,8 @@
 """Host logic of the product, no GPU: the C ABI loads and exports every
 symbol of include/apxb200.h, and its factor preparation (drop, transpose,
 levels, sum modes) is byte-identical to the reference's SpTRSV setup."""
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -166,3 +168,35 @@ def test_host_allocation_failure_is_a_status(extra_mb):
                        env=env, cwd=root, timeout=300)
     assert r.returncode == 0, r.stderr[-2000:]
     assert "host allocation failed" in r.stdout, (r.stdout, r.stderr[-2000:])
+
+
+def test_abi_rejects_bad_arguments_without_a_gpu():
+    """Every entry point given NULL handles or out-of-range arguments returns
+    APXB_ERR_INVALID with a message, before touching the device (the
+    reference throws std::runtime_error for the same misuse, cuda.h:36-39)."""
+    lib = native.load()
+    info = native.FactorInfo()
+    calls = {
+        "apxb_factor_info_get": (None, ctypes.byref(info)),
+        "apxb_sweep": (None, None, 0, None, None),
+        "apxb_sweep_pair": (None, None, None, None),
+        "apxb_sweep_pair_multi": (None, None, 4, None, None),
+        "apxb_sweep_pair_host": (None, None, None, None),
+        "apxb_apply": (None, None, None, None, 0, None),
+        "apxb_pcg": (None, None, None, None, None, 1e-8, 10, 0, 0, None),
+        "apxb_batch_admit": (None, 0, None, 1e-8, 10, 0),
+        "apxb_batch_step": (None, 1, None),
+        "apxb_batch_retire": (None, 0, None, 0),
+        "apxb_batch_set_refresh": (None, 25),
+    }
+    for name, args in calls.items():
+        rc = getattr(lib, name)(*args)
+        assert rc == native.ERR_INVALID, (name, rc)
+        assert lib.apxb_last_error(), name
+    A, F = problem("path_200")
+    items, chunks = np.zeros(2, np.uint32), np.zeros(2, np.uint32)
+    cp_, ri = np.ascontiguousarray(F.colptr, np.uint32), np.ascontiguousarray(F.rowidx, np.uint32)
+    va, pe = np.ascontiguousarray(F.vals, np.float32), np.ascontiguousarray(F.perm, np.uint32)
+    rc = lib.apxb_batch_plan_host(F.n, native.ptr(cp_), native.ptr(ri), native.ptr(va), native.ptr(pe), int(F.sddm),
+                                  None, 0, -1.0, 3, native.ptr(items), native.ptr(chunks))
+    assert rc == native.ERR_INVALID and b"k must be" in lib.apxb_last_error()
