@@ -3,12 +3,15 @@
 and the SpTRSV sweeps' HBM GB/s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--k K] [--grid G] [--no-serving] [--no-plain] [--no-cpu-baseline]
+                    [--workload grid3d_128|rmat_22|instances_256|serving_8]
+                    [--k K [--lanes L] [--sweep-grid B]] [--grid G]
+                    [--no-serving] [--no-plain] [--no-cpu-baseline]
 
 Our arm. The headline is the batched mixed-precision form: one step is one
 batched PCG solve of k right-hand sides, with fp32 factor sweeps and fp64
-SpMV, residual, dots and centring. k and the sweep grid are picked by the
-autotuner (apxchol_b200/autotune.py) unless --k is given. Every step solves a
+SpMV, residual, dots and centring. k, the sweep grid and the number of lanes
+are picked by the autotuner (apxchol_b200/autotune.py) unless --k is given.
+Every step solves a
 fresh set of N(0,1) right-hand sides from a pool of distinct sets. The line
 reports:
   * value      solves/s over K device-resident steps: every lane (a batch on
@@ -32,6 +35,12 @@ reports:
                (factor, matrix and every vector pass) over that time.
   * cpu_baseline  the reference's own cpu_solver (oracle/_ref) on the host cores.
 Inputs exceed L2 (factor + operator > 400 MB per iteration), so no flush is needed.
+
+--workload selects the other configurations (one JSON line each): rmat_22 (an
+R-MAT scale-22 Laplacian), instances_256 (256 uneven SDDM instances in one
+batch), serving_8 (8 resident matrices under open-loop Poisson arrivals at 50,
+200 and 800 requests/s, p50/p99 per rate). --grid G swaps the 128^3 grid for
+G^3 (a quick, L2-resident check, not a bench workload).
 
 --impl reference: the reference's CPU solve phase (rank 0 only), each step one
 solve of the same system; prints the same JSON line with "impl": "reference".
