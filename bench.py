@@ -40,7 +40,7 @@ Inputs exceed L2 (factor + operator > 400 MB per iteration), so no flush is need
 R-MAT scale-22 Laplacian), instances_256 (256 uneven SDDM instances in one
 batch), serving_8 (8 resident matrices under open-loop Poisson arrivals at 50,
 200 and 800 requests/s, p50/p99 per rate). --grid G swaps the 128^3 grid for
-G^3 (a quick, L2-resident check, not a bench workload).
+G^3, a quicker check; the config's "l2" note says whether its inputs fit in L2.
 
 --impl reference: the reference's CPU solve phase (rank 0 only), each step one
 solve of the same system; prints the same JSON line with "impl": "reference".
