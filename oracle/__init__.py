@@ -216,8 +216,29 @@ def _load_oracle():
         lib.ora_apply_fused.argtypes = [ctypes.POINTER(_System), c_p, ctypes.c_double, c_p]
         lib.ora_apply.argtypes = [ctypes.POINTER(_System), c_p, c_p]
         lib.ora_pcg.argtypes = [ctypes.POINTER(_System), c_p, ctypes.c_double, ctypes.c_int, c_p, c_p, c_p]
+        lib.ora_sweep16.argtypes = [ctypes.c_int, ctypes.c_uint32] + [c_p] * 7
         _ora = lib
     return _ora
+
+
+def sweep16(direction, h, rhs, in_scale=None):
+    """One fp64 sweep over the fp16 storage h (apxchol_b200.native.prepare_host_fp16's
+    arrays): the reference test's host sweep (test_sptrsv_drop.cpp:1100-1127).
+    direction 0: forward over CSR(L11); 1: backward over CSC(L11), the right-hand
+    side times in_scale (fp64) when given."""
+    lib = _load_oracle()
+    m = int(h["m"])
+    key = "csr" if direction == 0 else "csc"
+    ptr = np.ascontiguousarray(h[key + "_ptr"], np.uint32)
+    idx = np.ascontiguousarray(h[key + "_idx"], np.uint32)
+    v16 = np.ascontiguousarray(h[key + "_val16"], np.uint16)
+    diag = np.ascontiguousarray(h["diag"], np.float32)
+    r = np.ascontiguousarray(rhs, np.float64)
+    sc = None if in_scale is None else np.ascontiguousarray(in_scale, np.float64)
+    out = np.empty(m)
+    lib.ora_sweep16(int(direction), m, _ptr(ptr), _ptr(idx), _ptr(v16), _ptr(diag),
+                    _ptr(sc) if sc is not None else None, _ptr(r), _ptr(out))
+    return out
 
 
 THIN_THRESHOLD = 1024   # kSpTRSVOMPThreshold, include/apxchol/solver/sptrsv/omp.h:32

@@ -208,6 +208,27 @@ void ora_sweep(int dir, uint32_t m, const uint32_t* ptr, const uint32_t* idx, co
     }
 }
 
+/* The value of an IEEE binary16 bit pattern (exact in double). */
+static double half_value(uint16_t h) {
+    const int e = (h >> 10) & 0x1f, mant = h & 0x3ff;
+    const double sgn = (h & 0x8000u) ? -1.0 : 1.0;
+    if (e == 0) return sgn * ldexp((double)mant, -24);
+    if (e == 31) return mant ? NAN : sgn * INFINITY;
+    return sgn * ldexp((double)(mant | 0x400), e - 25);
+}
+
+void ora_sweep16(int dir, uint32_t m, const uint32_t* ptr, const uint32_t* idx, const uint16_t* val16,
+                 const float* diag, const double* in_scale, const double* rhs, double* out) {
+    for (uint32_t k = 0; k < m; ++k) {
+        const uint32_t i = dir == 0 ? k : m - 1 - k;
+        double sum = 0.0;
+        for (uint32_t p = ptr[i]; p < ptr[i + 1]; ++p)
+            if (idx[p] != i) sum += half_value(val16[p]) * out[idx[p]];
+        const double r = rhs[i] * (in_scale ? in_scale[i] : 1.0);
+        out[i] = (r - sum) / (double)diag[i];
+    }
+}
+
 /* ---------------------------------------------------------------- reductions */
 
 #define FUSED_OMP_MIN 2000  /* preconditioner.h:55 */

@@ -48,6 +48,14 @@ void ora_thin_flags(uint32_t m, const int32_t* level, int32_t n_levels, uint32_t
 void ora_sweep(int dir, uint32_t m, const uint32_t* ptr, const uint32_t* idx, const float* val,
                const uint8_t* thin, const double* in, double* out);
 
+/* One sweep over an fp16-stored factor, in fp64: the reference test's
+ * independent host sweep (tests/test_sptrsv_drop.cpp:1100-1127) over the
+ * storage of cuda_host.h:16-34. Rows in order (dir 0, CSR(L11)) or in reverse
+ * (dir 1, CSC(L11)); out[i] = (rhs[i] * (in_scale ? in_scale[i] : 1)
+ * - sum_{j != i} value(val16[p]) * out[j]) / diag[i], the sum in storage order. */
+void ora_sweep16(int dir, uint32_t m, const uint32_t* ptr, const uint32_t* idx, const uint16_t* val16,
+                 const float* diag, const double* in_scale, const double* rhs, double* out);
+
 typedef struct ora_system {
     /* operator: full symmetric CSR (== CSC for a symmetric matrix), int32 */
     uint32_t n;

@@ -4,7 +4,8 @@ right-hand side times (1/s)^2 in fp64.
 
 The gates are the reference's own (tests/test_sptrsv_drop.cpp:1198-1206):
 - each sweep against a serial fp64 host sweep over the same fp16 arrays
-  (host_reference_sweep, :1100-1127): max |diff| / max |ref| < 1e-6;
+  (oracle.sweep16, after host_reference_sweep :1100-1127):
+  max |diff| / max |ref| < 1e-6;
 - the pair against the CPU backend's fp64 pair of the fp32-stored factor:
   < 1e-3 (fp16 rounds every off-diagonal to 11 bits, so the pair is a
   slightly different preconditioner);
@@ -51,21 +52,6 @@ def _rel(a, b):
     return float(np.max(np.abs(a - b)) / max(float(np.max(np.abs(b))), 1e-300))
 
 
-def _host_sweep(m, reverse, ptr, idx, val16, diag, in_scale, rhs32):
-    """One row at a time in sweep order, accumulating in fp64 (the
-    reference test's independent host sweep)."""
-    w = val16.view(np.float16).astype(np.float64)
-    out = np.zeros(m)
-    for i in (range(m - 1, -1, -1) if reverse else range(m)):
-        lo, hi = int(ptr[i]), int(ptr[i + 1])
-        cols = idx[lo:hi].astype(np.int64)
-        off = cols != i
-        s = float(np.dot(w[lo:hi][off], out[cols[off]]))
-        r = float(rhs32[i]) * (float(in_scale[i]) if in_scale is not None else 1.0)
-        out[i] = (r - s) / float(diag[i])
-    return out.astype(np.float32)
-
-
 @pytest.mark.parametrize("name,rel", [("grid3d_24", -1.0), ("grid3d_24", 0.0), ("grid2d_64", -1.0),
                                       ("rmat_12", -1.0), ("path_200", -1.0)])
 def test_fp16_sweeps_match_the_host_sweep(eng, name, rel):
@@ -76,11 +62,12 @@ def test_fp16_sweeps_match_the_host_sweep(eng, name, rel):
     m = h["m"]
     x = np.random.default_rng(11).standard_normal(m)
     y = _run(eng, lambda a, b: D.sweep(0, a, b), x)
-    y_ref = _host_sweep(m, False, h["csr_ptr"], h["csr_idx"], h["csr_val16"], h["diag"], None, x.astype(np.float32))
+    # the kernels narrow their fp64 input to fp32 first: the host sweep gets the same input
+    y_ref = oracle.sweep16(0, h, x.astype(np.float32)).astype(np.float32)
     assert _rel(y, y_ref) < SWEEP_TOL
     is2 = h["inv_scale"].astype(np.float64) ** 2
     z = _run(eng, lambda a, b: D.sweep(1, a, b), y)
-    z_ref = _host_sweep(m, True, h["csc_ptr"], h["csc_idx"], h["csc_val16"], h["diag"], is2, y.astype(np.float32))
+    z_ref = oracle.sweep16(1, h, y.astype(np.float32), is2).astype(np.float32)
     assert _rel(z, z_ref) < SWEEP_TOL
 
 
