@@ -83,3 +83,19 @@ def test_dropin_matches_the_c_abi(dropin, tmp_path, name):
         Op.close(); D.close()
     finally:
         eng.close()
+
+
+@pytest.mark.parametrize("env,want", [(None, "-1 0 0"), ("1", "1 1 2"), ("0", "0 0 0"), ("yes", "-1 0 0")])
+def test_dropin_fp16_switch(tmp_path, env, want):
+    """APXCHOL_SPTRSV_FP16=1 selects the fp16 storage (APXB_PREC_FP16 = 2),
+    =0 or anything else keeps the default, the bit-exact fp64 sweeps (0)."""
+    exe = str(tmp_path / "fp16_env")
+    subprocess.run([_cxx(), "-std=c++17", "-O1", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "fp16_env.cpp"), "-L", LIBDIR, "-lapxb200",
+                    f"-Wl,-rpath,{LIBDIR}", "-o", exe], check=True)
+    e = dict(os.environ)
+    e.pop("APXCHOL_SPTRSV_FP16", None)
+    if env is not None:
+        e["APXCHOL_SPTRSV_FP16"] = env
+    r = subprocess.run([exe], capture_output=True, text=True, env=e, check=True)
+    assert r.stdout.strip() == want
