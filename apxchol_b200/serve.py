@@ -409,6 +409,86 @@ class SolveServer:
             self.pool = None
 
 
+class MultiServer:
+    """Requests routed by matrix id to one SolveServer per GPU (replicas, no
+    collective): each registered matrix has one home device, which holds its
+    factors, operator and batches; its requests go there. A matrix is placed
+    on the device given at registration, else on the one with the fewest
+    estimated bytes registered so far. The reference has one GPU path and no
+    serving layer; this is the placement its solve phase allows (a triangular
+    solve does not shard, the units -- matrices and their requests -- do)."""
+
+    def __init__(self, devices, **server_kwargs):
+        self.devices = list(devices)
+        if not self.devices:
+            raise ValueError("no devices")
+        self.servers = [SolveServer(device=d, **server_kwargs) for d in self.devices]
+        self.home: dict = {}                 # mid -> index into self.servers
+        self.placed = [0] * len(self.servers)   # estimated bytes registered per device
+
+    def register(self, mid, mat, fac, device=None):
+        if mid in self.home:
+            raise KeyError(f"matrix {mid!r} is already registered")
+        if device is None:
+            i = min(range(len(self.servers)), key=lambda j: (self.placed[j], j))
+        else:
+            i = self.devices.index(device)
+        srv = self.servers[i]
+        srv.register(mid, mat, fac)
+        self.home[mid] = i
+        self.placed[i] += srv.estimate(mid)
+        return self.devices[i]
+
+    def device_of(self, mid):
+        return self.devices[self.home[mid]]
+
+    def submit(self, mid, b, tol: float = 1e-8, arrival: float | None = None) -> Request:
+        if mid not in self.home:
+            raise KeyError(f"unknown matrix {mid!r}")
+        return self.servers[self.home[mid]].submit(mid, b, tol, arrival)
+
+    def pump(self) -> bool:
+        progressed = False
+        for srv in self.servers:
+            progressed |= srv.pump()
+        return progressed
+
+    def idle(self) -> bool:
+        return all(srv.idle() for srv in self.servers)
+
+    def drain(self, timeout: float = 600.0):
+        t0 = time.perf_counter()
+        while not self.idle():
+            if not self.pump():
+                time.sleep(20e-6)
+            if time.perf_counter() - t0 > timeout:
+                raise TimeoutError("servers did not drain")
+
+    def run_open_loop(self, arrivals):
+        """As SolveServer.run_open_loop, each request served on its matrix's device."""
+        start = [len(srv.completed) for srv in self.servers]
+        t0 = time.perf_counter()
+        i = 0
+        while i < len(arrivals) or not self.idle():
+            now = time.perf_counter() - t0
+            while i < len(arrivals) and arrivals[i][0] <= now:
+                dt, mid, b, tol = arrivals[i]
+                self.submit(mid, b, tol, arrival=t0 + dt)
+                i += 1
+            if not self.pump():
+                time.sleep(20e-6)
+        done = [q for srv, s0 in zip(self.servers, start) for q in srv.completed[s0:]]
+        return sorted(done, key=lambda q: q.arrival)
+
+    @property
+    def completed(self):
+        return [q for srv in self.servers for q in srv.completed]
+
+    def close(self):
+        for srv in self.servers:
+            srv.close()
+
+
 def latency_stats(reqs):
     lat = np.array([q.latency for q in reqs]) * 1e3
     if lat.size == 0:

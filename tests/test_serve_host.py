@@ -162,3 +162,42 @@ def test_open_loop_keeps_arrival_times(monkeypatch):
         assert sorted(round(q.arrival - t0, 6) for q in done) == [round(0.001 * j, 6) for j in range(12)]
     finally:
         srv.close()
+
+
+def test_multi_server_routes_by_matrix(monkeypatch):
+    """MultiServer: each matrix gets one home device (the fewest estimated
+    bytes so far, or the one given), its requests are served there and nowhere
+    else, and every result is the request's own."""
+    from apxchol_b200.serve import MultiServer
+
+    def make_lane(self, mat, fac, grid, room):
+        bt = FakeBatch(self.k)
+        return serve._Lane(eng=_Closable(), factor=_Closable(), op=_Closable(), batch=bt,
+                           bbuf=[np.empty(mat.n) for _ in range(self.k)],
+                           xbuf=[np.empty(mat.n) for _ in range(self.k)],
+                           slots=[None] * self.k, first_step=[0] * self.k, staging=[None] * self.k)
+
+    monkeypatch.setattr(SolveServer, "_make_lane", make_lane)
+    ms = MultiServer([0, 1, 2], budget_bytes=10**12, k=2, iters_per_step=1, sweep_grid=0, copy_threads=2)
+    try:
+        sizes = {"a": 50, "b": 70, "c": 60, "d": 40}
+        for mid, n in sizes.items():
+            ms.register(mid, _Mat(n), _Fac(n))
+        assert [ms.device_of(m) for m in "abcd"] == [0, 1, 2, 0]
+        assert ms.register("e", _Mat(10), _Fac(10), device=2) == 2
+        rng = np.random.default_rng(3)
+        reqs = []
+        for j in range(15):
+            mid = "abcde"[j % 5]
+            reqs.append(ms.submit(mid, rng.standard_normal(sizes.get(mid, 10)), 1e-8))
+        ms.drain(timeout=30)
+        for q in reqs:
+            assert q.status == 0 and np.array_equal(q.x, 2.0 * q.b)
+        assert set(ms.servers[0].resident) == {"a", "d"}
+        assert set(ms.servers[1].resident) == {"b"}
+        assert set(ms.servers[2].resident) == {"c", "e"}
+        assert len(ms.completed) == 15 and ms.idle()
+        with pytest.raises(KeyError):
+            ms.submit("zz", np.ones(3), 1e-8)
+    finally:
+        ms.close()
