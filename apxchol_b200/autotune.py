@@ -5,7 +5,8 @@ right-hand sides) for every right-hand-side block width k in {1, 2, 4, 8, 16}
 and every candidate sweep grid (the resident grid and one block per SM), and
 keeps the fastest solves/s. The sweeps' other knobs are fixed by the plan: the
 lanes per row follow the row length (1, 4, 8, 16 or 32), and the in-flight
-depth is the 3-stage item pipeline with 8 entries per lane.
+depth is the 3-stage item pipeline with 8 entries per lane, plus an L2
+prefetch of the next item's dependency rows.
 
 The reference has no autotuner; its GPU path solves one right-hand side at a
 time (cuda_pcg::solve, include/apxchol/solver/pcg_cuda.h:157-261).
