@@ -33,7 +33,7 @@ constexpr int kSd = 14;            // per-slot double arrays (bp::rz .. bp::tol)
 constexpr uint32_t kLongRow = 128;
 constexpr uint32_t kChunkNnz = 512;
 
-enum fin_mode : int { kFinSpmv = 0, kFinXr = 1, kFinZsum = 2, kFinRz = 3, kFinResid = 4 };
+enum fin_mode : int { kFinSpmv = 0, kFinXr = 1, kFinZsum = 2, kFinRz = 3, kFinResid = 4, kFinVerify = 5 };
 
 // Device pointers and settings of a batch.
 struct bp {
@@ -56,6 +56,8 @@ struct bp {
     // per slot [S*K]
     double *rz, *pAp, *alpha, *beta, *rr, *rs, *bnorm, *rnorm, *prev, *mean, *shift, *xmean, *tres, *tol;
     int *iters, *done, *status, *pmode, *center, *fresh;
+    double* xa;                // per slot: the alpha this iteration's x and r updates use (0: no update)
+    int* verify;               // per slot: converged on the recurrence, to be confirmed after a refresh
     unsigned long long* applies;
     int* all_done;
     int* any_center;           // some live slot centres its next preconditioner input
@@ -340,16 +342,20 @@ __global__ void __launch_bounds__(kBT) k_b_spmv_long(bp P, double* Y, int mode) 
 }
 
 // Whether slot sl refreshes its residual at the start of this iteration: every
-// refresh_every of its own completed iterations (so a slot's arithmetic does not
-// depend on the other slots).
+// refresh_every of its own completed iterations, and in the iteration after its
+// recurrence residual first dropped below its tolerance (verify: the stop is
+// then confirmed on a residual recomputed from x), so a slot's arithmetic does
+// not depend on the other slots.
 __device__ __forceinline__ bool refresh_slot(const bp& P, unsigned sl) {
     const int it = P.iters[sl];
-    return P.refresh_every > 0 && !P.done[sl] && !P.fresh[sl] && it > 0 && it % P.refresh_every == 0;
+    return P.refresh_every > 0 && !P.done[sl] && !P.fresh[sl] && it > 0 &&
+           (it % P.refresh_every == 0 || P.verify[sl]);
 }
 
-// Periodic true-residual refresh (fp64): r = b - A x for the due slots, with A x
-// in Ap from the mode-2 SpMV just before. The iteration's x/r update then
-// continues from the recomputed residual.
+// True-residual refresh (fp64): r = b - A x for the due slots, with A x in Ap
+// from the mode-2 SpMV just before, and r.r partials for kFinVerify (which
+// stops the slots whose convergence this refresh confirms). The iteration's
+// x/r update then continues from the recomputed residual.
 template <int K>
 __global__ void __launch_bounds__(kBT) k_b_refresh(bp P) {
     if (!*P.refresh_due) return;
@@ -357,15 +363,22 @@ __global__ void __launch_bounds__(kBT) k_b_refresh(bp P) {
     for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
         const unsigned i = P.tile_inst[t];
         const bool w0 = refresh_slot(P, i * K + c0), w1 = refresh_slot(P, i * K + c1);
-        if (!w0 && !w1) continue;
-        FLAT_PAIRS(t, {
-            if (two) {
-                if (w0) P.r[q] = P.b[q] - P.Ap[q];
-                if (w1) P.r[q + 1] = P.b[q + 1] - P.Ap[q + 1];
-            } else if (w0) {
-                P.r[q] = P.b[q] - P.Ap[q];
-            }
-        })
+        double acc[1][2] = {{0.0, 0.0}};
+        if (w0 || w1) {
+            FLAT_PAIRS(t, {
+                if (w0) {
+                    const double r = P.b[q] - P.Ap[q];
+                    P.r[q] = r;
+                    acc[0][0] = fma(r, r, acc[0][0]);
+                }
+                if (two && w1) {
+                    const double r = P.b[q + 1] - P.Ap[q + 1];
+                    P.r[q + 1] = r;
+                    acc[0][1] = fma(r, r, acc[0][1]);
+                }
+            })
+        }
+        col_store<K, 1>(acc, P.partials + static_cast<size_t>(t) * K * 2);   // every thread of the block
     }
 }
 
@@ -376,9 +389,10 @@ __device__ __forceinline__ bool centres_next(const bp& P, unsigned i, unsigned s
     return P.inst_lap[i] && (ap % static_cast<unsigned long long>(P.center_k)) == 0;
 }
 
-// x += alpha p; r -= alpha Ap (not for fresh or done slots); r.r and sum(r)
-// partials. Slots whose next preconditioner input is not centred get it here,
-// as fp32 r (k_b_prep writes the centred ones).
+// r -= alpha Ap with the iteration's per-slot alpha (xa: 0 for fresh and done
+// slots); r.r and sum(r) partials. x += alpha p is left to k_b_up, which reads p
+// anyway. Slots whose next preconditioner input is not centred get it here, as
+// fp32 r (k_b_prep writes the centred ones).
 template <int K>
 __global__ void __launch_bounds__(kBT) k_b_xr(bp P) {
     if (*P.all_done) return;
@@ -386,19 +400,14 @@ __global__ void __launch_bounds__(kBT) k_b_xr(bp P) {
     for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
         const unsigned i = P.tile_inst[t];
         const unsigned s0 = i * K + c0, s1 = i * K + c1;
-        const double a0 = (P.fresh[s0] || P.done[s0]) ? 0.0 : P.alpha[s0];
-        const double a1 = (P.fresh[s1] || P.done[s1]) ? 0.0 : P.alpha[s1];
+        const double a0 = P.xa[s0], a1 = P.xa[s1];
         const bool w0 = !centres_next(P, i, s0), w1 = !centres_next(P, i, s1);
         double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
         FLAT_PAIRS(t, {
             if (two) {
-                double2 x = *reinterpret_cast<const double2*>(P.x + q);
-                const double2 p = *reinterpret_cast<const double2*>(P.p + q);
                 double2 r = *reinterpret_cast<const double2*>(P.r + q);
                 const double2 ap = *reinterpret_cast<const double2*>(P.Ap + q);
-                x.x = fma(a0, p.x, x.x); x.y = fma(a1, p.y, x.y);
                 r.x = fma(-a0, ap.x, r.x); r.y = fma(-a1, ap.y, r.y);
-                *reinterpret_cast<double2*>(P.x + q) = x;
                 *reinterpret_cast<double2*>(P.r + q) = r;
                 if (w0 && w1) {
                     *reinterpret_cast<float2*>(P.rhs32 + q) = make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
@@ -409,7 +418,6 @@ __global__ void __launch_bounds__(kBT) k_b_xr(bp P) {
                 acc[0][0] = fma(r.x, r.x, acc[0][0]); acc[0][1] = fma(r.y, r.y, acc[0][1]);
                 acc[1][0] += r.x; acc[1][1] += r.y;
             } else {
-                P.x[q] = fma(a0, P.p[q], P.x[q]);
                 const double r = fma(-a0, P.Ap[q], P.r[q]);
                 P.r[q] = r;
                 if (w0) P.rhs32[q] = static_cast<float>(r);
@@ -488,31 +496,49 @@ __global__ void __launch_bounds__(kBT) k_b_rz(bp P) {
     }
 }
 
-// p = (z - shift) + beta p; first application of a slot: p = z - shift. Sets
-// the graph's WHILE condition.
+// x += alpha p (the iteration's step, with the old p; xa from k_b_fin), then
+// p = (z - shift) + beta p for live slots; first application of a slot:
+// p = z - shift. A slot that converged this iteration still takes its x step.
+// Sets the graph's WHILE condition.
 template <int K>
 __global__ void __launch_bounds__(kBT) k_b_up(bp P, unsigned long long handle, int use_cond) {
-    const bool stop = *P.all_done != 0 || P.err->code != 0;
+    const bool fault = P.err->code != 0;
+    const bool live = *P.all_done == 0;
     if (use_cond && blockIdx.x == 0 && threadIdx.x == 0)
-        cudaGraphSetConditional(static_cast<cudaGraphConditionalHandle>(handle), stop ? 0u : 1u);
-    if (stop) return;
+        cudaGraphSetConditional(static_cast<cudaGraphConditionalHandle>(handle), (live && !fault) ? 1u : 0u);
+    if (fault) return;
     const int c0 = K == 1 ? 0 : static_cast<int>((2 * threadIdx.x) % K), c1 = K == 1 ? 0 : c0 + 1;
     for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
         const unsigned i = P.tile_inst[t];
         const unsigned s0 = i * K + c0, s1 = i * K + c1;
+        const double xa0 = P.xa[s0], xa1 = P.xa[s1];
+        const bool l0 = live && !P.done[s0], l1 = live && !P.done[s1];
+        const bool xs = xa0 != 0.0 || xa1 != 0.0;
+        if (!l0 && !l1 && !xs) continue;
         const double h0 = P.shift[s0], h1 = P.shift[s1], b0 = P.beta[s0], b1 = P.beta[s1];
-        const bool cp0 = P.pmode[s0] == 1, cp1 = P.pmode[s1] == 1, l0 = !P.done[s0], l1 = !P.done[s1];
+        const bool cp0 = P.pmode[s0] == 1, cp1 = P.pmode[s1] == 1;
         FLAT_PAIRS(t, {
             if (two) {
-                const float2 z = *reinterpret_cast<const float2*>(P.z + q);
                 double2 p = *reinterpret_cast<const double2*>(P.p + q);
-                const double z0 = static_cast<double>(z.x) - h0, z1 = static_cast<double>(z.y) - h1;
-                if (l0) p.x = cp0 ? z0 : fma(b0, p.x, z0);
-                if (l1) p.y = cp1 ? z1 : fma(b1, p.y, z1);
-                *reinterpret_cast<double2*>(P.p + q) = p;
-            } else if (l0) {
-                const double z0 = static_cast<double>(P.z[q]) - h0;
-                P.p[q] = cp0 ? z0 : fma(b0, P.p[q], z0);
+                if (xs) {
+                    double2 x = *reinterpret_cast<const double2*>(P.x + q);
+                    x.x = fma(xa0, p.x, x.x); x.y = fma(xa1, p.y, x.y);
+                    *reinterpret_cast<double2*>(P.x + q) = x;
+                }
+                if (l0 || l1) {
+                    const float2 z = *reinterpret_cast<const float2*>(P.z + q);
+                    const double z0 = static_cast<double>(z.x) - h0, z1 = static_cast<double>(z.y) - h1;
+                    if (l0) p.x = cp0 ? z0 : fma(b0, p.x, z0);
+                    if (l1) p.y = cp1 ? z1 : fma(b1, p.y, z1);
+                    *reinterpret_cast<double2*>(P.p + q) = p;
+                }
+            } else {
+                const double pq = P.p[q];
+                if (xa0 != 0.0) P.x[q] = fma(xa0, pq, P.x[q]);
+                if (l0) {
+                    const double z0 = static_cast<double>(P.z[q]) - h0;
+                    P.p[q] = cp0 ? z0 : fma(b0, pq, z0);
+                }
             }
         })
     }
@@ -542,6 +568,7 @@ __device__ __forceinline__ void slot_sums(const bp& P, unsigned sl, int nv, doub
 constexpr int kFinThreads = 1024;   // one warp per slot, up to 32 slots at a time
 
 __global__ void __launch_bounds__(kFinThreads) k_b_fin(bp P, int mode) {
+    if (mode == kFinVerify && !*P.refresh_due) return;   // no refresh this iteration (uniform over the block)
     __shared__ int any_live, any_cen;
     if (threadIdx.x == 0) { any_live = 0; any_cen = 0; }
     __syncthreads();
@@ -580,6 +607,7 @@ __global__ void __launch_bounds__(kFinThreads) k_b_fin(bp P, int mode) {
                         P.prev[sl] = 1.0;
                         P.pmode[sl] = 1;
                         P.applies[sl] = 0;
+                        P.verify[sl] = 0;
                         if (P.bnorm[sl] == 0.0) { P.done[sl] = 1; P.status[sl] = 0; P.rnorm[sl] = 0.0; fin = true; }
                         else { P.rnorm[sl] = 1.0; P.status[sl] = 1; P.done[sl] = 0; }
                     } else {
@@ -587,7 +615,13 @@ __global__ void __launch_bounds__(kFinThreads) k_b_fin(bp P, int mode) {
                         P.rnorm[sl] = rn;
                         const int it = ++P.iters[sl];
                         int status = 1;
-                        if (rn < P.tol[sl]) { fin = true; status = 0; }
+                        if (rn < P.tol[sl]) {
+                            // below tol on the recurrence: the next iteration recomputes b - A x from this x
+                            // and kFinVerify stops the slot if that is below tol. With refreshes off, or at
+                            // the iteration limit, the recurrence decides (apxb_pcg's rule).
+                            if (P.refresh_every == 0 || it >= P.max_iter) { fin = true; status = 0; }
+                            else P.verify[sl] = 1;
+                        }
                         else if (!isfinite(rn)) { fin = true; status = 4; }
                         else if (P.stag > 0 && it % P.stag == 0) {
                             if (rn > P.prev[sl] * 0.5) { fin = true; status = 2; }
@@ -611,6 +645,15 @@ __global__ void __launch_bounds__(kFinThreads) k_b_fin(bp P, int mode) {
                 case kFinZsum:
                     P.shift[sl] = P.center[sl] ? s0 / ni : 0.0;
                     break;
+                case kFinVerify:
+                    // the refreshed residual of a slot whose recurrence fell below tol: its x stands
+                    // when ||b - A x|| / ||b|| < tol (the rest of the iteration leaves a done slot alone)
+                    if (P.verify[sl] && refresh_slot(P, sl)) {
+                        const double rn = sqrt(s0) / P.bnorm[sl];
+                        P.verify[sl] = 0;
+                        if (rn < P.tol[sl]) { P.rnorm[sl] = rn; P.done[sl] = 1; P.status[sl] = 0; }
+                    }
+                    break;
                 case kFinRz:
                     P.beta[sl] = P.pmode[sl] == 1 ? 0.0 : s0 / P.rz[sl];
                     P.rz[sl] = s0;
@@ -628,7 +671,10 @@ __global__ void __launch_bounds__(kFinThreads) k_b_fin(bp P, int mode) {
         __syncthreads();
         if (threadIdx.x == 0) *P.refresh_due = any_cen;
     }
-    if (mode == kFinXr || mode == kFinSpmv) {
+    if (mode == kFinSpmv)   // the step this iteration's x and r updates take (0: fresh or done)
+        for (unsigned sl = threadIdx.x; sl < nslots; sl += blockDim.x)
+            P.xa[sl] = (!P.done[sl] && !P.fresh[sl]) ? P.alpha[sl] : 0.0;
+    if (mode == kFinXr || mode == kFinSpmv || mode == kFinVerify) {
         for (unsigned sl = threadIdx.x; sl < nslots; sl += blockDim.x)
             if (!P.done[sl]) {
                 any_live = 1;
@@ -732,6 +778,7 @@ __global__ void k_b_mark_admit(bp P, unsigned sl, double tol) {
     if (threadIdx.x == 0) {
         P.fresh[sl] = 1;
         P.done[sl] = 0;
+        P.verify[sl] = 0;
         P.tol[sl] = tol;
         *P.all_done = 0;
     }
@@ -779,6 +826,8 @@ struct apxb_batch {
     bool y_armed = false;
     double* sd = nullptr;   // kSd double arrays of S*K
     int* si = nullptr;      // 6 int arrays of S*K, all_done, any_center, refresh_due
+    double* xa = nullptr;   // per slot (bp::xa)
+    int* verify = nullptr;  // per slot (bp::verify)
     int refresh_every = 25; // periodic fp64 residual refresh (bp::refresh_every)
     unsigned long long* applies = nullptr;
     double* partials = nullptr;
@@ -852,6 +901,7 @@ struct apxb_batch {
         P.fresh = s + 5 * ns; P.all_done = s + 6 * ns; P.any_center = s + 6 * ns + 1; P.refresh_due = s + 6 * ns + 2;
         P.refresh_every = refresh_every;
         P.applies = applies;
+        P.xa = xa; P.verify = verify;
         P.max_iter = max_iter; P.stag = 50; P.center_k = e->center_k;
         P.partials = partials; P.err = e->d_err;
         return P;
@@ -916,6 +966,7 @@ int launch_iteration_k(apxb_batch* bt, const bp& P, cudaStream_t s, unsigned lon
         if constexpr (K == 1) k_b_spmv<K><<<g, kBT, 0, s>>>(P, P.x, P.Ap, 2);
         else k_b_spmv_pairs<K><<<g, kBT, 0, s>>>(P, P.x, P.Ap, 2);
         k_b_refresh<K><<<g, kBT, 0, s>>>(P);
+        k_b_fin<<<1, kFinThreads, 0, s>>>(P, kFinVerify);
     }
     if (bt->n_long) {
         k_b_spmv_chunks<K><<<std::min<unsigned>(bt->n_sp_chunks, 4u * g), kBT, 0, s>>>(P, P.p, 0);
@@ -1236,6 +1287,7 @@ int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, a
             (rc = bt->dalloc(&bt->Ap, nk)) || (rc = bt->dalloc(&bt->b, nk)) || (rc = bt->dalloc(&bt->rhs32, nk)) ||
             (rc = bt->dalloc(&bt->Yf, nk)) || (rc = bt->dalloc(&bt->Zf, nk)) || (rc = bt->dalloc(&bt->sd, kSd * ns)) ||
             (rc = bt->dalloc(&bt->si, 6 * ns + 3)) || (rc = bt->dalloc(&bt->applies, ns)) ||
+            (rc = bt->dalloc(&bt->xa, ns)) || (rc = bt->dalloc(&bt->verify, ns)) ||
             (rc = bt->dalloc(&bt->partials, static_cast<size_t>(bt->n_tiles) * k * 2)) || (rc = bt->dalloc(&bt->d_B, nk)))
             return rc;
         APXB_CK(cudaMallocHost(&bt->h_sd, sizeof(double) * kSd * ns));
@@ -1251,6 +1303,8 @@ int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, a
             APXB_CK(cudaMemcpyAsync(bt->si + 6 * ns, idle.data(), sizeof(int), cudaMemcpyHostToDevice, s));
         }
         APXB_CK(cudaMemsetAsync(bt->applies, 0, sizeof(unsigned long long) * ns, s));
+        APXB_CK(cudaMemsetAsync(bt->xa, 0, sizeof(double) * ns, s));
+        APXB_CK(cudaMemsetAsync(bt->verify, 0, sizeof(int) * ns, s));
         APXB_CK(cudaMemsetAsync(bt->p, 0, sizeof(double) * nk, s));
         // Zf: markers on factor rows, 0 on each Laplacian instance's grounded row
         apxb::launch_fill_sent32(bt->Yf, nk, s);

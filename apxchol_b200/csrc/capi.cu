@@ -53,6 +53,7 @@ int apxb_engine_create(int device, apxb_engine** out) {
     *out = nullptr;
     int ndev = 0;
     APXB_CK(cudaGetDeviceCount(&ndev));
+    if (device == APXB_CURRENT_DEVICE) APXB_CK(cudaGetDevice(&device));
     if (device < 0 || device >= ndev) return fail(APXB_ERR_INVALID, "no such device " + std::to_string(device));
     APXB_CK(cudaSetDevice(device));
     std::unique_ptr<apxb_engine> e(new (std::nothrow) apxb_engine);
@@ -221,6 +222,7 @@ int apxb_factor_create(apxb_engine* e, uint32_t n, const uint32_t* colptr, const
         if (!f) return fail(APXB_ERR_INVALID, "host allocation failed");
         f->e = e;
         f->precision = precision;
+        f->drop_rel = drop_rel < 0.0 ? apxb::kDropRelDefault : drop_rel;
         const std::string why = apxb::prepare_factor(n, colptr, rowidx, vals, perm, sddm != 0, rounds, n_rounds,
                                                      drop_rel, f->h, fp16);
         if (!why.empty()) return fail(APXB_ERR_BAD_FACTOR, why);
@@ -315,6 +317,11 @@ int apxb_factor_info_get(const apxb_factor* f, apxb_factor_info* info) {
     info->fwd_levels = f->h.fwd_levels; info->bck_levels = f->h.bck_levels;
     info->precision = f->precision; info->sddm = f->h.sddm ? 1 : 0;
     info->device_bytes = f->dev_bytes; info->apply_count = f->apply_count;
+    info->drop_rel = f->drop_rel;
+    info->dropped_flush = f->h.dropped_flush;
+    info->sweep_grid = f->e->sweep_grid > 0 ? f->e->sweep_grid
+                     : f->precision == APXB_PREC_FP64 ? f->grid64 : apxb::sweep_grid32(1, f->e->num_sms);
+    info->reserved = 0;
     return APXB_OK;
 }
 
@@ -349,31 +356,6 @@ int apxb_factor_reset_apply_count(apxb_factor* f) {
 namespace {
 
 int grid64_of(const apxb_factor* f) { return f->e->sweep_grid > 0 ? f->e->sweep_grid : f->grid64; }
-
-template <class T>
-void plan_args(const apxb_factor* f, int dir, apxb::sweep_args<T>& a) {
-    const apxb::sweep_plan& pl = dir == 0 ? f->h.fwd_plan : f->h.bck_plan;
-    a.m = f->h.m;
-    a.n_items = pl.n_items;
-    a.info = f->info[dir];
-    a.ord = f->ord[dir];
-    a.ptr = f->ptr[dir];
-    a.idx = f->idx[dir];
-    a.val = f->val[dir];
-    a.val16 = f->val16[dir];
-    a.diag16 = f->diag16;
-    a.in_scale2 = nullptr;   // set for the backward of an fp16 factor by its caller
-    a.seg_first = pl.seg_first;
-    a.seg_rows = pl.seg_rows;
-    a.seg_levels = pl.seg_levels;
-    a.seg_row = f->seg_row[dir];
-    a.seg_lvl = f->seg_lvl[dir];
-    a.seg_ptr = f->seg_ptr[dir];
-    a.seg_idx = f->seg_idx[dir];
-    a.seg_val = f->seg_val[dir];
-    a.chunk = f->chunk[dir];
-    a.n_chunks = f->n_chunks[dir];
-}
 
 apxb::sweep_args<double> sweep64_args(apxb_factor* f, int dir) {
     apxb::sweep_args<double> a{};

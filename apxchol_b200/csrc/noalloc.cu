@@ -16,7 +16,11 @@
 // (1 MiB + 256 B), held by every GPU that loads this code until the process
 // exits. Its host-side name is not a device address: the address is taken with
 // cudaGetSymbolAddress once per device, with that device current, on the first
-// call that runs on it.
+// call that runs on it, and kept for the life of the process: after a
+// cudaDeviceReset the module is loaded again and the kept address is stale,
+// so this entry point must not be used on a device that has been reset.
+// Every call ends by reading the engine's error word, which waits for the
+// engine stream.
 #include <mutex>
 
 #include "objects.hpp"
@@ -65,15 +69,8 @@ int scratch_on(int device, double** out) {
 }
 
 apxb::sweep_args<double> noalloc_args(const apxb_factor* f, int dir, apxb::sweep_ctl* ctl) {
-    const apxb::sweep_plan& pl = dir == 0 ? f->h.fwd_plan : f->h.bck_plan;
     apxb::sweep_args<double> a{};
-    a.m = f->h.m;
-    a.n_items = pl.n_items;
-    a.info = f->info[dir]; a.ord = f->ord[dir]; a.ptr = f->ptr[dir]; a.idx = f->idx[dir]; a.val = f->val[dir];
-    a.seg_first = pl.seg_first; a.seg_rows = pl.seg_rows; a.seg_levels = pl.seg_levels;
-    a.seg_row = f->seg_row[dir]; a.seg_lvl = f->seg_lvl[dir]; a.seg_ptr = f->seg_ptr[dir];
-    a.seg_idx = f->seg_idx[dir]; a.seg_val = f->seg_val[dir];
-    a.chunk = f->chunk[dir]; a.n_chunks = f->n_chunks[dir];
+    plan_args(f, dir, a);
     a.ctl = ctl + dir;
     a.err = f->e->d_err;
     a.budget_ns = f->e->budget_ns;

@@ -131,6 +131,7 @@ struct apxb_factor {
     apxb_engine* e = nullptr;
     apxb::prepared_factor h;
     int precision = APXB_PREC_FP64;
+    double drop_rel = 0.0;                             // threshold in effect
     uint64_t apply_count = 0;
     uint64_t dev_bytes = 0;
     std::vector<std::pair<void*, size_t>> owned;
@@ -209,3 +210,30 @@ struct apxb_operator {
     }
 };
 
+// The plan pointers of direction dir of factor f (forward: CSR(L11), backward:
+// CSC(L11)) in a sweep's launch arguments; every sweep entry point starts from
+// this, then sets its vectors, counters and error word.
+template <class T>
+inline void plan_args(const apxb_factor* f, int dir, apxb::sweep_args<T>& a) {
+    const apxb::sweep_plan& pl = dir == 0 ? f->h.fwd_plan : f->h.bck_plan;
+    a.m = f->h.m;
+    a.n_items = pl.n_items;
+    a.info = f->info[dir];
+    a.ord = f->ord[dir];
+    a.ptr = f->ptr[dir];
+    a.idx = f->idx[dir];
+    a.val = f->val[dir];
+    a.val16 = f->val16[dir];
+    a.diag16 = f->diag16;
+    a.in_scale2 = nullptr;   // set for the backward of an fp16 factor by its caller
+    a.seg_first = pl.seg_first;
+    a.seg_rows = pl.seg_rows;
+    a.seg_levels = pl.seg_levels;
+    a.seg_row = f->seg_row[dir];
+    a.seg_lvl = f->seg_lvl[dir];
+    a.seg_ptr = f->seg_ptr[dir];
+    a.seg_idx = f->seg_idx[dir];
+    a.seg_val = f->seg_val[dir];
+    a.chunk = f->chunk[dir];
+    a.n_chunks = f->n_chunks[dir];
+}

@@ -37,7 +37,9 @@ class FactorInfo(ctypes.Structure):
                 ("nnz_stored", ctypes.c_uint64), ("dropped", ctypes.c_uint64),
                 ("fwd_levels", ctypes.c_int32), ("bck_levels", ctypes.c_int32),
                 ("precision", ctypes.c_int32), ("sddm", ctypes.c_int32),
-                ("device_bytes", ctypes.c_uint64), ("apply_count", ctypes.c_uint64)]
+                ("device_bytes", ctypes.c_uint64), ("apply_count", ctypes.c_uint64),
+                ("drop_rel", ctypes.c_double), ("dropped_flush", ctypes.c_uint64),
+                ("sweep_grid", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class PcgResult(ctypes.Structure):
@@ -418,7 +420,8 @@ class Batch:
         return res
 
     def set_refresh(self, every: int):
-        """Recompute a slot's residual as b - A x (fp64) every `every` of its iterations (0: never)."""
+        """Recompute a slot's residual as b - A x (fp64) every `every` of its iterations, and once more to
+        confirm convergence before a slot stops (0: never; the recurrence alone then stops a slot)."""
         check(self.lib.apxb_batch_set_refresh(self.h, every))
 
     # -- continuous batching (every call enqueues and returns) --

@@ -50,9 +50,13 @@ class Factor:
         return self.n if self.sddm else self.n - 1
 
 
-def build(ref_root: str = "/root/reference") -> None:
-    """Compile the library from the reference sources (needs the reference tree)."""
+def build(ref_root: str | None = None) -> None:
+    """Compile the library from the reference sources (ref_root, else
+    $APXCHOL_REF: the reference source tree)."""
     import subprocess
+    ref_root = ref_root or os.environ.get("APXCHOL_REF", "")
+    if not ref_root or not os.path.isdir(ref_root):
+        raise RuntimeError("reference source tree not found: pass ref_root or set APXCHOL_REF")
     subprocess.check_call(["make", "-s", "-C", _HERE, f"REF={ref_root}"])
 
 

@@ -5,15 +5,16 @@ and the SpTRSV sweeps' HBM GB/s.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
                     [--workload grid3d_128|rmat_22|instances_256|serving_8]
                     [--k K [--lanes L] [--sweep-grid B]] [--grid G]
-                    [--no-serving] [--no-plain] [--no-cpu-baseline]
+                    [--no-serving] [--no-serving-mix] [--no-plain] [--no-cpu-baseline]
 
 Our arm. The headline is the batched mixed-precision form: one step is one
 batched PCG solve of k right-hand sides, with fp32 factor sweeps and fp64
 SpMV, residual, dots and centring. k, the sweep grid and the number of lanes
 are picked by the autotuner (apxchol_b200/autotune.py) unless --k is given.
-Every step solves a
-fresh set of N(0,1) right-hand sides from a pool of distinct sets. The line
-reports:
+The right-hand sides
+come from a pool of 5 sets of N(0,1) vectors (5 is coprime with the 1-4
+lanes): within a step every lane solves a different set, and a lane's set
+changes from one step to the next. The line reports:
   * value      solves/s over K device-resident steps: every lane (a batch on
                its own stream, apxchol_b200/lanes.py) solves K batches back to
                back, the lanes joined once at the end; CUDA events on lane 0's
@@ -27,13 +28,21 @@ reports:
                (continuous batching) at 70% of the measured capacity, tolerance
                drawn from {1e-6, 1e-8, 1e-10}: solves/s and p50/p99 latency
                from arrival to result.
+  * serving_mix  the 8-matrix serving workload (serving_8 below) at 50, 200
+               and 800 req/s: solves/s, p50/p99 and not-converged per rate,
+               with two matrices admitted mid-stream under a 60 GB budget.
   * roofline   the fp32 k-RHS sweep kernel: algorithmic bytes per sweep
                (nnz_s*8 + 4(m+1) + 2*m*4*k) / measured sweep time, against the
                measured HBM copy bandwidth. iter_frac: the factor + matrix bytes
                of one PCG iteration (460 MB at 128^3) over the batch's time per
                iteration; iter_all_frac: all the iteration's algorithmic bytes
                (factor, matrix and every vector pass) over that time.
-  * cpu_baseline  the reference's own cpu_solver (oracle/_ref) on the host cores.
+  * cpu_baseline  the reference's own cpu_solver (oracle/_ref; its x86-64-v4
+               build on an AVX-512 host) on the host's physical cores: median of
+               8 solves of fresh seeded right-hand sides, and its omp_sptrsv
+               sweep pair. Those are the first right-hand sides lane 0 solved,
+               so oracle_err_max is the largest relative error of the batched
+               mixed-precision solutions against the reference's FP64 ones.
 Inputs exceed L2 (factor + operator > 400 MB per iteration), so no flush is needed.
 
 --workload selects the other configurations (one JSON line each): rmat_22 (an
@@ -42,8 +51,9 @@ batch), serving_8 (8 resident matrices under open-loop Poisson arrivals at 50,
 200 and 800 requests/s, p50/p99 per rate). --grid G swaps the 128^3 grid for
 G^3, a quicker check; the config's "l2" note says whether its inputs fit in L2.
 
---impl reference: the reference's CPU solve phase (rank 0 only), each step one
-solve of the same system; prints the same JSON line with "impl": "reference".
+--impl reference: the reference's CPU solve phase (rank 0 only) on the host's
+physical cores, each step one solve of a right-hand side from a pool of 5;
+prints the same JSON line with "impl": "reference".
 
 With torchrun (N > 1) every rank solves its own replica (no collective on the
 data path); value = all ranks' solves / max-over-ranks time.
@@ -69,7 +79,7 @@ TOL = 1e-8
 MAX_ITER = 500
 FACTOR_SEED = 1
 FACTOR_THREADS = 8
-POOL = 4            # distinct right-hand-side sets cycled through the steps
+POOL = 5            # distinct right-hand-side sets cycled through the steps (coprime with 1-4 lanes)
 
 
 def log(*a):
@@ -201,24 +211,39 @@ def from_rank0(values, world: int, device):
     return [float(v) for v in t.cpu()]
 
 
-def cpu_baseline(A, F, b, samples: int = 12):
-    """The reference cpu_solver on this host (bounded sample of solves)."""
+def cpu_baseline(A, F, rhs, samples: int = 8, X_gpu=None):
+    """The reference cpu_solver on this host's physical cores: `samples` solves
+    of fresh seeded right-hand sides rhs(0), rhs(1), ... (median time), and its
+    omp_sptrsv forward + backward pair. X_gpu[c] (optional): the GPU's
+    batched mixed-precision solution of rhs(c); each one's relative error
+    against the reference solution of the same system is reported."""
     import oracle
     if not oracle.ref_available():
         return None
-    cores = os.cpu_count() or 1
+    lib = oracle.use_fastest_ref()
+    cores = oracle.host_cores()
     oracle.set_threads(cores)
     R = oracle.Ref(A, F)
-    times, its = [], []
-    for _ in range(samples):
+    times, its, tres, errs = [], [], [], []
+    for j in range(samples):
+        b = rhs(j)
         x, it, res, secs = R.solve(b, TOL, MAX_ITER)
         times.append(secs)
-        its.append(it)
+        its.append(int(it))
+        tres.append(float(np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b)))
+        if X_gpu is not None and j < len(X_gpu):
+            errs.append(float(np.linalg.norm(X_gpu[j] - x) / np.linalg.norm(x)))
+    pair = R.pair_seconds(np.random.default_rng(5).standard_normal(R.m), 5)
     med = statistics.median(times)
-    return {"value": 1.0 / med, "unit": "solves/s", "cores": cores, "kind": "reference",
-            "sample": f"{samples} solves of the same system (median {med * 1e3:.0f} ms, {its[0]} iterations), "
-                      f"reference cpu_solver OMP_NUM_THREADS={cores}",
-            "iterations": int(its[0])}
+    out = {"value": 1.0 / med, "unit": "solves/s", "cores": cores, "kind": "reference",
+           "sample": f"{samples} solves of fresh seeded right-hand sides (median {med * 1e3:.0f} ms, "
+                     f"{min(its)}-{max(its)} iterations), reference cpu_solver ({lib}) "
+                     f"OMP_NUM_THREADS={cores} physical cores",
+           "iterations": [min(its), max(its)], "true_relres_max": max(tres),
+           "omp_sptrsv_pair_ms": pair * 1e3}
+    if errs:
+        out["oracle_err"] = errs
+    return out
 
 
 def run_reference(args, rank, world):
@@ -230,14 +255,16 @@ def run_reference(args, rank, world):
         print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref missing"}))
         return 0
     A, F = build_problem(args.grid)
-    b = gen.rhs(A.n, 1000, False)
-    cores = os.cpu_count() or 1
+    pool = [gen.rhs(A.n, 1000 + j, False) for j in range(POOL)]
+    lib = oracle.use_fastest_ref()
+    cores = oracle.host_cores()
     oracle.set_threads(cores)
     R = oracle.Ref(A, F)
-    for _ in range(args.warmup):
-        R.solve(b, TOL, MAX_ITER)
+    for j in range(args.warmup):
+        R.solve(pool[j % POOL], TOL, MAX_ITER)
     secs, its = [], []
-    for _ in range(args.steps):
+    for j in range(args.steps):
+        b = pool[j % POOL]           # a different right-hand side each step
         x, it, res, s = R.solve(b, TOL, MAX_ITER)
         secs.append(s)
         its.append(it)
@@ -250,7 +277,8 @@ def run_reference(args, rank, world):
             "config": workload_config(args.grid, A, F, "reference cpu_solver, 1 RHS per solve"),
             "impl": "reference",
             "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "reference",
-                             "sample": f"{args.steps} solves, reference cpu_solver OMP_NUM_THREADS={cores}"},
+                             "sample": f"{args.steps} solves of {POOL} cycled seeded right-hand sides, reference "
+                                       f"cpu_solver ({lib}) OMP_NUM_THREADS={cores} physical cores"},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "iterations": int(its[-1]), "true_relres": tres}
     print(json.dumps(line), flush=True)
@@ -352,8 +380,11 @@ def run_ours(args, rank, world, local_rank):
     its = [r.iterations for lane in res for r in lane[:k]]
     dev_tres = max(r.true_residual for lane in res for r in lane[:k])
     host_tres = 0.0
+    x_lane0 = None   # lane 0 solved set 0: right-hand sides rhs(0) .. rhs(k - 1)
     for j in range(nlanes):
         X0, B0 = dXs[j].cpu().numpy(), sets[j % POOL][0]
+        if j == 0:
+            x_lane0 = [X0[c * n:(c + 1) * n].copy() for c in range(k)]
         for c in range(k):
             bcol, xcol = B0[c * n:(c + 1) * n], X0[c * n:(c + 1) * n]
             host_tres = max(host_tres, float(np.linalg.norm(bcol - A.matvec(xcol)) / np.linalg.norm(bcol)))
@@ -477,6 +508,16 @@ def run_ours(args, rank, world, local_rank):
             log(f"[bench] plain fp64 failed: {ex}")
 
     value = world * args.steps * k * nlanes / dev_s
+    mix = None
+    if not args.no_serving_mix and rank == 0:
+        try:   # the 8-matrix serving workload beside the headline (reported in its field)
+            rates, resident_gb = serving_mix(local_rank)
+            mix = {"workload": "serving_8: 8 matrices (2 x 2D grid 1024^2, 2 x 3D grid 96^3, 2 x R-MAT scale 20 "
+                               "LCC, 2 x random 6-regular n=500k), Poisson arrivals, 60 GB budget, k=8",
+                   "rates": rates, "resident_gb": resident_gb}
+        except Exception as ex:
+            mix = {"error": f"{type(ex).__name__}: {ex}"}
+            log(f"[bench] serving mix failed: {ex}")
     serving = None
     if not args.no_serving and rank == 0:
         try:
@@ -490,9 +531,9 @@ def run_ours(args, rank, world, local_rank):
         eng.close()
         return 0
     mean_its = sum(iters_timed) / max(1, len(iters_timed))
-    # per batched solve: admit; per iteration 12 kernels plus the residual refresh's SpMV and update
-    # (on by default; no long rows here); x out
-    launches_per_step = nlanes * (1 + 14 * (mean_its + 1) + 3)
+    # per batched solve: admit; per iteration 12 kernels plus the residual refresh's SpMV, update and
+    # verification finalize (on by default; no long rows here); x out
+    launches_per_step = nlanes * (1 + 15 * (mean_its + 1) + 3)
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_s / args.steps * 1e3,
@@ -514,13 +555,22 @@ def run_ours(args, rank, world, local_rank):
         "plain_fp64": plain,
         "speedup_vs_plain_fp64": (value / world) / plain["solves_s"] if plain and "solves_s" in plain else None,
         "serving": serving,
+        "serving_mix": mix,
         "autotune": tuned,
         "gpu_launches": int(round(launches_per_step * args.steps)),
         "clocks": clk.summary(),
     }
     if not args.no_cpu_baseline:
         try:
-            line["cpu_baseline"] = cpu_baseline(A, F, rhs(0))
+            # the reference solves the first right-hand sides lane 0 solved, so the batched mixed-precision
+            # solutions get their error against the FP64 reference solution of the same systems
+            cb = cpu_baseline(A, F, rhs, X_gpu=x_lane0)
+            line["cpu_baseline"] = cb
+            if cb and cb.get("oracle_err"):
+                line["oracle_err_max"] = max(cb["oracle_err"])
+                line["oracle_err_note"] = (f"max over {len(cb['oracle_err'])} batched mixed-precision solutions of "
+                                           "||x - x_ref|| / ||x_ref||, x_ref the reference cpu_solver's FP64 "
+                                           "solution of the same system at the same tolerance")
         except Exception as ex:   # the baseline is context only
             line["cpu_baseline"] = {"error": str(ex)}
     print(json.dumps(line), flush=True)
@@ -655,17 +705,16 @@ def run_instances256(args, rank, world, local_rank):
     return 0
 
 
-def run_serving8(args, rank, world, local_rank):
-    """8 resident matrices, open-loop Poisson requests at 50/200/800 req/s
-    (matrix uniform, tol from {1e-6, 1e-8, 1e-10}); two matrices are admitted
-    only when their first request arrives (60 GB budget)."""
-    import torch
+def serving_mix(device, sweep_grid=None, log_fn=log):
+    """The 8-matrix serving workload (C5): 8 registered matrices, 6 resident at
+    the start, open-loop Poisson requests at 50 / 200 / 800 req/s (matrix
+    uniform, tolerance from {1e-6, 1e-8, 1e-10}, >= 1000 requests per rate);
+    the two matrices not resident are admitted when their first request
+    arrives, under a 60 GB budget. Returns (rates, resident GB)."""
     from apxchol_b200 import gen, workloads
     from apxchol_b200.serve import SolveServer, latency_stats
-    torch.cuda.set_device(local_rank)
-    mats = workloads.serving_8(log)
-    srv = SolveServer(device=local_rank, budget_bytes=60 * 10**9, k=8, iters_per_step=2,
-                      sweep_grid=args.sweep_grid or None)
+    mats = workloads.serving_8(log_fn)
+    srv = SolveServer(device=device, budget_bytes=60 * 10**9, k=8, iters_per_step=2, sweep_grid=sweep_grid or None)
     rates = []
     try:
         for name, A, F in mats:
@@ -693,11 +742,21 @@ def run_serving8(args, rank, world, local_rank):
             rates.append({"rate_req_s": rate, "requests": len(done), "solves_s": len(done) / wall,
                           "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "not_converged": sum(q.status != 0 for q in done),
                           "matrix_admissions": srv.admissions - adm0})
-            log(f"[bench] serving_8 {rate} req/s: {len(done) / wall:.1f} solves/s, p50 {st['p50_ms']:.1f} ms, "
-                f"p99 {st['p99_ms']:.1f} ms")
+            log_fn(f"[bench] serving_8 {rate} req/s: {len(done) / wall:.1f} solves/s, p50 {st['p50_ms']:.1f} ms, "
+                   f"p99 {st['p99_ms']:.1f} ms")
         resident_gb = srv.used_bytes() / 1e9
     finally:
         srv.close()
+    return rates, resident_gb
+
+
+def run_serving8(args, rank, world, local_rank):
+    """8 resident matrices, open-loop Poisson requests at 50/200/800 req/s
+    (matrix uniform, tol from {1e-6, 1e-8, 1e-10}); two matrices are admitted
+    only when their first request arrives (60 GB budget)."""
+    import torch
+    torch.cuda.set_device(local_rank)
+    rates, resident_gb = serving_mix(local_rank, args.sweep_grid)
     line = {"metric": METRIC, "value": rates[-1]["solves_s"], "unit": "solves/s", "n_gpus": world, "steps": len(rates),
             "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 sweeps / f64 outer", "data": "synthetic (seeded generator)",
@@ -722,6 +781,7 @@ def main():
     ap.add_argument("--iters-per-step", type=int, default=2, help="serving: iterations per server step")
     ap.add_argument("--serve-requests", type=int, default=1000)
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-serving-mix", action="store_true", help="skip the 8-matrix serving field")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="grid3d_128", choices=["grid3d_128", "rmat_22", "instances_256", "serving_8"],

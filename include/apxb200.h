@@ -71,6 +71,10 @@ typedef struct apxb_factor_info {
     int32_t  sddm;
     uint64_t device_bytes;   /* device memory held by the factor */
     uint64_t apply_count;    /* center-k application counter */
+    double   drop_rel;       /* drop threshold in effect (factor_drop.h: rel) */
+    uint64_t dropped_flush;  /* of `dropped`: off-diagonals fp16 storage would store as zero */
+    int32_t  sweep_grid;     /* blocks of the resident sweep grid of this factor's sweeps */
+    int32_t  reserved;
 } apxb_factor_info;
 
 typedef struct apxb_pcg_result {
@@ -84,7 +88,10 @@ typedef struct apxb_pcg_result {
 const char* apxb_last_error(void);
 const char* apxb_version(void);
 
-/* ---- engine: one GPU, one stream, an error word and workspaces ---- */
+/* ---- engine: one GPU, one stream, an error word and workspaces ----
+ * device: a CUDA device index, or APXB_CURRENT_DEVICE for the calling
+ * thread's current device (where the reference's classes run). */
+#define APXB_CURRENT_DEVICE (-1)
 int apxb_engine_create(int device, apxb_engine** out);
 /* With factors or operators still alive the engine is only marked closed; the
  * last of them to be destroyed releases it. */
@@ -171,6 +178,10 @@ int apxb_sweep_pair(apxb_engine* e, apxb_factor* f, const double* d_in, double* 
  * and the factor must be fp64. The engine and the factor are created (and
  * allocate) beforehand. The first call on a device looks up the array's
  * device address on it: make that first call before any stream capture.
+ * That address is kept for the life of the process; after cudaDeviceReset it
+ * is stale, so do not call this on a device that has been reset. Every call
+ * returns after the engine stream has finished its sweeps (it reads the
+ * engine's error word).
  * Every call re-arms the array, but all calls on one device share it: calls
  * whose work overlaps on the GPU (other engines' streams, other host threads)
  * race and corrupt each other's results. */
@@ -226,8 +237,15 @@ int apxb_batch_solve(apxb_batch* b, const double* B, double* X, const int* nrhs,
 /* Periodic true-residual refresh (fp64): every `every` iterations of a slot
  * (its own count, so a slot's arithmetic does not depend on the other
  * slots) its residual is recomputed as b - A x before the x/r update, which
- * keeps the fp64 recurrence from drifting away from the true residual. Default
- * 25; 0 turns it off. Only while no slot is admitted (else APXB_ERR_BUSY). */
+ * keeps the fp64 recurrence from drifting away from the true residual. The
+ * same refresh confirms convergence: a slot whose recurrence residual drops
+ * below its tolerance in an iteration that did not start with a refresh runs
+ * one more iteration that does, and stops only if the residual taken from the
+ * recomputed b - A x is below its tolerance (so a converged slot's fp64
+ * relative residual ||b - A x|| / ||b|| meets its tolerance, up to the rounding
+ * of one update). At max_iter the recurrence alone decides. Default 25; 0 turns
+ * off both (the stop then follows the recurrence, as apxb_pcg). Only while no
+ * slot is admitted (else APXB_ERR_BUSY). */
 int apxb_batch_set_refresh(apxb_batch* b, int every);
 
 /* Host-only (no GPU): builds and checks the batch sweep plans apxb_batch_create

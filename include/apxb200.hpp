@@ -16,6 +16,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -39,8 +40,13 @@ public:
     engine& operator=(const engine&) = delete;
     apxb_engine* get() const { return h_; }
 
-    static std::shared_ptr<engine> shared(int device = 0) {
-        static std::shared_ptr<engine> e;   // one device per process, as the reference
+    // The process's engine, created on first use on `device` (by default the
+    // calling thread's current device); one device per process, as the
+    // reference's classes. Thread-safe.
+    static std::shared_ptr<engine> shared(int device = APXB_CURRENT_DEVICE) {
+        static std::mutex mu;
+        static std::shared_ptr<engine> e;
+        std::lock_guard<std::mutex> lock(mu);
         if (!e) e = std::make_shared<engine>(device);
         return e;
     }

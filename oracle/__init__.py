@@ -19,6 +19,7 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(_HERE, "_ref", "libapxref.so")
+REF_LIB_V4 = os.path.join(_HERE, "_ref", "libapxref_v4.so")   # the same sources for x86-64-v4 (AVX-512)
 ORACLE_LIB = os.path.join(_HERE, "_build", "liboracle.so")
 
 c_p = ctypes.c_void_p
@@ -28,23 +29,71 @@ def _ptr(a):
     return None if a is None else a.ctypes.data
 
 
-def build(ref_root: str = "/root/reference") -> None:
+def build(ref_root: str | None = None) -> None:
+    """Compile the checkers; the reference library only where the reference
+    source tree (ref_root, else $APXCHOL_REF) is present."""
     import subprocess
-    targets = ["oracle"] + (["ref"] if os.path.isdir(ref_root) else [])
+    ref_root = ref_root or os.environ.get("APXCHOL_REF", "")
+    targets = ["oracle"] + (["ref"] if ref_root and os.path.isdir(ref_root) else [])
     subprocess.check_call(["make", "-s", "-C", _HERE, f"REF={ref_root}"] + targets)
 
 
 # --------------------------------------------------------------------- reference
 
 _ref = None
+_ref_path = REF_LIB
+
+_V4_FLAGS = ("avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl")
 
 
-def _load_ref():
+def host_has_avx512() -> bool:
+    """Whether this host runs x86-64-v4 code (the AVX-512 subsets it needs)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    fl = set(line.split(":", 1)[1].split())
+                    return all(x in fl for x in _V4_FLAGS)
+    except OSError:
+        pass
+    return False
+
+
+def use_fastest_ref() -> str:
+    """Load the x86-64-v4 build of the reference where this host supports it
+    (the timed CPU baseline); else the portable build. Call before the first
+    use of `Ref`. Returns the library's file name."""
+    global _ref_path
+    if _ref is None and os.path.exists(REF_LIB_V4) and host_has_avx512():
+        _ref_path = REF_LIB_V4
+    return os.path.basename(_ref_path)
+
+
+def host_cores() -> int:
+    """Physical cores this process may run on: the CPUs of its affinity mask
+    divided by the hardware threads per core (the count OMP_NUM_THREADS is set
+    to for the CPU baseline)."""
+    avail = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    try:
+        import psutil
+        logical, physical = psutil.cpu_count(logical=True), psutil.cpu_count(logical=False)
+        per_core = max(1, (logical or 1) // max(1, physical or 1))
+    except Exception:
+        per_core = 1
+    return max(1, avail // per_core)
+
+
+_ref_libs = {}
+
+
+def _load_ref(path: str | None = None):
+    """The reference library at `path` (default: the selected build), loaded once."""
     global _ref
-    if _ref is None:
-        if not os.path.exists(REF_LIB):
-            raise RuntimeError(f"reference CPU library missing: {REF_LIB}")
-        lib = ctypes.CDLL(REF_LIB)
+    path = path or _ref_path
+    if path not in _ref_libs:
+        if not os.path.exists(path):
+            raise RuntimeError(f"reference CPU library missing: {path}")
+        lib = ctypes.CDLL(path)
         lib.apxref_last_error.restype = ctypes.c_char_p
         lib.apxref_set_threads.argtypes = [ctypes.c_int]
         lib.apxref_solver_create.argtypes = [ctypes.c_int, c_p, c_p, c_p, c_p, c_p, c_p, c_p,
@@ -64,16 +113,18 @@ def _load_ref():
         lib.apxref_level_sizes.argtypes = [c_p, ctypes.c_int, c_p]
         lib.apxref_fp16_prep.argtypes = [ctypes.c_uint32, c_p, c_p, c_p, ctypes.c_int, ctypes.c_double,
                                          c_p, c_p] + [c_p] * 9
-        _ref = lib
-    return _ref
+        _ref_libs[path] = lib
+    if path == _ref_path:
+        _ref = _ref_libs[path]
+    return _ref_libs[path]
 
 
 def ref_available() -> bool:
     return os.path.exists(REF_LIB)
 
 
-def set_threads(t: int) -> int:
-    return _load_ref().apxref_set_threads(t)
+def set_threads(t: int, lib_path: str | None = None) -> int:
+    return _load_ref(lib_path).apxref_set_threads(t)
 
 
 def fp16_prep(fac, rel=-1.0):
@@ -105,8 +156,8 @@ class Ref:
     """The reference cpu_solver built on a given factor (cpu_solver(L, F),
     src/solve.cpp:295-318)."""
 
-    def __init__(self, mat, fac):
-        lib = _load_ref()
+    def __init__(self, mat, fac, lib_path: str | None = None):
+        lib = _load_ref(lib_path)
         self.lib = lib
         self.n = mat.n
         self._keep = [np.ascontiguousarray(a) for a in

@@ -137,3 +137,36 @@ def test_serial_segment_path_is_bit_exact(eng, name, monkeypatch):
     z32 = _pair_dev(eng, D32, x)
     want = O.pair(x)
     assert np.linalg.norm(z32 - want) / np.linalg.norm(want) < FP32_SWEEP_RTOL
+
+
+RZ_RTOL = 1e-12   # r.z: the same products, summed in another (fixed) association than the reference's
+
+
+@pytest.mark.parametrize("name", gc.NAMES)
+def test_apply_fused_and_rz_match_reference_golden(eng, name):
+    """apxb_apply on a fresh factor is the reference's first apply_fused of a
+    solve (preconditioner.h:370-377): z, and r.z returned beside it."""
+    A, F, g = gc.case(name)
+    D = native.DeviceFactor(eng, F)
+    z, rz = D.apply(g["b"])
+    zf, rz_ref = g["apply_fused"], float(g["rz"])
+    if F.sddm:
+        assert np.array_equal(z, zf)
+    else:
+        assert np.linalg.norm(z - zf) <= 1e-12 * np.linalg.norm(zf)
+    assert abs(rz - rz_ref) <= RZ_RTOL * abs(rz_ref), (rz, rz_ref)
+    assert abs(rz - float(np.dot(g["b"], z))) <= RZ_RTOL * abs(rz)
+
+
+def test_apply_rz_over_the_center_k_schedule(eng):
+    """r.z of every application of a 12-application schedule (the 10th centres)
+    against the oracle's apply_fused with the same r_sum."""
+    A, F, g = gc.case("grid2d_32")
+    D = native.DeviceFactor(eng, F)
+    O = oracle.Oracle(A, F)
+    b = g["b"]
+    for k in range(12):
+        z, rz = D.apply(b)
+        zo, rzo = O.apply_fused(b, float(b.sum()), reset=(k == 0))
+        assert np.linalg.norm(z - zo) <= 1e-12 * np.linalg.norm(zo), k
+        assert abs(rz - rzo) <= RZ_RTOL * abs(rzo), (k, rz, rzo)

@@ -70,3 +70,22 @@ def test_center_k_schedule_matches_reference():
     b = np.random.default_rng(5).standard_normal(A.n)
     for k in range(12):
         assert np.array_equal(R.apply(b, reset=(k == 0)), O.apply(b, reset=(k == 0))), k
+
+
+@pytest.mark.skipif(not (oracle.ref_available() and __import__("os").path.exists(oracle.REF_LIB_V4)
+                         and oracle.host_has_avx512()),
+                    reason="x86-64-v4 reference build or an AVX-512 host absent")
+def test_avx512_reference_build_gives_the_same_bits():
+    """The timed CPU baseline may run the x86-64-v4 build of the reference; it
+    must be the same arithmetic as the portable build the oracle is pinned to."""
+    A, F = problem("grid3d_24")
+    b = np.random.default_rng(8).standard_normal(A.n)
+    out = []
+    for path in (oracle.REF_LIB, oracle.REF_LIB_V4):
+        oracle.set_threads(4, path)
+        R = oracle.Ref(A, F, lib_path=path)
+        y = R.forward(b[:R.m])
+        x, it, res, _ = R.solve(b, 1e-8, 500)
+        out.append((y, R.transpose(y), x, it, res))
+    for a, c in zip(out[0], out[1]):
+        assert np.array_equal(a, c)

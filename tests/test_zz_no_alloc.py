@@ -51,6 +51,29 @@ def test_noalloc_matches_sweep_pair_on_two_calls(eng, name):
         D.close()
 
 
+def test_noalloc_on_a_fresh_factor_allocates_nothing(eng):
+    """The first sweep a factor ever runs goes through the no-alloc entry
+    point: the factor's own work vectors do not exist yet, and the call must
+    not create them (engine memory and the factor's device bytes unchanged).
+    Its result must still be the allocating pair's, bit for bit."""
+    import torch
+    A, F = problem("grid2d_256")
+    D = native.DeviceFactor(eng, F, precision=native.PREC_FP64)
+    try:
+        x = torch.from_numpy(np.random.default_rng(12).standard_normal(D.m)).cuda()
+        got = torch.full_like(x, float("nan"))
+        torch.cuda.synchronize()
+        used0, bytes0 = eng.memory_used(), D.get_info().device_bytes
+        _noalloc(eng, D, x, got)
+        assert eng.memory_used() == used0
+        assert D.get_info().device_bytes == bytes0
+        want = torch.empty_like(x)
+        D.sweep_pair(x, want)
+        assert np.array_equal(got.cpu().numpy(), want.cpu().numpy())
+    finally:
+        D.close()
+
+
 def test_noalloc_rejects_what_it_cannot_hold(eng):
     import torch
     A, F = problem("grid3d_48")          # m = 110,592 rows > 65,536
