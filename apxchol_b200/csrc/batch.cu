@@ -1161,9 +1161,30 @@ int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, a
         cudaStream_t s = e->stream;
         const size_t nk = static_cast<size_t>(bt->n_tot) * k, ns = bt->slots();
         int rc;
-        // ---- sweep plans (batch plans for this k; the two directions on two threads) ----
-        {
-            const uint32_t col_lanes = k >= 8 ? static_cast<uint32_t>(k / 4) : 1u;
+        // ---- sweep plans (batch plans for this k) ----
+        const uint32_t col_lanes = k >= 8 ? static_cast<uint32_t>(k / 4) : 1u;
+        if (n_inst == 1 && fs[0]->dev.on) {
+            // a device-prepared factor: the plans are built on the device from its canonical arrays
+            auto alloc_bytes = [&](void** q, size_t bytes) -> std::string {
+                char* c = nullptr;
+                const int r = bt->dalloc(&c, bytes);
+                *q = c;
+                return r ? std::string(apxb_last_error()) : std::string();
+            };
+            for (int dir = 0; dir < 2; ++dir) {
+                apxb::dev_plan_out o;
+                const std::string why = apxb::batch_plan_device(fs[0], dir, col_lanes, alloc_bytes, o, s);
+                if (!why.empty()) return fail(APXB_ERR_CUDA, why);
+                bt->n_items[dir] = o.n_items;
+                bt->info[dir] = o.info; bt->ord[dir] = o.ord; bt->ptr[dir] = o.ptr; bt->idx[dir] = o.idx;
+                bt->val[dir] = o.val; bt->chunk[dir] = o.chunk; bt->n_chunks[dir] = o.n_chunks;
+            }
+        } else {
+            for (const apxb_factor* f : fs)   // host plans read the canonical arrays on the host
+                if (!f->host_arrays) {
+                    const std::string why = apxb::factor_host_arrays(const_cast<apxb_factor*>(f));
+                    if (!why.empty()) return fail(APXB_ERR_CUDA, why);
+                }
             apxb::sweep_plan plans[2];
             std::string bad[2];
             {

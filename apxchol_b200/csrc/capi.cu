@@ -223,9 +223,20 @@ int apxb_factor_create(apxb_engine* e, uint32_t n, const uint32_t* colptr, const
         f->e = e;
         f->precision = precision;
         f->drop_rel = drop_rel < 0.0 ? apxb::kDropRelDefault : drop_rel;
-        const std::string why = apxb::prepare_factor(n, colptr, rowidx, vals, perm, sddm != 0, rounds, n_rounds,
-                                                     drop_rel, f->h, fp16);
-        if (!why.empty()) return fail(APXB_ERR_BAD_FACTOR, why);
+        // Factors with round sizes and fp32 / fp64 storage are prepared by kernels
+        // (devprep.cu); the others on the host. Both give the same arrays.
+        const bool on_device = apxb::device_prep_applies(fp16, n_rounds);
+        if (on_device) {
+            int arc = 0;
+            const std::string why = apxb::prepare_factor_device(f.get(), n, colptr, rowidx, vals, perm, sddm != 0,
+                                                                rounds, n_rounds, drop_rel, &arc);
+            if (arc) return arc;
+            if (!why.empty()) return fail(APXB_ERR_BAD_FACTOR, why);
+        } else {
+            const std::string why = apxb::prepare_factor(n, colptr, rowidx, vals, perm, sddm != 0, rounds, n_rounds,
+                                                         drop_rel, f->h, fp16);
+            if (!why.empty()) return fail(APXB_ERR_BAD_FACTOR, why);
+        }
         const auto& h = f->h;
         const size_t m = h.m, nnz = h.nnz_stored;
         if (nnz >= 0xffffffffull) return fail(APXB_ERR_BAD_FACTOR, "factor nnz exceeds the 32-bit offset range");
@@ -245,11 +256,14 @@ int apxb_factor_create(apxb_engine* e, uint32_t n, const uint32_t* colptr, const
             }
         }
         int rc;
-        if ((rc = f->dalloc(&f->perm, n)) || (rc = f->dalloc(&f->ctl, 2))) return rc;
         cudaStream_t s = e->stream;
-        APXB_CK(cudaMemcpyAsync(f->perm, h.perm.data(), 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s));
+        if ((rc = f->dalloc(&f->ctl, 2))) return rc;
         APXB_CK(cudaMemsetAsync(f->ctl, 0, sizeof(apxb::sweep_ctl) * 2, s));
-        for (int dir = 0; dir < 2; ++dir) {
+        if (!on_device) {
+            if ((rc = f->dalloc(&f->perm, n))) return rc;
+            APXB_CK(cudaMemcpyAsync(f->perm, h.perm.data(), 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s));
+        }
+        for (int dir = 0; dir < 2 && !on_device; ++dir) {
             const apxb::sweep_plan& pl = dir == 0 ? h.fwd_plan : h.bck_plan;
             if ((rc = f->dalloc(&f->info[dir], pl.info.size())) || (rc = f->dalloc(&f->ord[dir], pl.ord.size())) ||
                 (rc = f->dalloc(&f->ptr[dir], pl.ptr.size())) || (rc = f->dalloc(&f->idx[dir], pl.idx.size())) ||
@@ -329,6 +343,10 @@ int apxb_factor_arrays(const apxb_factor* f, uint32_t* csr_ptr, uint32_t* csr_id
                        uint32_t* csc_ptr, uint32_t* csc_idx, float* csc_val, uint8_t* fwd_thin,
                        uint8_t* bck_thin) {
     if (!f) return fail(APXB_ERR_INVALID, "factor is NULL");
+    if (!f->host_arrays) {   // prepared on the device: the host copies on first request
+        const std::string why = apxb::factor_host_arrays(const_cast<apxb_factor*>(f));
+        if (!why.empty()) return fail(APXB_ERR_CUDA, why);
+    }
     const auto& h = f->h;
     if (csr_ptr) std::memcpy(csr_ptr, h.csr_ptr.data(), 4 * h.csr_ptr.size());
     if (csr_idx) std::memcpy(csr_idx, h.csr_idx.data(), 4 * h.csr_idx.size());
@@ -639,22 +657,32 @@ int apxb_operator_create(apxb_engine* e, uint32_t n, const int32_t* colptr, cons
         a->e = e;
         a->n = n;
         std::vector<int32_t> ptr;
-        apxb::plan_vec<int32_t> idx;
-        apxb::plan_vec<double> val;
-        const std::string why = apxb::permute_operator(n, colptr, rowidx, vals, perm, ptr, idx, val);
-        if (!why.empty()) return fail(APXB_ERR_INVALID, why);
-        a->nnz = idx.size();
+        cudaStream_t s = e->stream;
         int rc;
-        if ((rc = a->dalloc(&a->ptr, n + 1)) || (rc = a->dalloc(&a->idx, a->nnz)) || (rc = a->dalloc(&a->val, a->nnz)) ||
-            (rc = a->dalloc(&a->perm, n)) || (rc = a->dalloc(&a->x, n)) || (rc = a->dalloc(&a->r, n)) ||
+        const char* hp = std::getenv("APXB_HOST_PREP");
+        if (hp && *hp && *hp != '0') {   // P A P^T on the host threads
+            apxb::plan_vec<int32_t> idx;
+            apxb::plan_vec<double> val;
+            const std::string why = apxb::permute_operator(n, colptr, rowidx, vals, perm, ptr, idx, val);
+            if (!why.empty()) return fail(APXB_ERR_INVALID, why);
+            a->nnz = idx.size();
+            if ((rc = a->dalloc(&a->ptr, n + 1)) || (rc = a->dalloc(&a->idx, a->nnz)) || (rc = a->dalloc(&a->val, a->nnz)))
+                return rc;
+            APXB_CK(cudaMemcpyAsync(a->ptr, ptr.data(), 4 * (static_cast<size_t>(n) + 1), cudaMemcpyHostToDevice, s));
+            APXB_CK(cudaMemcpyAsync(a->idx, idx.data(), 4 * a->nnz, cudaMemcpyHostToDevice, s));
+            APXB_CK(cudaMemcpyAsync(a->val, val.data(), 8 * a->nnz, cudaMemcpyHostToDevice, s));
+            APXB_CK(cudaStreamSynchronize(s));   // the host arrays go out of scope
+        } else {                          // P A P^T by kernels (devprep.cu): the same arrays
+            int arc = 0;
+            const std::string why = apxb::permute_operator_device(a.get(), n, colptr, rowidx, vals, perm, ptr, &arc);
+            if (arc) return arc;
+            if (!why.empty()) return fail(APXB_ERR_INVALID, why);
+        }
+        if ((rc = a->dalloc(&a->perm, n)) || (rc = a->dalloc(&a->x, n)) || (rc = a->dalloc(&a->r, n)) ||
             (rc = a->dalloc(&a->p, n)) || (rc = a->dalloc(&a->Ap, n)) || (rc = a->dalloc(&a->b_orig, n)) ||
             (rc = a->dalloc(&a->x_orig, n)) || (rc = a->dalloc(&a->st, 1)))
             return rc;
         APXB_CK(cudaMallocHost(&a->h_st, sizeof(apxb::pcg_state)));
-        cudaStream_t s = e->stream;
-        APXB_CK(cudaMemcpyAsync(a->ptr, ptr.data(), 4 * (static_cast<size_t>(n) + 1), cudaMemcpyHostToDevice, s));
-        APXB_CK(cudaMemcpyAsync(a->idx, idx.data(), 4 * a->nnz, cudaMemcpyHostToDevice, s));
-        APXB_CK(cudaMemcpyAsync(a->val, val.data(), 8 * a->nnz, cudaMemcpyHostToDevice, s));
         APXB_CK(cudaMemcpyAsync(a->perm, perm, 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s));
         {   // long rows: cut into chunks summed by one block each (power-law hubs)
             std::vector<uint32_t> lrow, lfirst, clo, chi;

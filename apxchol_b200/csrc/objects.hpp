@@ -5,6 +5,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <exception>
+#include <functional>
 #include <memory>
 #include <new>
 #include <string>
@@ -154,6 +155,19 @@ struct apxb_factor {
     uint32_t *seg_row[2] = {nullptr, nullptr}, *seg_lvl[2] = {nullptr, nullptr};
     uint32_t *seg_ptr[2] = {nullptr, nullptr}, *seg_idx[2] = {nullptr, nullptr};
     float* seg_val[2] = {nullptr, nullptr};
+    // Factors prepared on the device (devprep.cu): the canonical arrays stay
+    // there for batch plans; h then holds sizes and counts only, and its
+    // arrays are filled on demand (factor_host_arrays).
+    struct device_canon {
+        bool on = false;
+        uint32_t *csc_ptr = nullptr, *csc_idx = nullptr, *csr_ptr = nullptr, *csr_idx = nullptr;
+        float *csc_val = nullptr, *csr_val = nullptr;
+        int32_t* fl = nullptr;                         // forward level of every row
+        uint32_t* lb = nullptr;                        // forward level bounds (levels are row ranges)
+        int32_t n_levels = 0;
+        std::vector<uint8_t> thin_level;               // per forward level
+    } dev;
+    bool host_arrays = true;                           // h holds the canonical arrays
     // fp32 sweeps, k right-hand sides
     float *Yf = nullptr, *Zf = nullptr;
     size_t f32_cap = 0;                                // floats per buffer
@@ -237,3 +251,29 @@ inline void plan_args(const apxb_factor* f, int dir, apxb::sweep_args<T>& a) {
     a.chunk = f->chunk[dir];
     a.n_chunks = f->n_chunks[dir];
 }
+
+namespace apxb {
+// Device preparation (devprep.cu): the host preparation's arrays, byte for
+// byte, built by kernels. Applies to fp32/fp64 storage with round sizes.
+bool device_prep_applies(bool fp16, uint32_t n_rounds);
+// Fills f's plans (device), f->dev and f->h's sizes; "" or the reason it
+// failed (*alloc_rc set when a device allocation failed).
+std::string prepare_factor_device(apxb_factor* f, uint32_t n, const uint32_t* colptr, const uint32_t* rowidx,
+                                  const float* vals, const uint32_t* perm, bool sddm, const uint64_t* rounds,
+                                  uint32_t n_rounds, double drop_rel, int* alloc_rc);
+// Host copies of a device-prepared factor's canonical arrays, levels and thin bits.
+std::string factor_host_arrays(apxb_factor* f);
+// One plan on the device: factor plan (col_lanes 0) or batch plan.
+struct dev_plan_out {
+    uint32_t n_items = 0, n_chunks = 0;
+    uint64_t n_entries = 0;
+    uint32_t *info = nullptr, *ord = nullptr, *ptr = nullptr, *idx = nullptr, *chunk = nullptr;
+    float* val = nullptr;
+};
+std::string batch_plan_device(const apxb_factor* f, int dir, uint32_t col_lanes,
+                              const std::function<std::string(void**, size_t)>& alloc_bytes, dev_plan_out& out,
+                              cudaStream_t s);
+// P A P^T into a->ptr / idx / val on the device; hptr receives the row offsets.
+std::string permute_operator_device(apxb_operator* a, uint32_t n, const int32_t* colptr, const int32_t* rowidx,
+                                    const double* vals, const uint32_t* perm, std::vector<int32_t>& hptr, int* alloc_rc);
+}  // namespace apxb

@@ -82,6 +82,8 @@ _SIGS = {
     "apxb_pcg": (ctypes.c_int, [c_p, c_p, c_p, c_p, c_p, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                 ctypes.POINTER(PcgResult)]),
     "apxb_test_stalled_sweep": (ctypes.c_int, [c_p, c_p, ctypes.c_uint64]),
+    "apxb_test_prep_compare": (ctypes.c_int, [c_p, ctypes.c_uint32, c_p, c_p, c_p, c_p, ctypes.c_int, c_p,
+                                              ctypes.c_uint32, ctypes.c_double, ctypes.c_int, c_p, c_p, c_p]),
     "apxb_batch_create": (ctypes.c_int, [c_p, ctypes.c_int, c_p, c_p, ctypes.c_int, ctypes.POINTER(c_p)]),
     "apxb_batch_plan_host": (ctypes.c_int, [ctypes.c_uint32, c_p, c_p, c_p, c_p, ctypes.c_int, c_p, ctypes.c_uint32,
                                             ctypes.c_double, ctypes.c_int, c_p, c_p]),

@@ -28,6 +28,9 @@ changes from one step to the next. The line reports:
                (continuous batching) at 70% of the measured capacity, tolerance
                drawn from {1e-6, 1e-8, 1e-10}: solves/s and p50/p99 latency
                from arrival to result.
+  * admission_ms  host time to make a new matrix solvable: factor
+               preparation (on the device), the permuted operator and a k-slot
+               batch with its plans.
   * serving_mix  the 8-matrix serving workload (serving_8 below) at 50, 200
                and 800 req/s: solves/s, p50/p99 and not-converged per rate,
                with two matrices admitted mid-stream under a 60 GB budget.
@@ -357,6 +360,17 @@ def run_ours(args, rank, world, local_rank):
     k, grid, nlanes = (int(v) for v in from_rank0([k, grid, nlanes], world, dev))   # every replica runs rank 0's choice
     D32.close()
     Op.close()
+    # admission: what a new matrix costs before its first solve -- the factor
+    # (prepared on the device), the permuted operator and a k-slot batch
+    torch.cuda.synchronize()
+    t_adm = time.perf_counter()
+    Da = native.DeviceFactor(eng, F, precision=native.PREC_FP32)
+    Oa = native.DeviceOperator(eng, A, F.perm)
+    Ba = native.Batch(eng, [Da], [Oa], k)
+    eng.sync()
+    admission_ms = (time.perf_counter() - t_adm) * 1e3
+    Ba.close(); Oa.close(); Da.close()
+    log(f"[bench] admission (factor + operator + k={k} batch): {admission_ms:.0f} ms")
     lanes = Lanes(A, F, k, lanes=nlanes, grid=grid, device=local_rank)
     grid = lanes.grid
     bt = lanes.lanes[0].batch
@@ -556,6 +570,7 @@ def run_ours(args, rank, world, local_rank):
         "speedup_vs_plain_fp64": (value / world) / plain["solves_s"] if plain and "solves_s" in plain else None,
         "serving": serving,
         "serving_mix": mix,
+        "admission_ms": admission_ms,
         "autotune": tuned,
         "gpu_launches": int(round(launches_per_step * args.steps)),
         "clocks": clk.summary(),

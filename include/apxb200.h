@@ -302,6 +302,21 @@ int apxb_batch_sweep_timed(apxb_batch* b, int reps, double* fwd_seconds, double*
  * not a hang. */
 int apxb_test_stalled_sweep(apxb_engine* e, apxb_factor* f, uint64_t budget_ns);
 
+/* ---- device preparation test hook ----
+ * apxb_factor_create prepares factors with round sizes and fp32 / fp64
+ * storage on the device (the reference does this work on the host:
+ * cuda.h:280-420, cuda_host.h:66-558). This hook prepares the given factor
+ * both ways and compares every array: CSC(L11) and CSR(L11) after the drop,
+ * levels, row sum modes, both directions' sweep plans, the batch plans for
+ * k right-hand sides (k > 0) and, when the operator is given (full symmetric
+ * CSC, int32), its permutation P A P^T (pcg_cuda.h:304-404). APXB_OK when
+ * all are identical (or both preparations reject the input with the same
+ * message); else APXB_ERR_INVALID naming the first array that differs. */
+int apxb_test_prep_compare(apxb_engine* e, uint32_t n, const uint32_t* colptr, const uint32_t* rowidx,
+                           const float* vals, const uint32_t* perm, int sddm, const uint64_t* rounds,
+                           uint32_t n_rounds, double drop_rel, int k, const int32_t* a_colptr,
+                           const int32_t* a_rowidx, const double* a_vals);
+
 #ifdef __cplusplus
 }
 #endif

@@ -99,3 +99,17 @@ def test_dropin_fp16_switch(tmp_path, env, want):
         e["APXCHOL_SPTRSV_FP16"] = env
     r = subprocess.run([exe], capture_output=True, text=True, env=e, check=True)
     assert r.stdout.strip() == want
+
+
+REFDROPIN = os.path.join(ROOT, "tests", "cpp", "refdropin", "_ref", "libapxdropin.so")
+
+
+@pytest.mark.skipif(not os.path.exists(REFDROPIN), reason="drop-in build of the reference absent")
+def test_reference_dropin_library_resolves_every_symbol():
+    """The reference's solve phase compiled against include/apxchol_compat
+    (tests/cpp/refdropin) loads with every symbol bound (no GPU needed):
+    nothing it calls is left undefined by the replacement headers."""
+    import ctypes
+    lib = ctypes.CDLL(REFDROPIN, mode=os.RTLD_NOW)
+    for name in ("dap_solve", "dap_solver_create", "dap_apply", "dap_solver_solve", "dap_trsv_info"):
+        assert hasattr(lib, name), name
