@@ -1,8 +1,8 @@
 """Autotuner of the batched mixed-precision form.
 
 For one matrix it times a whole batched solve (CUDA events, device-resident
-right-hand sides) for every right-hand-side block width k in {1, 2, 4, 8, 16}
-and every candidate sweep grid (the resident grid and one block per SM), and
+right-hand sides) for every right-hand-side block width k in
+{1, 2, 4, 8, 16, 32, 64} and every candidate sweep grid (the resident grid and one block per SM), and
 keeps the fastest solves/s. The sweeps' other knobs are fixed by the plan: the
 lanes per row follow the row length (1, 4, 8, 16 or 32), and the in-flight
 depth is the 3-stage item pipeline with 8 entries per lane, plus an L2
@@ -19,7 +19,8 @@ import numpy as np
 
 from . import native
 
-KS = (1, 2, 4, 8, 16)
+KS = (1, 2, 4, 8, 16, 32, 64)
+KS_INSTANCES = (1, 2, 4, 8, 16)   # many small instances with 1-8 right-hand sides each
 
 
 @dataclass
@@ -113,7 +114,8 @@ def tune_lanes(mat, fac, rhs, k: int, lanes_list=(2, 3, 4), tol: float = 1e-8, m
     return table
 
 
-def tune_instances(eng: native.Engine, factors, ops, rhs, tol: float = 1e-8, max_iter: int = 500, ks=KS, log=None):
+def tune_instances(eng: native.Engine, factors, ops, rhs, tol: float = 1e-8, max_iter: int = 500, ks=KS_INSTANCES,
+                   log=None):
     """Pick k for a multi-instance batch: rhs[i] is instance i's (c_i, n_i)
     right-hand sides. A width k solves them in ceil(max c_i / k) passes of one
     batch; every pass is timed (device events), and the k with the highest

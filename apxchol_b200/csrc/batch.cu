@@ -882,6 +882,12 @@ struct apxb_batch {
         if (dir == 0) { a.in = rhs32; a.out = Yf; a.reset = Zf; }
         else { a.in = Yf; a.out = Zf; a.reset = Yf; }
     }
+    // Markers into the forward output; the forward sweep re-arms the backward
+    // output's factor rows itself, and Zf's grounded rows stay 0.
+    void arm(cudaStream_t s) {
+        apxb::launch_fill_sent32(Yf, static_cast<size_t>(n_tot) * K, s);
+        y_armed = true;
+    }
     bp params(int max_iter) const {
         bp P{};
         P.K = K; P.S = S; P.n_tot = n_tot; P.n_tiles = n_tiles;
@@ -1001,7 +1007,9 @@ int launch_iteration(apxb_batch* bt, const bp& P, cudaStream_t s, unsigned long 
         case 2: return launch_iteration_k<2>(bt, P, s, h, use_cond);
         case 4: return launch_iteration_k<4>(bt, P, s, h, use_cond);
         case 8: return launch_iteration_k<8>(bt, P, s, h, use_cond);
-        default: return launch_iteration_k<16>(bt, P, s, h, use_cond);
+        case 16: return launch_iteration_k<16>(bt, P, s, h, use_cond);
+        case 32: return launch_iteration_k<32>(bt, P, s, h, use_cond);
+        default: return launch_iteration_k<64>(bt, P, s, h, use_cond);
     }
 }
 
@@ -1029,7 +1037,9 @@ void launch_finish(apxb_batch* bt, const bp& P, double* X, bool resid, cudaStrea
         case 2: launch_finish_k<2>(bt, P, X, resid, s); break;
         case 4: launch_finish_k<4>(bt, P, X, resid, s); break;
         case 8: launch_finish_k<8>(bt, P, X, resid, s); break;
-        default: launch_finish_k<16>(bt, P, X, resid, s); break;
+        case 16: launch_finish_k<16>(bt, P, X, resid, s); break;
+        case 32: launch_finish_k<32>(bt, P, X, resid, s); break;
+        default: launch_finish_k<64>(bt, P, X, resid, s); break;
     }
 }
 
@@ -1044,7 +1054,9 @@ void launch_admit(apxb_batch* bt, const bp& P, const double* B, cudaStream_t s) 
         case 2: launch_admit_k<2>(bt, P, B, s); break;
         case 4: launch_admit_k<4>(bt, P, B, s); break;
         case 8: launch_admit_k<8>(bt, P, B, s); break;
-        default: launch_admit_k<16>(bt, P, B, s); break;
+        case 16: launch_admit_k<16>(bt, P, B, s); break;
+        case 32: launch_admit_k<32>(bt, P, B, s); break;
+        default: launch_admit_k<64>(bt, P, B, s); break;
     }
 }
 
@@ -1117,7 +1129,9 @@ void slot_io(apxb_batch* bt, const bp& P, unsigned sl, const double* in, double*
         case 2: slot_io_k<2>(bt, P, sl, in, out, s); break;
         case 4: slot_io_k<4>(bt, P, sl, in, out, s); break;
         case 8: slot_io_k<8>(bt, P, sl, in, out, s); break;
-        default: slot_io_k<16>(bt, P, sl, in, out, s); break;
+        case 16: slot_io_k<16>(bt, P, sl, in, out, s); break;
+        case 32: slot_io_k<32>(bt, P, sl, in, out, s); break;
+        default: slot_io_k<64>(bt, P, sl, in, out, s); break;
     }
 }
 
@@ -1137,7 +1151,8 @@ int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, a
                       apxb_batch** out) {
     return guarded([&]() -> int {
         if (!e || n_inst < 1 || !factors || !ops || !out) return fail(APXB_ERR_INVALID, "bad argument");
-        if (k != 1 && k != 2 && k != 4 && k != 8 && k != 16) return fail(APXB_ERR_INVALID, "k must be 1, 2, 4, 8 or 16");
+        if (k != 1 && k != 2 && k != 4 && k != 8 && k != 16 && k != 32 && k != 64)
+            return fail(APXB_ERR_INVALID, "k must be 1, 2, 4, 8, 16, 32 or 64");
         *out = nullptr;
         APXB_CK(cudaSetDevice(e->device));
         std::unique_ptr<apxb_batch> bt(new (std::nothrow) apxb_batch);
@@ -1405,10 +1420,7 @@ int apxb_batch_solve(apxb_batch* bt, const double* B, double* X, const int* nrhs
         APXB_CK(cudaMemcpyAsync(P.fresh, ones.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, s));
         APXB_CK(cudaMemsetAsync(P.all_done, 0, sizeof(int), s));
         APXB_CK(cudaMemsetAsync(P.refresh_due, 0, sizeof(int), s));
-        // Only the forward output needs its markers now: the forward sweep re-arms
-        // every factor row of Zf itself, and Zf's grounded rows must stay 0.
-        if (!bt->y_armed) apxb::launch_fill_sent32(bt->Yf, nk, s);
-        bt->y_armed = true;
+        if (!bt->y_armed) bt->arm(s);
         APXB_CK(cudaEventRecord(e->ev0, s));
         launch_admit(bt, P, dB, s);
         if (no_graph()) {
@@ -1462,7 +1474,8 @@ int apxb_batch_plan_host(uint32_t n, const uint32_t* colptr, const uint32_t* row
                          int k, uint32_t* n_items, uint32_t* n_chunks) {
     return guarded([&]() -> int {
         if (!colptr || !rowidx || !vals || !perm || !n_items || !n_chunks) return fail(APXB_ERR_INVALID, "NULL argument");
-        if (k != 1 && k != 2 && k != 4 && k != 8 && k != 16) return fail(APXB_ERR_INVALID, "k must be 1, 2, 4, 8 or 16");
+        if (k != 1 && k != 2 && k != 4 && k != 8 && k != 16 && k != 32 && k != 64)
+            return fail(APXB_ERR_INVALID, "k must be 1, 2, 4, 8, 16, 32 or 64");
         apxb_factor f;
         const std::string why = apxb::prepare_factor(n, colptr, rowidx, vals, perm, sddm != 0, rounds, n_rounds,
                                                      drop_rel < 0.0 ? apxb::kDropRelDefault : drop_rel, f.h);
@@ -1547,7 +1560,7 @@ int apxb_batch_admit(apxb_batch* bt, int slot, const double* b, double tol, int 
         APXB_CK(cudaMemcpyAsync(st, b, 8 * static_cast<size_t>(bt->n[sl / bt->K]), cudaMemcpyHostToDevice, s));
         db = st;
     }
-    if (!bt->y_armed) { apxb::launch_fill_sent32(bt->Yf, static_cast<size_t>(bt->n_tot) * bt->K, s); bt->y_armed = true; }
+    if (!bt->y_armed) bt->arm(s);
     slot_io(bt, P, sl, db, nullptr, s);
     k_b_mark_admit<<<1, 32, 0, s>>>(P, sl, tol);
     APXB_CK(cudaGetLastError());
@@ -1659,7 +1672,7 @@ int apxb_batch_sweep_timed(apxb_batch* bt, int reps, double* fwd_seconds, double
     cudaStream_t s = e->stream;
     cudaEvent_t ev[3];
     for (auto& v : ev) APXB_CK(cudaEventCreate(&v));
-    if (!bt->y_armed) { apxb::launch_fill_sent32(bt->Yf, static_cast<size_t>(bt->n_tot) * bt->K, s); bt->y_armed = true; }
+    if (!bt->y_armed) bt->arm(s);
     apxb::sweep_args<float> a{};
     a.k = bt->K; a.err = e->d_err; a.budget_ns = e->budget_ns; a.skip = nullptr; a.m = bt->n_tot;
     double tf = 0.0, tb = 0.0;

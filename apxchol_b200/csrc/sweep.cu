@@ -646,7 +646,7 @@ template <int K>
 struct wide_cfg {
     static constexpr int KC = K < 4 ? K : 4;   // columns per lane
     static constexpr int C = K / KC;           // column lanes per row
-    static constexpr int LC = C == 4 ? 2 : (C == 2 ? 1 : 0);
+    static constexpr int LC = C == 16 ? 4 : (C == 8 ? 3 : (C == 4 ? 2 : (C == 2 ? 1 : 0)));
     static constexpr int B = 8;                // entries in flight per lane
 };
 
@@ -1055,7 +1055,9 @@ void launch_sweep32_batch(int dir, const sweep_args<float>& a, int grid, cudaStr
         case 2:  sweep32_batch_dir<2>(dir, a, grid, s); break;
         case 4:  sweep32_batch_dir<4>(dir, a, grid, s); break;
         case 8:  sweep32_batch_dir<8>(dir, a, grid, s); break;
-        default: sweep32_batch_dir<16>(dir, a, grid, s); break;
+        case 16: sweep32_batch_dir<16>(dir, a, grid, s); break;
+        case 32: sweep32_batch_dir<32>(dir, a, grid, s); break;
+        default: sweep32_batch_dir<64>(dir, a, grid, s); break;
     }
 }
 
@@ -1073,7 +1075,9 @@ int sweep_grid32_batch(int k, int num_sms) {
         case 2: b = occ32_batch<2>(); break;
         case 4: b = occ32_batch<4>(); break;
         case 8: b = occ32_batch<8>(); break;
-        default: b = occ32_batch<16>(); break;
+        case 16: b = occ32_batch<16>(); break;
+        case 32: b = occ32_batch<32>(); break;
+        default: b = occ32_batch<64>(); break;
     }
     return (b > 0 ? b : 1) * num_sms;
 }

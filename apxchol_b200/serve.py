@@ -96,10 +96,13 @@ class _Resident:
 
 
 def estimate_bytes(n: int, nnz_factor: int, nnz_a: int, k: int) -> int:
-    """Upper estimate of the device bytes of one resident matrix: the two
-    sweep plans (entries + 32-position items), the fp32 sweep vectors, the
-    permuted operator with its PCG vectors, and the batch's k-slot vectors."""
-    plan = 2 * (nnz_factor * 8 + n * 4 * 6)
+    """Upper estimate of the device bytes of one resident matrix: three pairs
+    of factor arrays -- the factor's two sweep plans (entries + 32-position
+    items), its canonical CSC / CSR (kept on the device for batch plans when
+    it was prepared there) and the batch's two plans -- the fp32 sweep
+    vectors, the permuted operator with its PCG vectors, and the batch's
+    k-slot vectors."""
+    plan = 6 * (nnz_factor * 8 + n * 4 * 6)
     operator = nnz_a * 12 + n * (4 + 8 * 7)
     batch = n * k * (8 * 5 + 4 * 3) + n * 8
     return int(1.25 * (plan + operator + batch)) + (4 << 20)
