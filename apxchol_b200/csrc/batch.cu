@@ -43,6 +43,7 @@ struct bp {
     const unsigned* inst_t0; const unsigned* inst_t1;
     const unsigned* inst_off; const unsigned* inst_n; const int* inst_lap;
     const int32_t* a_ptr; const int32_t* a_idx; const double* a_val;
+    const float* a_valf;       // non-null: the operator's values in fp32 (a_val unused)
     // long SpMV rows: long row i is lr_row[i], its chunks [lr_first[i], lr_first[i+1]);
     // chunk c covers entries [ch_lo[c], ch_hi[c]); its partial sums go to ch_part[c][K]
     const uint32_t* lr_row; const uint32_t* lr_first; const uint32_t* ch_lo; const uint32_t* ch_hi;
@@ -65,6 +66,8 @@ struct bp {
     int refresh_every;         // a slot's residual is recomputed as b - A x every this many of its iterations (0: never)
     int max_iter, stag, center_k;
     double* partials;          // [n_tiles][K][2]
+    double* sub_partials;      // [n_tiles][K/2][K]: p.Ap of every SpMV sub-tile (K >= 4)
+    unsigned* sub_count;       // [n_tiles]: sub-tiles of the tile summed so far (0 between launches)
     apxb::dev_error* err;
 };
 
@@ -136,6 +139,13 @@ __device__ __forceinline__ void col_store(double (&a)[NV][2], double* dst) {
         }                                                                                      \
     }
 
+// fp32-stored operator values widened into a combined fp64 array.
+__global__ void __launch_bounds__(kBT) k_b_widen(const float* src, double* dst, uint64_t n) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        dst[i] = static_cast<double>(src[i]);
+}
+
 // x = 0, r = b = P B (fresh slots only); B in the caller's layout: instance i,
 // column c, original local index v at B[K * off_i + c * n_i + v]. Columns
 // >= nrhs[i] are zero (their slots finish at once). Walks the original order
@@ -183,7 +193,7 @@ __global__ void __launch_bounds__(kBT) k_b_spmv(bp P, const double* X, double* Y
             }
 #pragma unroll 2
             for (int k = b0; k < e; ++k) {
-                const double w = __ldg(P.a_val + k);
+                const double w = apxb::op_val(P.a_val, P.a_valf, k);
                 const double* src = X + static_cast<size_t>(__ldg(P.a_idx + k)) * K;
                 if constexpr (K == 1) {
                     acc[0] = fma(w, src[0], acc[0]);
@@ -230,16 +240,32 @@ __global__ void __launch_bounds__(kBT) k_b_spmv(bp P, const double* X, double* Y
 // original order, the neighbours of the rows in flight lie in one window of
 // the mesh, and every operand row is reused while it is in L2. Each row's sum
 // is unchanged; only the rows that share a p.Ap tile partial differ.
+// That window is the rows all blocks have in flight at once. A tile is cut
+// into K/2 sub-tiles of 8 block passes (16 * kBT / K rows) and the blocks
+// stride over sub-tiles, so the window holds gridDim.x * 16 * kBT * 8 bytes of
+// operand rows whatever K is (19 MB at 592 blocks), well inside L2; a block per
+// tile would hold gridDim.x whole tiles (620 MB at K = 64). Each sub-tile
+// stores its p.Ap partial; the block that completes a tile's last sub-tile
+// (a per-tile counter) adds the tile's sub-partials in sub-tile order into the
+// tile partial and clears the counter, so the tile partial does not depend on
+// which blocks ran which sub-tiles.
 template <int K>
 __global__ void __launch_bounds__(kBT, 4) k_b_spmv_pairs(bp P, const double* X, double* Y, int mode) {
     if (*P.all_done && mode == 0) return;
     if (mode == 2 && !*P.refresh_due) return;   // the residual refresh's A x, only when due
     constexpr unsigned kRows = 2 * kBT / K;      // rows per pass of the block
+    constexpr unsigned kNS = K >= 4 ? K / 2 : 1; // sub-tiles per tile
+    constexpr unsigned kSubRows = kTile / kNS;   // 8 passes (kTile rows when K == 2)
     constexpr int kE = 4;                        // nonzeros whose gathers are in flight together
+    static_assert(kSubRows % kRows == 0, "a sub-tile is whole passes");
+    __shared__ int s_last;
     const unsigned c0 = (2 * threadIdx.x) % K, rsub = (2 * threadIdx.x) / K;
-    for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
+    for (unsigned u = blockIdx.x; u < P.n_tiles * kNS; u += gridDim.x) {
+        const unsigned t = u / kNS;
+        const unsigned lo = P.tile_lo[t] + (u % kNS) * kSubRows;
+        const unsigned hi = min(P.tile_hi[t], lo + kSubRows);
         double acc[1][2] = {{0.0, 0.0}};
-        for (unsigned g = P.tile_lo[t] + rsub; g < P.tile_hi[t]; g += kRows) {
+        for (unsigned g = lo + rsub; g < hi; g += kRows) {
             const unsigned row = __ldg(P.gperm + g);
             double a0 = 0.0, a1 = 0.0;
             double2 own = make_double2(0.0, 0.0);
@@ -264,7 +290,7 @@ __global__ void __launch_bounds__(kBT, 4) k_b_spmv_pairs(bp P, const double* X, 
                 double2 v[kE];
 #pragma unroll
                 for (int j = 0; j < kE; ++j)
-                    if (k0 + j < e) { col[j] = static_cast<unsigned>(__ldg(P.a_idx + k0 + j)); w[j] = __ldg(P.a_val + k0 + j); }
+                    if (k0 + j < e) { col[j] = static_cast<unsigned>(__ldg(P.a_idx + k0 + j)); w[j] = apxb::op_val(P.a_val, P.a_valf, k0 + j); }
 #pragma unroll
                 for (int j = 0; j < kE; ++j)
                     if (k0 + j < e) v[j] = *reinterpret_cast<const double2*>(X + static_cast<size_t>(col[j]) * K + c0);
@@ -283,7 +309,30 @@ __global__ void __launch_bounds__(kBT, 4) k_b_spmv_pairs(bp P, const double* X, 
                 acc[0][1] = fma(own.y, a1, acc[0][1]);
             }
         }
-        if (mode == 0) col_store<K, 1>(acc, P.partials + static_cast<size_t>(t) * K * 2);
+        if (mode != 0) continue;
+        if constexpr (kNS == 1) {
+            col_store<K, 1>(acc, P.partials + static_cast<size_t>(t) * K * 2);
+        } else {
+            col_store<K, 1>(acc, P.sub_partials + static_cast<size_t>(u) * K);
+            __threadfence();   // this block's sub-partial before its count
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                const unsigned before = atomicAdd(P.sub_count + t, 1u);
+                s_last = before == kNS - 1;
+                if (s_last) __threadfence();   // the other blocks' sub-partials before the reads below
+            }
+            __syncthreads();
+            if (s_last) {
+                if (threadIdx.x < static_cast<unsigned>(K)) {
+                    const double* src = P.sub_partials + static_cast<size_t>(t) * kNS * K + threadIdx.x;
+                    double sum = 0.0;
+#pragma unroll 8
+                    for (unsigned q = 0; q < kNS; ++q) sum += __ldcg(src + static_cast<size_t>(q) * K);
+                    P.partials[static_cast<size_t>(t) * K * 2 + threadIdx.x] = sum;
+                }
+                if (threadIdx.x == 0) P.sub_count[t] = 0u;
+            }
+        }
     }
 }
 
@@ -300,7 +349,7 @@ __global__ void __launch_bounds__(kBT) k_b_spmv_chunks(bp P, const double* X, in
         double a0 = 0.0, a1 = 0.0;
         if constexpr (K == 1) {
             for (uint32_t q = lo + threadIdx.x; q < hi; q += kBT)
-                a0 = fma(__ldg(P.a_val + q), X[__ldg(P.a_idx + q)], a0);
+                a0 = fma(apxb::op_val(P.a_val, P.a_valf, q), X[__ldg(P.a_idx + q)], a0);
             double v[1] = {a0};
             apxb::block_sum<1>(v, red);
             if (threadIdx.x == 0) P.ch_part[ch] = v[0];
@@ -308,7 +357,7 @@ __global__ void __launch_bounds__(kBT) k_b_spmv_chunks(bp P, const double* X, in
             constexpr unsigned kLanes = 2 * kBT / K;   // entry lanes
             const unsigned c0 = (2 * threadIdx.x) % K, el = (2 * threadIdx.x) / K;
             for (uint32_t q = lo + el; q < hi; q += kLanes) {
-                const double w = __ldg(P.a_val + q);
+                const double w = apxb::op_val(P.a_val, P.a_valf, q);
                 const double2 v = *reinterpret_cast<const double2*>(X + static_cast<size_t>(__ldg(P.a_idx + q)) * K + c0);
                 a0 = fma(w, v.x, a0);
                 a1 = fma(w, v.y, a1);
@@ -808,6 +857,7 @@ struct apxb_batch {
     // operator (combined, permuted) and permutation
     const int32_t *a_ptr = nullptr, *a_idx = nullptr;
     const double* a_val = nullptr;
+    const float* a_valf = nullptr;   // fp32 storage (every instance's operator fp32)
     // long SpMV rows (bp::lr_row ...)
     uint32_t n_long = 0, n_sp_chunks = 0;
     uint32_t *lr_row = nullptr, *lr_first = nullptr, *ch_lo = nullptr, *ch_hi = nullptr;
@@ -831,6 +881,8 @@ struct apxb_batch {
     int refresh_every = 25; // periodic fp64 residual refresh (bp::refresh_every)
     unsigned long long* applies = nullptr;
     double* partials = nullptr;
+    double* sub_partials = nullptr;   // SpMV sub-tile partials (bp::sub_partials)
+    unsigned* sub_count = nullptr;
     double* d_B = nullptr;  // staging of right-hand sides / solutions in the caller layout
     // graphs (max_iter is baked into them; tolerances are per slot on the device)
     cudaGraphExec_t loop = nullptr;
@@ -893,7 +945,7 @@ struct apxb_batch {
         P.K = K; P.S = S; P.n_tot = n_tot; P.n_tiles = n_tiles;
         P.tile_inst = tile_inst; P.tile_lo = tile_lo; P.tile_hi = tile_hi; P.inst_t0 = inst_t0; P.inst_t1 = inst_t1;
         P.inst_off = inst_off; P.inst_n = inst_n; P.inst_lap = inst_lap;
-        P.a_ptr = a_ptr; P.a_idx = a_idx; P.a_val = a_val; P.gperm = gperm; P.inst_of = inst_of;
+        P.a_ptr = a_ptr; P.a_idx = a_idx; P.a_val = a_val; P.a_valf = a_valf; P.gperm = gperm; P.inst_of = inst_of;
         P.lr_row = lr_row; P.lr_first = lr_first; P.ch_lo = ch_lo; P.ch_hi = ch_hi;
         P.n_long = n_long; P.n_sp_chunks = n_sp_chunks; P.ch_part = ch_part;
         P.x = x; P.r = r; P.p = p; P.Ap = Ap; P.b = b; P.rhs32 = rhs32; P.z = Zf;
@@ -909,7 +961,7 @@ struct apxb_batch {
         P.applies = applies;
         P.xa = xa; P.verify = verify;
         P.max_iter = max_iter; P.stag = 50; P.center_k = e->center_k;
-        P.partials = partials; P.err = e->d_err;
+        P.partials = partials; P.sub_partials = sub_partials; P.sub_count = sub_count; P.err = e->d_err;
         return P;
     }
 };
@@ -1236,11 +1288,17 @@ int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, a
         bt->grid32 = e->sweep_grid > 0 ? e->sweep_grid : apxb::sweep_grid32_batch(k, e->num_sms);
         // ---- operator ----
         if (n_inst == 1) {
-            bt->a_ptr = ops[0]->ptr; bt->a_idx = ops[0]->idx; bt->a_val = ops[0]->val;
+            bt->a_ptr = ops[0]->ptr; bt->a_idx = ops[0]->idx; bt->a_val = ops[0]->val; bt->a_valf = ops[0]->valf;
         } else {
+            // the combined values are fp32 when every instance stores fp32, else fp64
+            // (fp32-stored instances widened: the same values)
+            bool all32 = true;
+            for (int i = 0; i < n_inst; ++i) all32 = all32 && ops[i]->valf != nullptr;
             int32_t *ap, *ai;
-            double* av;
-            if ((rc = bt->dalloc(&ap, bt->n_tot + 1)) || (rc = bt->dalloc(&ai, nnz_a)) || (rc = bt->dalloc(&av, nnz_a)))
+            double* av = nullptr;
+            float* avf = nullptr;
+            if ((rc = bt->dalloc(&ap, bt->n_tot + 1)) || (rc = bt->dalloc(&ai, nnz_a)) ||
+                (rc = all32 ? bt->dalloc(&avf, nnz_a) : bt->dalloc(&av, nnz_a)))
                 return rc;
             std::vector<int32_t> hp(bt->n_tot + 1, 0);
             uint64_t base = 0;
@@ -1252,11 +1310,19 @@ int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, a
                 for (uint32_t r = 0; r <= a->n; ++r) hp[bt->off[i] + r] = static_cast<int32_t>(base + p[r]);
                 for (auto& c : ix) c += static_cast<int32_t>(bt->off[i]);
                 APXB_CK(cudaMemcpy(ai + base, ix.data(), 4 * a->nnz, cudaMemcpyHostToDevice));
-                APXB_CK(cudaMemcpy(av + base, a->val, 8 * a->nnz, cudaMemcpyDeviceToDevice));
+                if (all32) {
+                    APXB_CK(cudaMemcpy(avf + base, a->valf, 4 * a->nnz, cudaMemcpyDeviceToDevice));
+                } else if (a->valf) {
+                    k_b_widen<<<e->vec_grid, kBT, 0, s>>>(a->valf, av + base, a->nnz);
+                    APXB_CK(cudaGetLastError());
+                    APXB_CK(cudaStreamSynchronize(s));
+                } else {
+                    APXB_CK(cudaMemcpy(av + base, a->val, 8 * a->nnz, cudaMemcpyDeviceToDevice));
+                }
                 base += a->nnz;
             }
             APXB_CK(cudaMemcpy(ap, hp.data(), 4 * hp.size(), cudaMemcpyHostToDevice));
-            bt->a_ptr = ap; bt->a_idx = ai; bt->a_val = av;
+            bt->a_ptr = ap; bt->a_idx = ai; bt->a_val = av; bt->a_valf = avf;
         }
         // ---- long SpMV rows ----
         {
@@ -1324,8 +1390,11 @@ int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, a
             (rc = bt->dalloc(&bt->Yf, nk)) || (rc = bt->dalloc(&bt->Zf, nk)) || (rc = bt->dalloc(&bt->sd, kSd * ns)) ||
             (rc = bt->dalloc(&bt->si, 6 * ns + 3)) || (rc = bt->dalloc(&bt->applies, ns)) ||
             (rc = bt->dalloc(&bt->xa, ns)) || (rc = bt->dalloc(&bt->verify, ns)) ||
-            (rc = bt->dalloc(&bt->partials, static_cast<size_t>(bt->n_tiles) * k * 2)) || (rc = bt->dalloc(&bt->d_B, nk)))
+            (rc = bt->dalloc(&bt->partials, static_cast<size_t>(bt->n_tiles) * k * 2)) || (rc = bt->dalloc(&bt->d_B, nk)) ||
+            (rc = bt->dalloc(&bt->sub_partials, static_cast<size_t>(bt->n_tiles) * std::max(1, k / 2) * k)) ||
+            (rc = bt->dalloc(&bt->sub_count, bt->n_tiles)))
             return rc;
+        APXB_CK(cudaMemsetAsync(bt->sub_count, 0, sizeof(unsigned) * bt->n_tiles, s));
         APXB_CK(cudaMallocHost(&bt->h_sd, sizeof(double) * kSd * ns));
         APXB_CK(cudaMallocHost(&bt->h_si, sizeof(int) * (6 * ns + 1)));
         std::fill(bt->h_sd, bt->h_sd + kSd * ns, 0.0);

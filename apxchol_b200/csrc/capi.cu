@@ -678,6 +678,15 @@ int apxb_operator_create(apxb_engine* e, uint32_t n, const int32_t* colptr, cons
             if (arc) return arc;
             if (!why.empty()) return fail(APXB_ERR_INVALID, why);
         }
+        {   // storage precision: fp32 iff every value is fp32-exact; APXCHOL_GPU_FP32_OPERATOR overrides
+            // ("0": fp64, any other value: fp32), the reference's rule (pcg_cuda.h:100-111)
+            const char* ev = std::getenv("APXCHOL_GPU_FP32_OPERATOR");
+            const int want = ev && std::string(ev) == "0" ? 0 : (ev && *ev ? 1 : -1);
+            int arc = 0;
+            const std::string why = apxb::operator_precision_device(a.get(), want, &arc);
+            if (arc) return arc;
+            if (!why.empty()) return fail(APXB_ERR_CUDA, why);
+        }
         if ((rc = a->dalloc(&a->perm, n)) || (rc = a->dalloc(&a->x, n)) || (rc = a->dalloc(&a->r, n)) ||
             (rc = a->dalloc(&a->p, n)) || (rc = a->dalloc(&a->Ap, n)) || (rc = a->dalloc(&a->b_orig, n)) ||
             (rc = a->dalloc(&a->x_orig, n)) || (rc = a->dalloc(&a->st, 1)))
@@ -727,6 +736,12 @@ int apxb_operator_destroy(apxb_operator* a) {
     return APXB_OK;
 }
 
+int apxb_operator_fp32(const apxb_operator* a, int* fp32) {
+    if (!a || !fp32) return fail(APXB_ERR_INVALID, "bad argument");
+    *fp32 = a->valf != nullptr ? 1 : 0;
+    return APXB_OK;
+}
+
 }  // extern "C"
 
 namespace apxb {
@@ -748,7 +763,7 @@ int apxb_operator_matvec(apxb_engine* e, apxb_operator* a, const double* x, doub
     std::memcpy(e->h_stage_a, x, 8 * n);
     APXB_CK(cudaMemcpyAsync(e->d_stage_a, e->h_stage_a, 8 * n, cudaMemcpyHostToDevice, s));
     apxb::launch_perm_in(a->perm, e->d_stage_a, a->Ap, a->n, e->vec_grid, s);
-    apxb::launch_spmv_plain(a->ptr, a->idx, a->val, a->Ap, a->r, a->n, e->vec_grid, s);
+    apxb::launch_spmv_plain(a->ptr, a->idx, a->val, a->valf, a->Ap, a->r, a->n, e->vec_grid, s);
     apxb::launch_perm_out(a->perm, a->r, e->d_stage_b, a->n, e->vec_grid, s);
     APXB_CK(cudaMemcpyAsync(e->h_stage_b, e->d_stage_b, 8 * n, cudaMemcpyDeviceToHost, s));
     APXB_CK(cudaStreamSynchronize(s));
@@ -764,7 +779,7 @@ namespace {
 
 apxb::pcg_ptrs pcg_ptrs_of(apxb_operator* a, apxb_factor* f) {
     apxb::pcg_ptrs p{};
-    p.a_ptr = a->ptr; p.a_idx = a->idx; p.a_val = a->val; p.perm = a->perm;
+    p.a_ptr = a->ptr; p.a_idx = a->idx; p.a_val = a->val; p.a_valf = a->valf; p.perm = a->perm;
     p.x = a->x; p.r = a->r; p.p = a->p; p.Ap = a->Ap; p.z = f->Z;
     p.b_orig = a->b_orig; p.x_orig = a->x_orig;
     p.st = a->st; p.err = a->e->d_err; p.partials = a->e->d_partials; p.counters = a->e->d_counters;
@@ -938,7 +953,7 @@ int apxb_pcg(apxb_engine* e, apxb_factor* f, apxb_operator* a, const double* b, 
     res->true_residual = -1.0;
     if (want_true_residual) {
         // ||b - A x|| / ||b|| in fp64 on the device, from the permuted x.
-        apxb::launch_spmv_plain(a->ptr, a->idx, a->val, a->x, a->Ap, a->n, e->vec_grid, s);
+        apxb::launch_spmv_plain(a->ptr, a->idx, a->val, a->valf, a->x, a->Ap, a->n, e->vec_grid, s);
         apxb::launch_resid(a->perm, a->b_orig, a->Ap, e->d_scal, e->d_partials, e->d_counters + 8, a->n,
                            e->vec_grid, s);
         APXB_CK(cudaMemcpyAsync(e->h_scal, e->d_scal, sizeof(double) * 8, cudaMemcpyDeviceToHost, s));

@@ -484,6 +484,24 @@ __global__ void __launch_bounds__(kPT) k_op_scatter(uint32_t n, const int32_t* c
     }
 }
 
+// Clears *exact unless every value round-trips fp32: v == double(float(v))
+// (the reference's fp32_exact test, pcg_cuda.h:298-380).
+__global__ void __launch_bounds__(kPT) k_fp32_exact(const double* v, size_t n, uint32_t* inexact) {
+    bool bad = false;
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const double x = v[i];
+        if (static_cast<double>(__double2float_rn(x)) != x) bad = true;
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31u) == 0) atomicOr(inexact, 1u);
+}
+
+__global__ void __launch_bounds__(kPT) k_narrow(const double* v, float* f, size_t n) {
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x)
+        f[i] = __double2float_rn(v[i]);
+}
+
 }  // namespace
 
 // ================================================================ host side
@@ -885,6 +903,34 @@ std::string permute_operator_device(apxb_operator* a, uint32_t n, const int32_t*
     DP_CK(cudaStreamSynchronize(s));
     if (bad == 3u) return "operator row index out of range";
     a->nnz = static_cast<uint64_t>(nnz);
+    return {};
+}
+
+std::string operator_precision_device(apxb_operator* a, int want, int* alloc_rc) {
+    cudaStream_t s = a->e->stream;
+    const size_t nnz = a->nnz;
+    bool fp32 = want > 0;
+    if (want < 0 && nnz > 0) {
+        dbuf flag;
+        DP_CK(flag.alloc(4, s));
+        DP_CK(cudaMemsetAsync(flag.p, 0, 4, s));
+        k_fp32_exact<<<grid_for(nnz), kPT, 0, s>>>(a->val, nnz, flag.get<uint32_t>());
+        uint32_t inexact = 1;
+        DP_CK(cudaMemcpyAsync(&inexact, flag.p, 4, cudaMemcpyDeviceToHost, s));
+        DP_CK(cudaStreamSynchronize(s));
+        fp32 = inexact == 0;
+    }
+    if (!fp32 || nnz == 0) return {};
+    const int rc = a->dalloc(&a->valf, nnz);
+    if (rc) {
+        *alloc_rc = rc;
+        return std::string(apxb_last_error());
+    }
+    k_narrow<<<grid_for(nnz), kPT, 0, s>>>(a->val, a->valf, nnz);
+    DP_CK(cudaGetLastError());
+    DP_CK(cudaStreamSynchronize(s));
+    a->drop(a->val);
+    a->val = nullptr;
     return {};
 }
 

@@ -90,6 +90,12 @@ struct pcg_state {
     unsigned n, m;
 };
 
+// An operator value: the fp32 copy when the operator is stored in fp32 (every
+// value fp32-exact, so the widened value is the fp64 one), else the fp64 array.
+__device__ __forceinline__ double op_val(const double* val, const float* valf, int64_t k) {
+    return valf ? static_cast<double>(__ldg(valf + k)) : __ldg(val + k);
+}
+
 struct reduce_ws {
     double* partials;   // [grid * 4]
     unsigned* counter;  // one per reduction site
@@ -98,6 +104,7 @@ struct reduce_ws {
 struct pcg_ptrs {
     // operator (permuted ordering)
     const int32_t* a_ptr; const int32_t* a_idx; const double* a_val;
+    const float* a_valf;   // non-null: values stored in fp32 (a_val unused)
     const uint32_t* perm;
     // vectors, permuted ordering
     double* x; double* r; double* p; double* Ap; const double* z;
@@ -146,8 +153,9 @@ void launch_apply_permute(const apply_ptrs& a, cudaStream_t s);   // zp[perm[v]]
 void launch_apply_zsum(const apply_ptrs& a, cudaStream_t s);      // scal[1] = sum(zsol)/n if center
 void launch_apply_gather(const apply_ptrs& a, cudaStream_t s);    // z[v] = zsol[perm[v]] - scal[1]; scal[2] = b.z
 
-// y = A x over the permuted operator with permute / unpermute (residual checks).
-void launch_spmv_plain(const int32_t* ptr, const int32_t* idx, const double* val, const double* x, double* y,
-                       unsigned n, int grid, cudaStream_t s);
+// y = A x over the permuted operator with permute / unpermute (residual checks);
+// values from valf when it is given (fp32 storage), else from val.
+void launch_spmv_plain(const int32_t* ptr, const int32_t* idx, const double* val, const float* valf, const double* x,
+                       double* y, unsigned n, int grid, cudaStream_t s);
 
 }  // namespace apxb

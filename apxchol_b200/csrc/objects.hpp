@@ -194,7 +194,8 @@ struct apxb_operator {
     uint64_t nnz = 0;
     std::vector<std::pair<void*, size_t>> owned;
     int32_t *ptr = nullptr, *idx = nullptr;
-    double* val = nullptr;
+    double* val = nullptr;    // fp64 values (null once narrowed into valf)
+    float* valf = nullptr;    // fp32 values when every value is fp32-exact (or forced)
     uint32_t* perm = nullptr;
     // SpMV rows longer than apxb::kLongRowPlain (see pcg_ptrs)
     uint32_t n_long = 0, n_chunks = 0;
@@ -216,6 +217,15 @@ struct apxb_operator {
         if (rc) return rc;
         owned.emplace_back(*q, bytes);
         return APXB_OK;
+    }
+    // Releases one buffer this operator allocated (no-op for any other pointer).
+    void drop(void* q) {
+        for (size_t i = 0; i < owned.size(); ++i)
+            if (owned[i].first == q) {
+                e->release(q, owned[i].second);
+                owned.erase(owned.begin() + static_cast<std::ptrdiff_t>(i));
+                return;
+            }
     }
     ~apxb_operator() {
         if (loop) cudaGraphExecDestroy(loop);
@@ -276,4 +286,8 @@ std::string batch_plan_device(const apxb_factor* f, int dir, uint32_t col_lanes,
 // P A P^T into a->ptr / idx / val on the device; hptr receives the row offsets.
 std::string permute_operator_device(apxb_operator* a, uint32_t n, const int32_t* colptr, const int32_t* rowidx,
                                     const double* vals, const uint32_t* perm, std::vector<int32_t>& hptr, int* alloc_rc);
+// Storage precision of a's values: want > 0 stores them in fp32, want == 0 keeps
+// fp64, want < 0 stores fp32 when every value is fp32-exact. fp32 storage
+// narrows a->val into a->valf and releases a->val.
+std::string operator_precision_device(apxb_operator* a, int want, int* alloc_rc);
 }  // namespace apxb

@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg_spmv(pcg_ptrs p) {
             is_long = static_cast<uint32_t>(e - b) > kLongRowPlain;   // summed by the chunk kernels
             if (!is_long)
                 for (int k = b + static_cast<int>(lane); k < e; k += G)
-                    s = fma(__ldg(p.a_val + k), p.p[__ldg(p.a_idx + k)], s);
+                    s = fma(op_val(p.a_val, p.a_valf, k), p.p[__ldg(p.a_idx + k)], s);
         }
 #pragma unroll
         for (int o = G / 2; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o, G);
@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg_spmv_rows(pcg_ptrs p) {
             double w[kE], x[kE];
 #pragma unroll
             for (int j = 0; j < kE; ++j)
-                if (k0 + j < e) { col[j] = __ldg(p.a_idx + k0 + j); w[j] = __ldg(p.a_val + k0 + j); }
+                if (k0 + j < e) { col[j] = __ldg(p.a_idx + k0 + j); w[j] = op_val(p.a_val, p.a_valf, k0 + j); }
 #pragma unroll
             for (int j = 0; j < kE; ++j)
                 if (k0 + j < e) x[j] = p.p[col[j]];
@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(kThreads) k_apply_gather(apply_ptrs a) {
 }
 
 __global__ void __launch_bounds__(kThreads) k_spmv_plain(const int32_t* ptr, const int32_t* idx, const double* val,
-                                                         const double* x, double* y, unsigned n) {
+                                                         const float* valf, const double* x, double* y, unsigned n) {
     constexpr int G = 8;
     constexpr unsigned kRowsPerWarp = 32 / G;
     const unsigned lane = threadIdx.x & (G - 1);
@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(kThreads) k_spmv_plain(const int32_t* ptr, con
         double s = 0.0;
         if (row < n) {
             const int b = ptr[row], e = ptr[row + 1];
-            for (int k = b + static_cast<int>(lane); k < e; k += G) s = fma(val[k], x[idx[k]], s);
+            for (int k = b + static_cast<int>(lane); k < e; k += G) s = fma(op_val(val, valf, k), x[idx[k]], s);
         }
 #pragma unroll
         for (int o = G / 2; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o, G);
@@ -331,7 +331,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg_spmv_chunks(pcg_ptrs p) {
     for (unsigned ch = blockIdx.x; ch < p.n_chunks; ch += gridDim.x) {
         double a = 0.0;
         for (uint32_t q = p.ch_lo[ch] + threadIdx.x; q < p.ch_hi[ch]; q += blockDim.x)
-            a = fma(__ldg(p.a_val + q), p.p[__ldg(p.a_idx + q)], a);
+            a = fma(op_val(p.a_val, p.a_valf, q), p.p[__ldg(p.a_idx + q)], a);
         double v[1] = {a};
         block_sum<1>(v, red);
         if (threadIdx.x == 0) p.ch_part[ch] = v[0];
@@ -368,9 +368,9 @@ void launch_apply_permute(const apply_ptrs& a, cudaStream_t s) { k_apply_permute
 void launch_apply_zsum(const apply_ptrs& a, cudaStream_t s) { k_apply_zsum<<<a.grid, kThreads, 0, s>>>(a); }
 void launch_apply_gather(const apply_ptrs& a, cudaStream_t s) { k_apply_gather<<<a.grid, kThreads, 0, s>>>(a); }
 
-void launch_spmv_plain(const int32_t* ptr, const int32_t* idx, const double* val, const double* x, double* y,
-                       unsigned n, int grid, cudaStream_t s) {
-    k_spmv_plain<<<grid, kThreads, 0, s>>>(ptr, idx, val, x, y, n);
+void launch_spmv_plain(const int32_t* ptr, const int32_t* idx, const double* val, const float* valf, const double* x,
+                       double* y, unsigned n, int grid, cudaStream_t s) {
+    k_spmv_plain<<<grid, kThreads, 0, s>>>(ptr, idx, val, valf, x, y, n);
 }
 
 }  // namespace apxb

@@ -78,6 +78,7 @@ _SIGS = {
     "apxb_apply": (ctypes.c_int, [c_p, c_p, c_p, c_p, ctypes.c_int, c_p]),
     "apxb_operator_create": (ctypes.c_int, [c_p, ctypes.c_uint32, c_p, c_p, c_p, c_p, ctypes.POINTER(c_p)]),
     "apxb_operator_destroy": (ctypes.c_int, [c_p]),
+    "apxb_operator_fp32": (ctypes.c_int, [c_p, ctypes.POINTER(ctypes.c_int)]),
     "apxb_operator_matvec": (ctypes.c_int, [c_p, c_p, c_p, c_p]),
     "apxb_pcg": (ctypes.c_int, [c_p, c_p, c_p, c_p, c_p, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                 ctypes.POINTER(PcgResult)]),
@@ -276,6 +277,14 @@ class DeviceOperator:
             self.h = None
 
     __del__ = close
+
+    @property
+    def fp32(self) -> bool:
+        """Whether the values are stored in fp32 (all fp32-exact, or forced by
+        APXCHOL_GPU_FP32_OPERATOR at creation)."""
+        v = ctypes.c_int()
+        check(self.lib.apxb_operator_fp32(self.h, ctypes.byref(v)))
+        return bool(v.value)
 
     def matvec(self, x: np.ndarray) -> np.ndarray:
         x = np.ascontiguousarray(x, np.float64)

@@ -101,10 +101,11 @@ def estimate_bytes(n: int, nnz_factor: int, nnz_a: int, k: int) -> int:
     items), its canonical CSC / CSR (kept on the device for batch plans when
     it was prepared there) and the batch's two plans -- the fp32 sweep
     vectors, the permuted operator with its PCG vectors, and the batch's
-    k-slot vectors."""
+    k-slot vectors (six fp64, three fp32) with its SpMV sub-tile partials
+    (k * k / 2 doubles per 2048 rows)."""
     plan = 6 * (nnz_factor * 8 + n * 4 * 6)
     operator = nnz_a * 12 + n * (4 + 8 * 7)
-    batch = n * k * (8 * 5 + 4 * 3) + n * 8
+    batch = n * k * (8 * 6 + 4 * 3) + n * 8 + (n // 2048 + 1) * max(1, k // 2) * k * 8
     return int(1.25 * (plan + operator + batch)) + (4 << 20)
 
 

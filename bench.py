@@ -25,12 +25,14 @@ changes from one step to the next. The line reports:
   * plain_fp64 the plain single-RHS fp64 path (apxb_pcg; sweeps reproducing
                the reference's arithmetic), its solves/s and the speed-up.
   * serving    an open-loop Poisson request stream through SolveServer
-               (continuous batching) at 70% of the measured capacity, tolerance
-               drawn from {1e-6, 1e-8, 1e-10}: solves/s and p50/p99 latency
-               from arrival to result.
+               (continuous batching; 16 slots per lane unless --serve-k) at 70%
+               of the server's own saturation throughput, measured first,
+               tolerance drawn from {1e-6, 1e-8, 1e-10}: solves/s and p50/p99
+               latency from arrival to result.
   * admission_ms  host time to make a new matrix solvable: factor
                preparation (on the device), the permuted operator and a k-slot
-               batch with its plans.
+               batch with its plans; the median of three admissions (the
+               "admission" field holds the samples and their breakdown).
   * serving_mix  the 8-matrix serving workload (serving_8 below) at 50, 200
                and 800 req/s: solves/s, p50/p99 and not-converged per rate,
                with two matrices admitted mid-stream under a 60 GB budget.
@@ -288,8 +290,10 @@ def run_reference(args, rank, world):
     return 0
 
 
-def serving_run(A, F, k, nlanes, grid, iters_per_step, rate, n_req, seed, log_fn):
-    """Open-loop Poisson requests through SolveServer; returns its summary."""
+def serving_run(A, F, k, nlanes, grid, iters_per_step, load, n_req, seed, log_fn):
+    """Open-loop Poisson requests through SolveServer at `load` times the
+    server's own saturation throughput (measured first: 2 k lanes requests
+    submitted at once, drained); returns its summary."""
     from apxchol_b200 import gen
     from apxchol_b200.serve import SolveServer, latency_stats
     srv = SolveServer(k=k, iters_per_step=iters_per_step, lanes=nlanes, sweep_grid=grid)
@@ -301,6 +305,13 @@ def serving_run(A, F, k, nlanes, grid, iters_per_step, rate, n_req, seed, log_fn
             srv.submit("g", pool[j % 8], TOL)
         srv.drain()
         srv.completed.clear()
+        t0 = time.perf_counter()
+        for j in range(2 * k * nlanes):          # saturation throughput
+            srv.submit("g", pool[j % 8], TOL)
+        srv.drain()
+        capacity = 2 * k * nlanes / (time.perf_counter() - t0)
+        srv.completed.clear()
+        rate = load * capacity
         rng = np.random.default_rng(seed)
         t = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
         tols = (1e-6, 1e-8, 1e-10)
@@ -315,7 +326,8 @@ def serving_run(A, F, k, nlanes, grid, iters_per_step, rate, n_req, seed, log_fn
         for q in done[:: max(1, len(done) // 16)]:
             worst = max(worst, float(np.linalg.norm(q.b - A.matvec(q.x)) / np.linalg.norm(q.b)) / q.tol)
         out = {"rate_req_s": rate, "requests": len(done), "solves_s": len(done) / wall, "p50_ms": st["p50_ms"],
-               "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "k": k, "iters_per_step": iters_per_step,
+               "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "capacity_solves_s": capacity, "load": load,
+               "k": k, "iters_per_step": iters_per_step,
                "lanes": nlanes, "not_converged": bad, "max_true_relres_over_tol": worst}
         log_fn(f"[bench] serving {rate:.0f} req/s: {out['solves_s']:.1f} solves/s, p50 {st['p50_ms']:.1f} ms, "
                f"p99 {st['p99_ms']:.1f} ms, {bad} not converged, worst fp64 relres/tol {worst:.2f}")
@@ -361,20 +373,30 @@ def run_ours(args, rank, world, local_rank):
     D32.close()
     Op.close()
     # admission: what a new matrix costs before its first solve -- the factor
-    # (prepared on the device), the permuted operator and a k-slot batch
-    torch.cuda.synchronize()
-    t_adm = time.perf_counter()
-    Da = native.DeviceFactor(eng, F, precision=native.PREC_FP32)
-    t_f = time.perf_counter()
-    Oa = native.DeviceOperator(eng, A, F.perm)
-    t_o = time.perf_counter()
-    Ba = native.Batch(eng, [Da], [Oa], k)
-    eng.sync()
-    t_b = time.perf_counter()
-    admission_ms = (t_b - t_adm) * 1e3
-    Ba.close(); Oa.close(); Da.close()
-    log(f"[bench] admission (factor + operator + k={k} batch): {admission_ms:.0f} ms "
-        f"({(t_f - t_adm) * 1e3:.0f} + {(t_o - t_f) * 1e3:.0f} + {(t_b - t_o) * 1e3:.0f})")
+    # (prepared on the device), the permuted operator and a k-slot batch. Three
+    # admissions, the median reported; objects left by the tuning are collected
+    # first, so that no destructor's device free lands inside a timed admission.
+    import gc
+    gc.collect()
+    adm = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t_adm = time.perf_counter()
+        Da = native.DeviceFactor(eng, F, precision=native.PREC_FP32)
+        t_f = time.perf_counter()
+        Oa = native.DeviceOperator(eng, A, F.perm)
+        t_o = time.perf_counter()
+        Ba = native.Batch(eng, [Da], [Oa], k)
+        eng.sync()
+        t_b = time.perf_counter()
+        Ba.close(); Oa.close(); Da.close()
+        adm.append([(t_b - t_adm) * 1e3, (t_f - t_adm) * 1e3, (t_o - t_f) * 1e3, (t_b - t_o) * 1e3])
+    admission_ms = float(np.median([a[0] for a in adm]))
+    admission = {"median_ms": admission_ms, "samples_ms": [round(a[0], 1) for a in adm],
+                 "factor_ms": [round(a[1], 1) for a in adm], "operator_ms": [round(a[2], 1) for a in adm],
+                 "batch_ms": [round(a[3], 1) for a in adm], "k": k}
+    log(f"[bench] admission (factor + operator + k={k} batch), 3 times: " +
+        ", ".join(f"{a[0]:.0f} ms ({a[1]:.0f} + {a[2]:.0f} + {a[3]:.0f})" for a in adm))
     lanes = Lanes(A, F, k, lanes=nlanes, grid=grid, device=local_rank)
     grid = lanes.grid
     bt = lanes.lanes[0].batch
@@ -539,7 +561,8 @@ def run_ours(args, rank, world, local_rank):
     serving = None
     if not args.no_serving and rank == 0:
         try:
-            serving = serving_run(A, F, k, nlanes, grid, args.iters_per_step, 0.7 * value / world,
+            sk = min(k, args.serve_k)
+            serving = serving_run(A, F, sk, nlanes, grid, args.iters_per_step, args.serve_load,
                                   args.serve_requests, 11, log)
         except Exception as ex:   # reported in its field; the headline stands
             serving = {"error": f"{type(ex).__name__}: {ex}"}
@@ -575,6 +598,7 @@ def run_ours(args, rank, world, local_rank):
         "serving": serving,
         "serving_mix": mix,
         "admission_ms": admission_ms,
+        "admission": admission,
         "autotune": tuned,
         "gpu_launches": int(round(launches_per_step * args.steps)),
         "clocks": clk.summary(),
@@ -799,6 +823,10 @@ def main():
     ap.add_argument("--lanes", type=int, default=1, help="concurrent batches (streams) with --k")
     ap.add_argument("--iters-per-step", type=int, default=2, help="serving: iterations per server step")
     ap.add_argument("--serve-requests", type=int, default=1000)
+    ap.add_argument("--serve-k", type=int, default=16,
+                    help="serving: slots per lane (at most the batch k; fewer slots, shorter iterations, lower latency)")
+    ap.add_argument("--serve-load", type=float, default=0.7,
+                    help="serving: Poisson rate as a fraction of the server's measured saturation throughput")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-serving-mix", action="store_true", help="skip the 8-matrix serving field")
     ap.add_argument("--no-plain", action="store_true")

@@ -202,10 +202,18 @@ int apxb_sweep_pair_multi(apxb_engine* e, apxb_factor* f, int k, const double* d
 int apxb_apply(apxb_engine* e, apxb_factor* f, const double* b, double* z, int flags, double* rz_out);
 
 /* ---- operator: A in the factor's permuted ordering (cuda_pcg::setup, pcg_cuda.h:68-152) ----
- * colptr[n+1], rowidx[nnz], vals[nnz]: full symmetric CSC (int32, rows ascending). */
+ * colptr[n+1], rowidx[nnz], vals[nnz]: full symmetric CSC (int32, rows ascending).
+ * Values are stored in fp32 when every one round-trips fp32 (v == (double)(float)v),
+ * else in fp64 (the reference's rule, pcg_cuda.h:100-111); the SpMV widens each
+ * value to fp64, so an fp32-stored exact operator gives the same results. The
+ * environment variable APXCHOL_GPU_FP32_OPERATOR, read at creation, overrides:
+ * "0" keeps fp64, any other non-empty value forces fp32 (values rounded). */
 int apxb_operator_create(apxb_engine* e, uint32_t n, const int32_t* colptr, const int32_t* rowidx,
                          const double* vals, const uint32_t* perm, apxb_operator** out);
 int apxb_operator_destroy(apxb_operator* a);
+/* *fp32 = 1 when the operator's values are stored in fp32, else 0
+ * (cuda_pcg::fp32_operator, pcg_cuda.h:267). */
+int apxb_operator_fp32(const apxb_operator* a, int* fp32);
 /* y = A x in the original ordering (host pointers), for residual checks. */
 int apxb_operator_matvec(apxb_engine* e, apxb_operator* a, const double* x, double* y);
 

@@ -68,8 +68,11 @@ public:
     bool ready() const { return a_ != nullptr; }
     int64_t n() const { return n_; }
     int64_t nnz() const { return nnz_; }
-    // The operator is stored in fp64 (fp32-exact values are not narrowed).
-    bool fp32_operator() const { return false; }
+    // The operator's values are stored in fp32 when every one is fp32-exact.
+    bool fp32_operator() const {
+        int v = 0;
+        return a_ && apxb_operator_fp32(a_, &v) == APXB_OK && v != 0;
+    }
     // Threads per row of the plain SpMV: the library picks them per row from
     // the average row length, so no single count applies; 1 is reported.
     int spmv_lanes() const { return 1; }

@@ -81,3 +81,46 @@ def test_pcg_edge_cases(eng):
     # and the engine keeps working
     x, r = native.pcg(eng, D, Op, b, tol=TOL, max_iter=500)
     assert r.status == 0
+
+
+def test_fp32_exact_operator_is_stored_in_fp32(eng, monkeypatch):
+    """An operator whose values are all fp32-exact is stored in fp32 (the
+    reference's rule, pcg_cuda.h:100-111) and solves to the same bits as the
+    same operator stored in fp64 (APXCHOL_GPU_FP32_OPERATOR=0): the SpMV widens
+    every value to fp64 either way. Plain PCG, and batches of one instance, of
+    two fp32 instances and of a mixed pair (combined operator widened)."""
+    from apxchol_b200 import refsetup
+    from apxchol_b200.gen import Matrix
+    A0, F0 = problem("grid2d_64")
+    assert not native.DeviceOperator(eng, A0, F0.perm).fp32
+    # the same Laplacian with weights rounded to multiples of 1/8: every value,
+    # diagonal sums included, is exact in fp32
+    cols = np.repeat(np.arange(A0.n), np.diff(A0.colptr))
+    diag = A0.rowidx == cols
+    vals = np.where(diag, 0.0, -np.round(np.abs(A0.vals) * 8.0) / 8.0)
+    vals[diag] = -np.bincount(cols, weights=vals, minlength=A0.n)[cols[diag]]
+    assert np.array_equal(vals, vals.astype(np.float32).astype(np.float64))
+    A = Matrix(n=A0.n, colptr=A0.colptr, rowidx=A0.rowidx, vals=vals, name="grid2d_64_f32", sddm=A0.sddm)
+    F = refsetup.factorize(A, seed=0, threads=refsetup.DEFAULT_THREADS)
+    D = native.DeviceFactor(eng, F)
+    Op32 = native.DeviceOperator(eng, A, F.perm)
+    monkeypatch.setenv("APXCHOL_GPU_FP32_OPERATOR", "0")
+    Op64 = native.DeviceOperator(eng, A, F.perm)
+    monkeypatch.delenv("APXCHOL_GPU_FP32_OPERATOR")
+    assert Op32.fp32 and not Op64.fp32
+    b = gen.rhs(A.n, 31, not F.sddm)
+    x32, r32 = native.pcg(eng, D, Op32, b, tol=TOL, max_iter=500)
+    x64, r64 = native.pcg(eng, D, Op64, b, tol=TOL, max_iter=500)
+    assert r32.status == 0 and r32.iterations == r64.iterations
+    assert np.array_equal(x32, x64)
+    assert np.array_equal(Op32.matvec(b), Op64.matvec(b))
+    D32 = native.DeviceFactor(eng, F, precision=native.PREC_FP32)
+    B = np.stack([gen.rhs(A.n, 40 + c, not F.sddm) for c in range(4)])
+    out = []
+    for ops in ([Op32], [Op64], [Op32, Op32], [Op32, Op64]):
+        bt = native.Batch(eng, [D32] * len(ops), ops, 4)
+        out.append(bt.solve([B] * len(ops), tol=TOL)[0])
+        bt.close()
+    for o in out:
+        for xi in o:
+            assert np.array_equal(xi, out[0][0])
