@@ -84,7 +84,7 @@ def tune(eng: native.Engine, factor: native.DeviceFactor, op: native.DeviceOpera
 
 
 def tune_lanes(mat, fac, rhs, k: int, lanes_list=(2, 3, 4), tol: float = 1e-8, max_iter: int = 500,
-               device: int = 0, log=None):
+               device: int = 0, log=None, precision: int = native.PREC_FP32):
     """Solves/s of `lanes` concurrent k-slot batches (apxchol_b200.lanes), for
     each lane count; returns [(lanes, grid, solves/s, iterations)]."""
     import time
@@ -92,7 +92,7 @@ def tune_lanes(mat, fac, rhs, k: int, lanes_list=(2, 3, 4), tol: float = 1e-8, m
     from .lanes import Lanes
     table = []
     for nl in lanes_list:
-        ln = Lanes(mat, fac, k, lanes=nl, device=device)
+        ln = Lanes(mat, fac, k, lanes=nl, device=device, precision=precision)
         try:
             B, nrhs = ln.pack(np.stack([rhs(c) for c in range(k)]))
             dB = [torch.from_numpy(B).cuda(device) for _ in range(nl)]

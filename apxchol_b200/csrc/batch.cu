@@ -852,6 +852,12 @@ struct apxb_batch {
     const float* val[2] = {nullptr, nullptr};
     const uint32_t* chunk[2] = {nullptr, nullptr};
     uint32_t n_chunks[2] = {0, 0};
+    // fp16 factors (every instance's): binary16 plan values, per-row diagonal
+    // and (backward input) inverse scale squared, in the batch's row numbering
+    bool fp16 = false;
+    const uint16_t* val16[2] = {nullptr, nullptr};
+    const float* diag16 = nullptr;
+    const double* inv_scale2 = nullptr;
     apxb::sweep_ctl* ctl = nullptr;
     int grid32 = 0;
     // operator (combined, permuted) and permutation
@@ -931,6 +937,7 @@ struct apxb_batch {
         a.n_items = n_items[dir]; a.info = info[dir]; a.ord = ord[dir]; a.ptr = ptr[dir];
         a.idx = idx[dir]; a.val = val[dir]; a.ctl = ctl + dir;
         a.chunk = chunk[dir]; a.n_chunks = n_chunks[dir];
+        a.val16 = val16[dir]; a.diag16 = diag16; a.in_scale2 = dir == 1 ? inv_scale2 : nullptr;
         if (dir == 0) { a.in = rhs32; a.out = Yf; a.reset = Zf; }
         else { a.in = Yf; a.out = Zf; a.reset = Yf; }
     }
@@ -1005,6 +1012,7 @@ void batch_plan(const std::vector<const apxb_factor*>& fs, const std::vector<uin
             for (uint32_t q = p.ptr[sp]; q < p.ptr[sp + 1]; ++q) {
                 out.idx.push_back(p.idx[q] + off[sit.inst]);
                 out.val.push_back(p.val[q]);
+                if (!p.val16.empty()) out.val16.push_back(p.val16[q]);
                 ++e;
             }
         }
@@ -1230,7 +1238,11 @@ int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, a
         int rc;
         // ---- sweep plans (batch plans for this k) ----
         const uint32_t col_lanes = k >= 8 ? static_cast<uint32_t>(k / 4) : 1u;
-        if (n_inst == 1 && fs[0]->dev.on) {
+        // fp16 storage when every instance's factor has it (otherwise every
+        // instance sweeps over its fp32 values)
+        bt->fp16 = true;
+        for (const apxb_factor* f : fs) bt->fp16 = bt->fp16 && f->precision == APXB_PREC_FP16 && f->h.fp16;
+        if (n_inst == 1 && fs[0]->dev.on && !bt->fp16) {
             // a device-prepared factor: the plans are built on the device from its canonical arrays
             auto alloc_bytes = [&](void** q, size_t bytes) -> std::string {
                 char* c = nullptr;
@@ -1265,22 +1277,50 @@ int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, a
             for (int dir = 0; dir < 2; ++dir) {
                 const apxb::sweep_plan& pl = plans[dir];
                 if (!bad[dir].empty()) return fail(APXB_ERR_INVALID, "internal batch plan error: " + bad[dir]);
+                if (bt->fp16 && pl.val16.size() != pl.idx.size())
+                    return fail(APXB_ERR_INVALID, "internal batch plan error: fp16 values missing");
                 uint32_t *info, *ord, *ptr, *idx, *chunk;
-                float* val;
+                float* val = nullptr;
+                uint16_t* v16 = nullptr;
                 if ((rc = bt->dalloc(&info, pl.info.size())) || (rc = bt->dalloc(&ord, pl.ord.size())) ||
                     (rc = bt->dalloc(&ptr, pl.ptr.size())) || (rc = bt->dalloc(&idx, pl.idx.size())) ||
-                    (rc = bt->dalloc(&val, pl.val.size())) || (rc = bt->dalloc(&chunk, pl.chunk.size())))
+                    (rc = bt->fp16 ? bt->dalloc(&v16, pl.val16.size()) : bt->dalloc(&val, pl.val.size())) ||
+                    (rc = bt->dalloc(&chunk, pl.chunk.size())))
                     return rc;
                 APXB_CK(cudaMemcpyAsync(info, pl.info.data(), 4 * pl.info.size(), cudaMemcpyHostToDevice, s));
                 APXB_CK(cudaMemcpyAsync(ord, pl.ord.data(), 4 * pl.ord.size(), cudaMemcpyHostToDevice, s));
                 APXB_CK(cudaMemcpyAsync(ptr, pl.ptr.data(), 4 * pl.ptr.size(), cudaMemcpyHostToDevice, s));
                 APXB_CK(cudaMemcpyAsync(idx, pl.idx.data(), 4 * pl.idx.size(), cudaMemcpyHostToDevice, s));
-                APXB_CK(cudaMemcpyAsync(val, pl.val.data(), 4 * pl.val.size(), cudaMemcpyHostToDevice, s));
+                if (bt->fp16)
+                    APXB_CK(cudaMemcpyAsync(v16, pl.val16.data(), 2 * pl.val16.size(), cudaMemcpyHostToDevice, s));
+                else
+                    APXB_CK(cudaMemcpyAsync(val, pl.val.data(), 4 * pl.val.size(), cudaMemcpyHostToDevice, s));
                 APXB_CK(cudaMemcpyAsync(chunk, pl.chunk.data(), 4 * pl.chunk.size(), cudaMemcpyHostToDevice, s));
                 APXB_CK(cudaStreamSynchronize(s));
                 bt->n_items[dir] = pl.n_items;
                 bt->info[dir] = info; bt->ord[dir] = ord; bt->ptr[dir] = ptr; bt->idx[dir] = idx; bt->val[dir] = val;
+                bt->val16[dir] = v16;
                 bt->chunk[dir] = chunk; bt->n_chunks[dir] = static_cast<uint32_t>(pl.chunk.size() - 1);
+            }
+        }
+        if (bt->fp16) {   // per-row diagonal and inverse scale squared of every instance, at its row offset
+            if (n_inst == 1) {
+                bt->diag16 = fs[0]->diag16;
+                bt->inv_scale2 = fs[0]->inv_scale2;
+            } else {
+                float* dg;
+                double* is2;
+                if ((rc = bt->dalloc(&dg, bt->n_tot)) || (rc = bt->dalloc(&is2, bt->n_tot))) return rc;
+                APXB_CK(cudaMemsetAsync(dg, 0, 4 * static_cast<size_t>(bt->n_tot), s));
+                APXB_CK(cudaMemsetAsync(is2, 0, 8 * static_cast<size_t>(bt->n_tot), s));
+                for (int i = 0; i < n_inst; ++i) {
+                    const size_t m = fs[i]->h.m;
+                    APXB_CK(cudaMemcpyAsync(dg + bt->off[i], fs[i]->diag16, 4 * m, cudaMemcpyDeviceToDevice, s));
+                    APXB_CK(cudaMemcpyAsync(is2 + bt->off[i], fs[i]->inv_scale2, 8 * m, cudaMemcpyDeviceToDevice, s));
+                }
+                APXB_CK(cudaStreamSynchronize(s));
+                bt->diag16 = dg;
+                bt->inv_scale2 = is2;
             }
         }
         if ((rc = bt->dalloc(&bt->ctl, 2))) return rc;

@@ -330,6 +330,8 @@ void build_batch_plan(const prepared_factor& h, int dir, uint32_t col_lanes, swe
     const uint32_t total = row_e.back();
     plan.idx.resize(total);
     plan.val.resize(total);
+    const plan_vec<uint16_t>* val16 = h.fp16 ? (forward ? &h.csr_h : &h.csc_h) : nullptr;
+    if (val16) plan.val16.resize(total);
     std::vector<uint32_t> item_e(static_cast<size_t>(plan.n_items) + 1);
     for (uint32_t c = 0; c <= plan.n_items; ++c) item_e[c] = row_e[item_k[c]];
     const unsigned T = prep_threads(total);
@@ -353,8 +355,14 @@ void build_batch_plan(const prepared_factor& h, int dir, uint32_t col_lanes, swe
                 std::sort(order.begin(), order.end(), [&](const auto& x, const auto& y) {
                     return x.first != y.first ? x.first < y.first : idx[x.second] < idx[y.second];
                 });
-                for (const auto& o : order) { plan.idx[e] = idx[o.second]; plan.val[e] = val[o.second]; ++e; }
+                for (const auto& o : order) {
+                    plan.idx[e] = idx[o.second];
+                    plan.val[e] = val[o.second];
+                    if (val16) plan.val16[e] = (*val16)[o.second];
+                    ++e;
+                }
                 plan.idx[e] = idx[d]; plan.val[e] = val[d];
+                if (val16) plan.val16[e] = (*val16)[d];
             }
         }
     });

@@ -230,7 +230,9 @@ inline uint32_t group_width(uint32_t len) {
 //  * a row's off-diagonals are ordered by the level of the row they depend on,
 //    oldest first (ties by column), then the diagonal: consumed in order, a
 //    row then waits only at its end, on its newest dependencies;
-//  * item_level holds each item's level; chunk (see chunk_plan) the claim units.
+//  * item_level holds each item's level; chunk (see chunk_plan) the claim units;
+//  * fp16 factors: val16 holds the binary16 values in the same layout (the
+//    diagonal slot's is not read: the sweep divides by diag16 of the row).
 // The fp32 sweep need not follow the reference's sum order (it has a
 // tolerance); this order is fixed, so results stay deterministic.
 void build_batch_plan(const prepared_factor& h, int dir, uint32_t col_lanes, sweep_plan& out);

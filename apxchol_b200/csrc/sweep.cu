@@ -660,7 +660,7 @@ struct stage_wide {
     float ww[wide_cfg<K>::B];
 };
 
-template <int K>
+template <int K, bool H>
 __device__ __forceinline__ void load_wide(const sweep_args<float>& a, const stage_desc& ds, stage_wide<K>& s) {
     using W = wide_cfg<K>;
     s.v = view_of(ds);
@@ -675,13 +675,19 @@ __device__ __forceinline__ void load_wide(const sweep_args<float>& a, const stag
 #pragma unroll
     for (int k = 0; k < W::B; ++k) {
         const uint32_t t = (static_cast<uint32_t>(k) << s.glg) + s.ue;
-        if (t < v.len) { s.jj[k] = __ldg(a.idx + v.q + t); s.ww[k] = __ldg(a.val + v.q + t); }
+        if (t < v.len) { s.jj[k] = __ldg(a.idx + v.q + t); s.ww[k] = weight32<H>(a, v.q + t); }
     }
     if (v.valid && s.ue == 0) {
         const size_t base = static_cast<size_t>(v.row) * K + s.cl * W::KC;
+        if (H && a.in_scale2) {   // fp16 storage, backward: the input times inv_scale^2, in fp64, rounded once
+            const double sc = a.in_scale2[v.row];
 #pragma unroll
-        for (int r = 0; r < W::KC; ++r) s.rhs[r] = a.in[base + r];
-        s.d = __ldg(a.val + v.q + v.len);
+            for (int r = 0; r < W::KC; ++r) s.rhs[r] = static_cast<float>(static_cast<double>(a.in[base + r]) * sc);
+        } else {
+#pragma unroll
+            for (int r = 0; r < W::KC; ++r) s.rhs[r] = a.in[base + r];
+        }
+        s.d = H ? __ldg(a.diag16 + v.row) : __ldg(a.val + v.q + v.len);
     }
 }
 
@@ -702,7 +708,7 @@ __device__ __forceinline__ void prefetch_wide(const sweep_args<float>& a, const 
     }
 }
 
-template <int DIR, int K>
+template <int DIR, int K, bool H>
 __device__ __forceinline__ bool run_wide(const sweep_args<float>& a, stage_wide<K>& s, const stage_wide<K>& next) {
     using W = wide_cfg<K>;
     constexpr int B = W::B, KC = W::KC;
@@ -721,7 +727,7 @@ __device__ __forceinline__ bool run_wide(const sweep_args<float>& a, stage_wide<
 #pragma unroll
             for (int k = 0; k < B; ++k) {
                 const uint32_t t = ((jb + k) << s.glg) + s.ue;
-                if (t < v.len) { s.jj[k] = __ldg(a.idx + v.q + t); s.ww[k] = __ldg(a.val + v.q + t); }
+                if (t < v.len) { s.jj[k] = __ldg(a.idx + v.q + t); s.ww[k] = weight32<H>(a, v.q + t); }
             }
         }
         const uint32_t t0 = (jb << s.glg) + s.ue;
@@ -774,7 +780,7 @@ __device__ __forceinline__ bool run_wide(const sweep_args<float>& a, stage_wide<
     return true;
 }
 
-template <int DIR, int K>
+template <int DIR, int K, bool H>
 __global__ void __launch_bounds__(kSweepThreads, 2) k_dw32(const sweep_args<float> a) {
     if (a.skip && *a.skip) return;
     const unsigned lane = threadIdx.x & 31u;
@@ -783,16 +789,16 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_dw32(const sweep_args<floa
     stage_desc dD;
     load_desc(a, cc.next(a), dD);
     stage_wide<K> sL;
-    load_wide<K>(a, dD, sL);
+    load_wide<K, H>(a, dD, sL);
     load_desc(a, cc.next(a), dD);
     int bad = 0;   // the error word, read one item late so the load is never waited on
     while (sL.v.c < a.n_items) {
         stage_wide<K> sR = sL;
-        load_wide<K>(a, dD, sL);
+        load_wide<K, H>(a, dD, sL);
         load_desc(a, cc.next(a), dD);
         if (__shfl_sync(kFull, bad, 0)) break;
         if (lane == 0) bad = ld_relaxed_int(&a.err->code);
-        if (!run_wide<DIR, K>(a, sR, sL)) break;
+        if (!run_wide<DIR, K, H>(a, sR, sL)) break;
     }
     leave(a.ctl);
 }
@@ -1045,8 +1051,13 @@ int sweep_grid64(int num_sms) {
 template <int K>
 void sweep32_batch_dir(int dir, const sweep_args<float>& a, int grid, cudaStream_t s) {
     if (!a.n_items) return;
-    if (dir == 0) k_dw32<0, K><<<grid, kSweepThreads, 0, s>>>(a);
-    else          k_dw32<1, K><<<grid, kSweepThreads, 0, s>>>(a);
+    if (a.val16) {
+        if (dir == 0) k_dw32<0, K, true><<<grid, kSweepThreads, 0, s>>>(a);
+        else          k_dw32<1, K, true><<<grid, kSweepThreads, 0, s>>>(a);
+    } else {
+        if (dir == 0) k_dw32<0, K, false><<<grid, kSweepThreads, 0, s>>>(a);
+        else          k_dw32<1, K, false><<<grid, kSweepThreads, 0, s>>>(a);
+    }
 }
 
 void launch_sweep32_batch(int dir, const sweep_args<float>& a, int grid, cudaStream_t s) {
@@ -1064,7 +1075,7 @@ void launch_sweep32_batch(int dir, const sweep_args<float>& a, int grid, cudaStr
 template <int K>
 int occ32_batch() {
     int b = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_dw32<1, K>, kSweepThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_dw32<1, K, false>, kSweepThreads, 0);
     return b;
 }
 

@@ -8,8 +8,9 @@ persistent sweep grid is cut to its share of the SMs, so the lanes' sweeps
 are co-resident. Lanes never wait on one another (every sweep claims its
 work in level order from its own counter), so any grid is safe.
 
-Each lane holds its own copy of the factor (fp32) and the operator. One lane
-of 128^3 at k = 16 is about 2.6 GB of device memory.
+Each lane holds its own copy of the factor (fp32, or fp16 storage with
+precision=native.PREC_FP16) and the operator. One lane of 128^3 at k = 16 is
+about 2.6 GB of device memory.
 """
 from __future__ import annotations
 
@@ -21,12 +22,12 @@ from . import native
 
 
 class Lane:
-    def __init__(self, mat, fac, k: int, grid: int, device: int):
+    def __init__(self, mat, fac, k: int, grid: int, device: int, precision: int = native.PREC_FP32):
         self.batch = self.op = self.factor = None
         self.eng = native.Engine(device)
         self.eng.set_sweep_grid(grid)
         try:
-            self.factor = native.DeviceFactor(self.eng, fac, precision=native.PREC_FP32)
+            self.factor = native.DeviceFactor(self.eng, fac, precision=precision)
             self.op = native.DeviceOperator(self.eng, mat, fac.perm)
             self.batch = native.Batch(self.eng, [self.factor], [self.op], k)
         except Exception:
@@ -43,9 +44,11 @@ class Lane:
 
 class Lanes:
     """`lanes` batches of k slots over one matrix. grid: sweep blocks per lane
-    (0 = the resident grid divided among the lanes)."""
+    (0 = the resident grid divided among the lanes); precision: the factor
+    storage (native.PREC_FP32, or native.PREC_FP16)."""
 
-    def __init__(self, mat, fac, k: int, lanes: int = 1, grid: int = 0, device: int = 0):
+    def __init__(self, mat, fac, k: int, lanes: int = 1, grid: int = 0, device: int = 0,
+                 precision: int = native.PREC_FP32):
         import torch
         self.k, self.n, self.device = k, mat.n, device
         if grid <= 0 and lanes > 1:
@@ -55,7 +58,7 @@ class Lanes:
         self.lanes = []
         try:
             for _ in range(lanes):
-                self.lanes.append(Lane(mat, fac, k, grid, device))
+                self.lanes.append(Lane(mat, fac, k, grid, device, precision))
         except Exception:
             self.close()
             raise

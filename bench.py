@@ -347,9 +347,10 @@ def run_ours(args, rank, world, local_rank):
     n = A.n
     eng = native.Engine(local_rank)
     t0 = time.time()
-    D32 = native.DeviceFactor(eng, F, precision=native.PREC_FP32)
+    prec = native.PREC_FP16 if args.storage == "fp16" else native.PREC_FP32
+    D32 = native.DeviceFactor(eng, F, precision=prec)
     Op = native.DeviceOperator(eng, A, F.perm)
-    log(f"[bench] upload fp32 factor + operator {time.time() - t0:.1f}s; stored nnz {D32.info.nnz_stored}; "
+    log(f"[bench] upload {args.storage} factor + operator {time.time() - t0:.1f}s; stored nnz {D32.info.nnz_stored}; "
         f"levels {D32.info.fwd_levels}")
     stream = torch.cuda.ExternalStream(eng.stream)
 
@@ -365,7 +366,8 @@ def run_ours(args, rank, world, local_rank):
         ch = autotune.tune(eng, D32, Op, rhs, tol=TOL, max_iter=MAX_ITER, log=lg)
         k, grid, nlanes, best = ch.k, ch.grid, 1, ch.solves_per_s
         tuned = [{"k": t[0], "lanes": 1, "grid": t[1] or "resident", "solves_s": t[2]} for t in ch.table]
-        for nl, g, sps, _ in autotune.tune_lanes(A, F, rhs, k, tol=TOL, max_iter=MAX_ITER, device=local_rank, log=lg):
+        for nl, g, sps, _ in autotune.tune_lanes(A, F, rhs, k, tol=TOL, max_iter=MAX_ITER, device=local_rank, log=lg,
+                                                 precision=prec):
             tuned.append({"k": k, "lanes": nl, "grid": g, "solves_s": sps})
             if sps > best:
                 grid, nlanes, best = g, nl, sps
@@ -382,7 +384,7 @@ def run_ours(args, rank, world, local_rank):
     for _ in range(3):
         torch.cuda.synchronize()
         t_adm = time.perf_counter()
-        Da = native.DeviceFactor(eng, F, precision=native.PREC_FP32)
+        Da = native.DeviceFactor(eng, F, precision=prec)
         t_f = time.perf_counter()
         Oa = native.DeviceOperator(eng, A, F.perm)
         t_o = time.perf_counter()
@@ -397,7 +399,7 @@ def run_ours(args, rank, world, local_rank):
                  "batch_ms": [round(a[3], 1) for a in adm], "k": k}
     log(f"[bench] admission (factor + operator + k={k} batch), 3 times: " +
         ", ".join(f"{a[0]:.0f} ms ({a[1]:.0f} + {a[2]:.0f} + {a[3]:.0f})" for a in adm))
-    lanes = Lanes(A, F, k, lanes=nlanes, grid=grid, device=local_rank)
+    lanes = Lanes(A, F, k, lanes=nlanes, grid=grid, device=local_rank, precision=prec)
     grid = lanes.grid
     bt = lanes.lanes[0].batch
     streams = [torch.cuda.ExternalStream(h) for h in lanes.streams]
@@ -494,21 +496,25 @@ def run_ours(args, rank, world, local_rank):
     fwd_s = sum(t[0] for t in st) / len(st)
     bck_s = sum(t[1] for t in st) / len(st)
     m, nnz_s = D32.info.m, D32.info.nnz_stored
-    sweep_bytes = nnz_s * 8 + 4 * (m + 1) + 2 * m * 4 * k
+    # per stored entry: index + value (fp32 4 B, fp16 2 B); fp16 adds the per-row fp32 diagonal and,
+    # in the backward sweep, the fp64 inverse scale squared (4 B per row on average over the pair)
+    e_bytes, r_bytes = (6, 8) if args.storage == "fp16" else (8, 0)
+    sweep_bytes = nnz_s * e_bytes + 4 * (m + 1) + r_bytes * m + 2 * m * 4 * k
     sweep_s = (fwd_s + bck_s) / 2
     peak, peak_kind = measured_peak_hbm()
     achieved = sum(2 * sweep_bytes / (t[0] + t[1]) for t in st) / 1e9   # summed over the concurrent lanes
     traffic, traffic_src = profiled_traffic(k, args.grid)
-    b_iter = 2 * (nnz_s * 8 + 4 * (m + 1)) + A.nnz * 12 + 4 * (n + 1)
+    b_iter = 2 * (nnz_s * e_bytes + 4 * (m + 1) + r_bytes * m) + A.nnz * 12 + 4 * (n + 1)
     b_iter *= nlanes   # every lane reads the factor and the matrix once per iteration
     iter_s = dev_s / max(1, sum(iters_timed))
     iter_gbs = b_iter / iter_s / 1e9
     # all algorithmic traffic of one batched iteration (every vector pass the kernels make), per lane:
-    # SpMV (A, p gathered once, Ap written), x/r update (x, p, r, Ap read; x, r written; fp32 input
-    # written), two sweeps (factor, input read, output and re-armed buffer written), r.z, p update
+    # SpMV (A, p gathered once, Ap written), r update (r, Ap read; r and the fp32 sweep input
+    # written), two sweeps (factor, input read, output and re-armed buffer written), r.z (r, z read),
+    # x and p update (x, p, z read; x, p written)
     v8, v4 = 8 * n * k, 4 * n * k
-    b_all = (A.nnz * 12 + 4 * (n + 1) + 2 * v8) + (6 * v8 + v4) + \
-        2 * (nnz_s * 8 + 4 * (m + 1) + 3 * v4) + (v8 + v4) + (v4 + 2 * v8)
+    b_all = (A.nnz * 12 + 4 * (n + 1) + 2 * v8) + (3 * v8 + v4) + \
+        2 * (nnz_s * e_bytes + 4 * (m + 1) + r_bytes * m + 3 * v4) + (v8 + v4) + (v4 + 4 * v8)
     b_all *= nlanes
     iter_all_gbs = b_all / iter_s / 1e9
     dev_s, e2e_s = max_over_ranks([dev_s, e2e_s], world, dev)
@@ -578,18 +584,20 @@ def run_ours(args, rank, world, local_rank):
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_s / args.steps * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 sweeps / f64 outer",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 sweeps / f64 outer" + (" (fp16 factor storage)" if args.storage == "fp16" else ""),
         "data": "synthetic (seeded generator, reference factorization)",
         "config": workload_config(args.grid, A, F, f"batched mixed precision, {nlanes} lane(s) x {k} RHS per step",
                                   {"k": k, "lanes": nlanes, "sweep_grid": grid or "resident", "rhs_sets": POOL,
-                                   "parallelism": f"replicas x{world}"}),
+                                   "factor_storage": args.storage, "parallelism": f"replicas x{world}"}),
         "iterations": [min(iters_timed), max(iters_timed)], "true_relres_max": host_tres,
         "e2e": {"value": world * args.steps * k * nlanes / e2e_s, "unit": "solves/s",
                 "h2d_bytes_per_step": 8 * n * k * nlanes, "d2h_bytes_per_step": (8 * n * k + 24 * k) * nlanes},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "traffic_source": traffic_src,
-                     "kernel": f"k_dw32<DIR,{k}> (batched fp32 sweep, {k} RHS, {nlanes} concurrent lane(s), "
-                               f"{grid} blocks each)",
+                     "kernel": f"k_dw32<DIR,{k},{'true' if args.storage == 'fp16' else 'false'}> (batched fp32 "
+                               f"sweep, {args.storage} factor storage, {k} RHS, {nlanes} concurrent lane(s), "
+                               f"{grid or 'resident'} blocks each)",
                      "bytes_per_launch": sweep_bytes, "fwd_us": fwd_s * 1e6, "bck_us": bck_s * 1e6,
                      "peak_kind": peak_kind, "iter_bytes": b_iter, "iter_gbs": iter_gbs, "iter_frac": iter_gbs / peak,
                      "iter_all_bytes": b_all, "iter_all_gbs": iter_all_gbs, "iter_all_frac": iter_all_gbs / peak},
@@ -823,6 +831,8 @@ def main():
     ap.add_argument("--lanes", type=int, default=1, help="concurrent batches (streams) with --k")
     ap.add_argument("--iters-per-step", type=int, default=2, help="serving: iterations per server step")
     ap.add_argument("--serve-requests", type=int, default=1000)
+    ap.add_argument("--storage", choices=["fp32", "fp16"], default="fp32",
+                    help="batched factor storage: fp32 values, or the reference GPU default fp16 (column-scaled)")
     ap.add_argument("--serve-k", type=int, default=16,
                     help="serving: slots per lane (at most the batch k; fewer slots, shorter iterations, lower latency)")
     ap.add_argument("--serve-load", type=float, default=0.7,

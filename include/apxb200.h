@@ -201,6 +201,17 @@ int apxb_sweep_pair_multi(apxb_engine* e, apxb_factor* f, int k, const double* d
  * flags: APXB_DEVICE_PTRS | APXB_CENTER_*; rz_out (may be NULL) receives b.z. */
 int apxb_apply(apxb_engine* e, apxb_factor* f, const double* b, double* z, int flags, double* rz_out);
 
+/* ---- the reference's raw dataflow sweep (cuda_dataflow.h:160-208) ----
+ * apxchol::dataflow_solve / dataflow_solve_fp16 / dataflow_grid_size /
+ * dataflow_prefetch_depth are C++ functions of this library, declared by the
+ * replacement header apxchol/solver/sptrsv/cuda_dataflow.h (include/apxchol_compat).
+ * They report nothing themselves (the reference's return void): a launch whose
+ * wait made no progress for one second (a plan or epoch that breaks the
+ * contract) stops and records it. apxb_dataflow_status returns that record
+ * (APXB_ERR_TIMEOUT or APXB_ERR_INVALID with apxb_last_error set, else APXB_OK)
+ * and clears it; it synchronizes with the device. */
+int apxb_dataflow_status(void);
+
 /* ---- operator: A in the factor's permuted ordering (cuda_pcg::setup, pcg_cuda.h:68-152) ----
  * colptr[n+1], rowidx[nnz], vals[nnz]: full symmetric CSC (int32, rows ascending).
  * Values are stored in fp32 when every one round-trips fp32 (v == (double)(float)v),

@@ -197,3 +197,66 @@ def test_residual_refresh(eng, every):
         assert r1[0][c].status == 0 and r1[0][c].true_residual < TRUE_RES_FACTOR * TOL
         xo, ito, _ = O.solve(B[c], TOL, 500)
         assert np.linalg.norm(x1[0][c] - xo) <= 1e-6 * np.linalg.norm(xo)
+
+
+def _centred(x):
+    return x - x.mean()
+
+
+@pytest.mark.parametrize("k", [4, 16, 64])
+def test_fp16_factor_storage_in_the_batch(eng, k):
+    """The reference GPU path's default storage -- fp16 values of the
+    column-scaled factor, a per-row fp32 diagonal, the backward input times
+    (1/s)^2 in fp64 (cuda.h:131-163, cuda_dataflow.cu:395) -- in the batched
+    sweeps. Every slot meets the true-residual gate and lies within the PCG
+    tolerance of the reference's FP64 solution (the oracle); iterations stay
+    within 3 of the fp32-stored factor's (fp16 rounds every off-diagonal to 11
+    bits, a slightly different preconditioner)."""
+    for name in ("grid3d_24", "grid2d_64"):
+        A, F = problem(name)
+        D16 = native.DeviceFactor(eng, F, precision=native.PREC_FP16)
+        D32 = native.DeviceFactor(eng, F, precision=native.PREC_FP32)
+        Op = native.DeviceOperator(eng, A, F.perm)
+        B = np.stack([gen.rhs(A.n, 300 + c, not F.sddm) for c in range(k)])
+        b16 = native.Batch(eng, [D16], [Op], k)
+        x16, r16 = b16.solve([B], tol=TOL)
+        x16b, _ = b16.solve([B], tol=TOL)
+        assert np.array_equal(x16[0], x16b[0])            # repeats bitwise
+        b32 = native.Batch(eng, [D32], [Op], k)
+        _, r32 = b32.solve([B], tol=TOL)
+        O = oracle.Oracle(A, F, nt=8)
+        for c in range(k):
+            r = r16[0][c]
+            assert r.status == 0 and r.true_residual < TRUE_RES_FACTOR * TOL, (name, c, r.status, r.true_residual)
+            assert abs(r.iterations - r32[0][c].iterations) <= 3, (name, c, r.iterations, r32[0][c].iterations)
+            if c < 8:
+                xo, _, _ = O.solve(B[c], TOL, 500)
+                assert np.linalg.norm(_centred(x16[0][c]) - _centred(xo)) <= 1e-6 * np.linalg.norm(_centred(xo))
+        b16.close(); b32.close()
+
+
+def test_fp16_instances_share_one_batch(eng):
+    """fp16 instances of different sizes in one batch give each instance's
+    bytes alone; a batch mixing fp16 and fp32 factors sweeps every instance
+    over its fp32 values and still converges."""
+    names = ["grid2d_64", "grid3d_24", "regular_3000"]
+    objs = []
+    for nm in names:
+        A, F = problem(nm)
+        objs.append((A, F, native.DeviceFactor(eng, F, precision=native.PREC_FP16),
+                     native.DeviceFactor(eng, F, precision=native.PREC_FP32), native.DeviceOperator(eng, A, F.perm)))
+    rhs = [np.stack([gen.rhs(A.n, 50 + 3 * i + j, not F.sddm) for j in range(1 + i)])
+           for i, (A, F, _, _, _) in enumerate(objs)]
+    bt = native.Batch(eng, [o[2] for o in objs], [o[4] for o in objs], 4)
+    xs, res = bt.solve(rhs, tol=TOL)
+    for i, (A, F, D16, D32, Op) in enumerate(objs):
+        alone = native.Batch(eng, [D16], [Op], 4)
+        xa, _ = alone.solve([rhs[i]], tol=TOL)
+        assert np.array_equal(xs[i], xa[0]), names[i]
+        for r in res[i]:
+            assert r.status == 0 and r.true_residual < TRUE_RES_FACTOR * TOL
+    mixed = native.Batch(eng, [objs[0][2], objs[1][3]], [objs[0][4], objs[1][4]], 4)
+    _, rm = mixed.solve(rhs[:2], tol=TOL)
+    for ri in rm:
+        for r in ri:
+            assert r.status == 0 and r.true_residual < TRUE_RES_FACTOR * TOL
