@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <memory>
 #include <new>
 #include <string>
@@ -79,6 +80,8 @@ int apxb_engine_create(int device, apxb_engine** out) {
     APXB_CK(cudaEventCreate(&e->ev1));
     APXB_CK(cudaStreamSynchronize(e->stream));
     e->mem_used = 0;   // engine scratch is not charged to the factor/operator budget
+    e->pool = apxb::device_pool(device);   // the scratch above stays on cudaMalloc (engine_free frees it)
+    apxb::pool_engine_added(device);
     *out = e.release();
     return APXB_OK;
 }
@@ -90,7 +93,10 @@ void engine_free(apxb_engine* e) {
     cudaSetDevice(e->device);
     cudaStreamSynchronize(e->stream);
     cudaFree(e->d_err); cudaFree(e->d_partials); cudaFree(e->d_counters); cudaFree(e->d_scal);
-    cudaFree(e->d_stage_a); cudaFree(e->d_stage_b);
+    e->release(e->d_stage_a, e->stage_n * 8);
+    e->release(e->d_stage_b, e->stage_n * 8);
+    cudaStreamSynchronize(e->stream);
+    apxb::pool_engine_removed(e->device);
     if (e->h_err) cudaFreeHost(e->h_err);
     if (e->h_scal) cudaFreeHost(e->h_scal);
     if (e->h_stage_a) cudaFreeHost(e->h_stage_a);
@@ -106,6 +112,61 @@ void apxb_detail::release_child(apxb_engine* e) {
     if (--e->children == 0 && e->closing) engine_free(e);
 }
 using apxb_detail::release_child;
+
+namespace apxb {
+
+namespace {
+std::mutex g_pool_mu;
+std::vector<cudaMemPool_t> g_pools;   // per device
+std::vector<int> g_pool_engines;      // engines alive per device
+int g_pools_off = -1;
+}  // namespace
+
+cudaMemPool_t device_pool(int device) {
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (g_pools_off < 0) {
+        const char* ev = std::getenv("APXB_NO_POOL");
+        g_pools_off = ev && *ev && *ev != '0' ? 1 : 0;
+    }
+    if (g_pools_off || device < 0) return nullptr;
+    if (static_cast<int>(g_pools.size()) <= device) {
+        g_pools.resize(static_cast<size_t>(device) + 1, nullptr);
+        g_pool_engines.resize(static_cast<size_t>(device) + 1, 0);
+    }
+    if (!g_pools[device]) {
+        int supported = 0;
+        if (cudaDeviceGetAttribute(&supported, cudaDevAttrMemoryPoolsSupported, device) != cudaSuccess || !supported) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t pool = nullptr;
+        if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        uint64_t keep = UINT64_MAX;   // freed memory stays in the pool until the last engine goes
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        g_pools[device] = pool;
+    }
+    return g_pools[device];
+}
+
+void pool_engine_added(int device) {
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (device >= 0 && device < static_cast<int>(g_pool_engines.size())) ++g_pool_engines[device];
+}
+
+void pool_engine_removed(int device) {
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (device < 0 || device >= static_cast<int>(g_pool_engines.size())) return;
+    if (--g_pool_engines[device] == 0 && g_pools[device]) cudaMemPoolTrimTo(g_pools[device], 0);
+}
+
+}  // namespace apxb
 
 extern "C" {
 

@@ -107,7 +107,11 @@ struct dbuf {
     T* get() const { return static_cast<T*>(p); }
     cudaError_t alloc(size_t bytes, cudaStream_t st) {
         s = st;
-        return cudaMallocAsync(&p, bytes ? bytes : 16, st);
+        int dev = 0;
+        const cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        cudaMemPool_t pool = device_pool(dev);   // the library's pool, else the device's default one
+        return pool ? cudaMallocFromPoolAsync(&p, bytes ? bytes : 16, pool, st) : cudaMallocAsync(&p, bytes ? bytes : 16, st);
     }
 };
 

@@ -48,8 +48,21 @@ using apxb_detail::guarded;
     } while (0)
 
 
+namespace apxb {
+// The library's stream-ordered memory pool on `device` (created on first use,
+// kept for the process): freed buffers stay mapped in it for the next
+// allocation instead of going back to the driver, and freeing does not
+// synchronize the device. nullptr when pools are off (APXB_NO_POOL=1) or the
+// device has none; then plain cudaMalloc / cudaFree are used.
+cudaMemPool_t device_pool(int device);
+// Engines alive per device; the pool is trimmed when the last one goes.
+void pool_engine_added(int device);
+void pool_engine_removed(int device);
+}  // namespace apxb
+
 struct apxb_engine {
     int device = 0;
+    cudaMemPool_t pool = nullptr;         // apxb::device_pool(device) for factor / operator / batch buffers
     int num_sms = 148;
     cudaStream_t stream = nullptr;
     apxb::dev_error* d_err = nullptr;
@@ -76,18 +89,28 @@ struct apxb_engine {
         if (mem_budget && mem_used + bytes > mem_budget)
             return fail(APXB_ERR_BUDGET, "device memory budget exhausted: " + std::to_string(mem_used) + " + " +
                                              std::to_string(bytes) + " > " + std::to_string(mem_budget));
-        const cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+        cudaError_t e;
+        if (pool) {   // stream-ordered; synchronized so that every stream may use the buffer at once
+            e = cudaMallocFromPoolAsync(p, bytes ? bytes : 16, pool, stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        } else {
+            e = cudaMalloc(p, bytes ? bytes : 16);
+        }
         if (e != cudaSuccess) {
             *p = nullptr;
             cudaGetLastError();
-            return fail(APXB_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+            return fail(APXB_ERR_OOM, std::string(pool ? "cudaMallocFromPoolAsync: " : "cudaMalloc: ") +
+                                          cudaGetErrorString(e));
         }
         mem_used += bytes;
         return APXB_OK;
     }
+    // Frees a buffer from alloc(): in stream order on the engine stream (after
+    // the work already queued there), without a device-wide synchronization.
     void release(void* p, size_t bytes) {
         if (p) {
-            cudaFree(p);
+            if (pool) cudaFreeAsync(p, stream);
+            else cudaFree(p);
             mem_used -= bytes;
         }
     }
