@@ -651,7 +651,7 @@ def run_rmat22(args, rank, world, local_rank):
     eng = native.Engine(local_rank)
     D32 = native.DeviceFactor(eng, F, precision=native.PREC_FP32)
     Op = native.DeviceOperator(eng, A, F.perm)
-    ch = autotune.tune(eng, D32, Op, rhs, tol=TOL, max_iter=MAX_ITER, ks=(1, 4, 8, 16), grids=(0,), log=log)
+    ch = autotune.tune(eng, D32, Op, rhs, tol=TOL, max_iter=MAX_ITER, ks=(1, 4, 8, 16, 32, 64), grids=(0,), log=log)
     k = ch.k
     bt = native.Batch(eng, [D32], [Op], k)
     B = np.stack([rhs(c) for c in range(k)])
@@ -681,9 +681,14 @@ def run_rmat22(args, rank, world, local_rank):
     D64.close(); Op.close(); eng.close()
     ref = None
     if oracle.ref_available():
-        oracle.set_threads(os.cpu_count() or 1)
+        lib = oracle.use_fastest_ref()
+        cores = oracle.host_cores()
+        oracle.set_threads(cores)
         xr, itr, _, sr = oracle.Ref(A, F).solve(B[0], TOL, MAX_ITER)
-        ref = {"iterations": int(itr), "seconds": sr, "solves_s": 1.0 / sr, "cores": os.cpu_count()}
+        xa, xb = X[:n] - X[:n].mean(), xr - xr.mean()   # a Laplacian's solutions, compared up to the null space
+        err = float(np.linalg.norm(xa - xb) / np.linalg.norm(xb))   # batched slot 0 against the reference
+        ref = {"iterations": int(itr), "seconds": sr, "solves_s": 1.0 / sr, "cores": cores, "lib": lib,
+               "oracle_err_slot0": err}
     line = {"metric": METRIC, "value": k * steps / secs, "unit": "solves/s", "n_gpus": world, "steps": steps,
             "warmup": args.warmup, "ms_per_step": secs / steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 sweeps / f64 outer", "data": "synthetic (seeded generator)",
