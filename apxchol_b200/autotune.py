@@ -2,7 +2,7 @@
 
 For one matrix it times a whole batched solve (CUDA events, device-resident
 right-hand sides) for every right-hand-side block width k in
-{1, 2, 4, 8, 16, 32, 64} and every candidate sweep grid (the resident grid and one block per SM), and
+{1, 2, 4, 8, 16, 32, 64, 128} and every candidate sweep grid (the resident grid and one block per SM), and
 keeps the fastest solves/s. The sweeps' other knobs are fixed by the plan: the
 lanes per row follow the row length (1, 4, 8, 16 or 32), and the in-flight
 depth is the 3-stage item pipeline with 8 entries per lane, plus an L2
@@ -19,7 +19,7 @@ import numpy as np
 
 from . import native
 
-KS = (1, 2, 4, 8, 16, 32, 64)
+KS = (1, 2, 4, 8, 16, 32, 64, 128)
 KS_INSTANCES = (1, 2, 4, 8, 16)   # many small instances with 1-8 right-hand sides each
 
 

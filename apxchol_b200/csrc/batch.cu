@@ -100,7 +100,9 @@ __device__ __forceinline__ void col_store(double (&a)[NV][2], double* dst) {
             for (int o = H; o < 32; o <<= 1) a[v][e] += __shfl_xor_sync(apxb::kFull, a[v][e], o);
     }
     if (lane < static_cast<unsigned>(H)) {
-        const int c0 = K == 1 ? 0 : 2 * static_cast<int>(lane);
+        // the thread's pair (2 * threadIdx.x) % K: 2 * lane for K <= 64; warp w holds columns
+        // [64 w % K, 64 w % K + 64) for K = 128
+        const int c0 = K == 1 ? 0 : static_cast<int>((2u * threadIdx.x) % static_cast<unsigned>(K));
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             red[warp][v][c0] = a[v][0];
@@ -111,7 +113,8 @@ __device__ __forceinline__ void col_store(double (&a)[NV][2], double* dst) {
     if (threadIdx.x < static_cast<unsigned>(K * NV)) {
         const int v = threadIdx.x / K, c = threadIdx.x % K;
         double s = 0.0;
-        for (int w = 0; w < kBT / 32; ++w) s += red[w][v][c];
+        for (int w = 0; w < kBT / 32; ++w)
+            if (K <= 64 || (64 * w) % K == (c & ~63)) s += red[w][v][c];   // the warps holding column c
         dst[v * K + c] = s;
     }
     __syncthreads();
@@ -742,13 +745,16 @@ __global__ void __launch_bounds__(kFinThreads) k_b_fin(bp P, int mode) {
 template <int K>
 __global__ void __launch_bounds__(kBT) k_b_xsum(bp P) {
     for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
-        double v[K];
-#pragma unroll
-        for (int c = 0; c < K; ++c) v[c] = 0.0;
-        for (unsigned row = P.tile_lo[t] + threadIdx.x; row < P.tile_hi[t]; row += blockDim.x)
-#pragma unroll
-            for (int c = 0; c < K; ++c) v[c] += P.x[static_cast<size_t>(row) * K + c];
-        tile_store<K>(v, P.partials + static_cast<size_t>(t) * K * 2);
+        double acc[1][2] = {{0.0, 0.0}};
+        FLAT_PAIRS(t, {
+            if (two) {
+                const double2 x = *reinterpret_cast<const double2*>(P.x + q);
+                acc[0][0] += x.x; acc[0][1] += x.y;
+            } else {
+                acc[0][0] += P.x[q];
+            }
+        })
+        col_store<K, 1>(acc, P.partials + static_cast<size_t>(t) * K * 2);
     }
 }
 
@@ -779,18 +785,21 @@ __global__ void __launch_bounds__(kBT) k_b_out(bp P, double* X) {
 template <int K>
 __global__ void __launch_bounds__(kBT) k_b_resid(bp P) {
     for (unsigned t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
-        double v[2 * K];
-#pragma unroll
-        for (int c = 0; c < 2 * K; ++c) v[c] = 0.0;
-        for (unsigned row = P.tile_lo[t] + threadIdx.x; row < P.tile_hi[t]; row += blockDim.x)
-#pragma unroll
-            for (int c = 0; c < K; ++c) {
-                const size_t q = static_cast<size_t>(row) * K + c;
+        double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};   // [0]: ||b - A x||^2, [1]: ||b||^2
+        FLAT_PAIRS(t, {
+            if (two) {
+                const double2 b = *reinterpret_cast<const double2*>(P.b + q);
+                const double2 y = *reinterpret_cast<const double2*>(P.Ap + q);
+                const double d0 = b.x - y.x, d1 = b.y - y.y;
+                acc[0][0] = fma(d0, d0, acc[0][0]); acc[0][1] = fma(d1, d1, acc[0][1]);
+                acc[1][0] = fma(b.x, b.x, acc[1][0]); acc[1][1] = fma(b.y, b.y, acc[1][1]);
+            } else {
                 const double d = P.b[q] - P.Ap[q];
-                v[c] = fma(d, d, v[c]);
-                v[K + c] = fma(P.b[q], P.b[q], v[K + c]);
+                acc[0][0] = fma(d, d, acc[0][0]);
+                acc[1][0] = fma(P.b[q], P.b[q], acc[1][0]);
             }
-        tile_store<2 * K>(v, P.partials + static_cast<size_t>(t) * K * 2);
+        })
+        col_store<K, 2>(acc, P.partials + static_cast<size_t>(t) * K * 2);
     }
 }
 
@@ -1069,7 +1078,8 @@ int launch_iteration(apxb_batch* bt, const bp& P, cudaStream_t s, unsigned long 
         case 8: return launch_iteration_k<8>(bt, P, s, h, use_cond);
         case 16: return launch_iteration_k<16>(bt, P, s, h, use_cond);
         case 32: return launch_iteration_k<32>(bt, P, s, h, use_cond);
-        default: return launch_iteration_k<64>(bt, P, s, h, use_cond);
+        case 64: return launch_iteration_k<64>(bt, P, s, h, use_cond);
+        default: return launch_iteration_k<128>(bt, P, s, h, use_cond);
     }
 }
 
@@ -1099,7 +1109,8 @@ void launch_finish(apxb_batch* bt, const bp& P, double* X, bool resid, cudaStrea
         case 8: launch_finish_k<8>(bt, P, X, resid, s); break;
         case 16: launch_finish_k<16>(bt, P, X, resid, s); break;
         case 32: launch_finish_k<32>(bt, P, X, resid, s); break;
-        default: launch_finish_k<64>(bt, P, X, resid, s); break;
+        case 64: launch_finish_k<64>(bt, P, X, resid, s); break;
+        default: launch_finish_k<128>(bt, P, X, resid, s); break;
     }
 }
 
@@ -1116,7 +1127,8 @@ void launch_admit(apxb_batch* bt, const bp& P, const double* B, cudaStream_t s) 
         case 8: launch_admit_k<8>(bt, P, B, s); break;
         case 16: launch_admit_k<16>(bt, P, B, s); break;
         case 32: launch_admit_k<32>(bt, P, B, s); break;
-        default: launch_admit_k<64>(bt, P, B, s); break;
+        case 64: launch_admit_k<64>(bt, P, B, s); break;
+        default: launch_admit_k<128>(bt, P, B, s); break;
     }
 }
 
@@ -1191,7 +1203,8 @@ void slot_io(apxb_batch* bt, const bp& P, unsigned sl, const double* in, double*
         case 8: slot_io_k<8>(bt, P, sl, in, out, s); break;
         case 16: slot_io_k<16>(bt, P, sl, in, out, s); break;
         case 32: slot_io_k<32>(bt, P, sl, in, out, s); break;
-        default: slot_io_k<64>(bt, P, sl, in, out, s); break;
+        case 64: slot_io_k<64>(bt, P, sl, in, out, s); break;
+        default: slot_io_k<128>(bt, P, sl, in, out, s); break;
     }
 }
 
@@ -1211,8 +1224,8 @@ int apxb_batch_create(apxb_engine* e, int n_inst, apxb_factor* const* factors, a
                       apxb_batch** out) {
     return guarded([&]() -> int {
         if (!e || n_inst < 1 || !factors || !ops || !out) return fail(APXB_ERR_INVALID, "bad argument");
-        if (k != 1 && k != 2 && k != 4 && k != 8 && k != 16 && k != 32 && k != 64)
-            return fail(APXB_ERR_INVALID, "k must be 1, 2, 4, 8, 16, 32 or 64");
+        if (k != 1 && k != 2 && k != 4 && k != 8 && k != 16 && k != 32 && k != 64 && k != 128)
+            return fail(APXB_ERR_INVALID, "k must be 1, 2, 4, 8, 16, 32, 64 or 128");
         *out = nullptr;
         APXB_CK(cudaSetDevice(e->device));
         std::unique_ptr<apxb_batch> bt(new (std::nothrow) apxb_batch);
@@ -1583,8 +1596,8 @@ int apxb_batch_plan_host(uint32_t n, const uint32_t* colptr, const uint32_t* row
                          int k, uint32_t* n_items, uint32_t* n_chunks) {
     return guarded([&]() -> int {
         if (!colptr || !rowidx || !vals || !perm || !n_items || !n_chunks) return fail(APXB_ERR_INVALID, "NULL argument");
-        if (k != 1 && k != 2 && k != 4 && k != 8 && k != 16 && k != 32 && k != 64)
-            return fail(APXB_ERR_INVALID, "k must be 1, 2, 4, 8, 16, 32 or 64");
+        if (k != 1 && k != 2 && k != 4 && k != 8 && k != 16 && k != 32 && k != 64 && k != 128)
+            return fail(APXB_ERR_INVALID, "k must be 1, 2, 4, 8, 16, 32, 64 or 128");
         apxb_factor f;
         const std::string why = apxb::prepare_factor(n, colptr, rowidx, vals, perm, sddm != 0, rounds, n_rounds,
                                                      drop_rel < 0.0 ? apxb::kDropRelDefault : drop_rel, f.h);

@@ -977,8 +977,8 @@ extern "C" int apxb_test_prep_compare(apxb_engine* e, uint32_t n, const uint32_t
     return guarded([&]() -> int {
         if (!e || !colptr || !rowidx || !vals || !perm || !rounds || n_rounds == 0)
             return fail(APXB_ERR_INVALID, "bad argument (the device path needs round sizes)");
-        if (k != 0 && k != 1 && k != 2 && k != 4 && k != 8 && k != 16 && k != 32 && k != 64)
-            return fail(APXB_ERR_INVALID, "k must be 0 or 1..64");
+        if (k != 0 && k != 1 && k != 2 && k != 4 && k != 8 && k != 16 && k != 32 && k != 64 && k != 128)
+            return fail(APXB_ERR_INVALID, "k must be 0 or 1..128");
         APXB_CK(cudaSetDevice(e->device));
         cudaStream_t s = e->stream;
         apxb::prepared_factor hf;

@@ -67,7 +67,7 @@ void launch_sweep32(int dir, const sweep_args<float>& a, int grid, cudaStream_t 
 // The same with the right-hand side read from fp64 (minus rhs_sub[s] when given).
 void launch_sweep32_from64(int dir, const sweep_args<float>& a, const double* in64, int grid, cudaStream_t s);
 // Batched fp32 sweep over a batch plan (column lanes, chunked claims), k in
-// {1, 2, 4, 8, 16, 32, 64}: a.k, a.chunk and a.n_chunks must be set; over
+// {1, 2, 4, 8, 16, 32, 64, 128}: a.k, a.chunk and a.n_chunks must be set; over
 // binary16 plan values when a.val16 is set (a.diag16 and, backward,
 // a.in_scale2 too).
 void launch_sweep32_batch(int dir, const sweep_args<float>& a, int grid, cudaStream_t s);

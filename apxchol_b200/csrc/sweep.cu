@@ -646,7 +646,7 @@ template <int K>
 struct wide_cfg {
     static constexpr int KC = K < 4 ? K : 4;   // columns per lane
     static constexpr int C = K / KC;           // column lanes per row
-    static constexpr int LC = C == 16 ? 4 : (C == 8 ? 3 : (C == 4 ? 2 : (C == 2 ? 1 : 0)));
+    static constexpr int LC = C == 32 ? 5 : (C == 16 ? 4 : (C == 8 ? 3 : (C == 4 ? 2 : (C == 2 ? 1 : 0))));
     static constexpr int B = 8;                // entries in flight per lane
 };
 
@@ -1068,7 +1068,8 @@ void launch_sweep32_batch(int dir, const sweep_args<float>& a, int grid, cudaStr
         case 8:  sweep32_batch_dir<8>(dir, a, grid, s); break;
         case 16: sweep32_batch_dir<16>(dir, a, grid, s); break;
         case 32: sweep32_batch_dir<32>(dir, a, grid, s); break;
-        default: sweep32_batch_dir<64>(dir, a, grid, s); break;
+        case 64: sweep32_batch_dir<64>(dir, a, grid, s); break;
+        default: sweep32_batch_dir<128>(dir, a, grid, s); break;
     }
 }
 
@@ -1088,7 +1089,8 @@ int sweep_grid32_batch(int k, int num_sms) {
         case 8: b = occ32_batch<8>(); break;
         case 16: b = occ32_batch<16>(); break;
         case 32: b = occ32_batch<32>(); break;
-        default: b = occ32_batch<64>(); break;
+        case 64: b = occ32_batch<64>(); break;
+        default: b = occ32_batch<128>(); break;
     }
     return (b > 0 ? b : 1) * num_sms;
 }

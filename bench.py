@@ -651,7 +651,7 @@ def run_rmat22(args, rank, world, local_rank):
     eng = native.Engine(local_rank)
     D32 = native.DeviceFactor(eng, F, precision=native.PREC_FP32)
     Op = native.DeviceOperator(eng, A, F.perm)
-    ch = autotune.tune(eng, D32, Op, rhs, tol=TOL, max_iter=MAX_ITER, ks=(1, 4, 8, 16, 32, 64), grids=(0,), log=log)
+    ch = autotune.tune(eng, D32, Op, rhs, tol=TOL, max_iter=MAX_ITER, ks=(1, 4, 8, 16, 32, 64, 128), grids=(0,), log=log)
     k = ch.k
     bt = native.Batch(eng, [D32], [Op], k)
     B = np.stack([rhs(c) for c in range(k)])

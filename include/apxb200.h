@@ -238,7 +238,7 @@ int apxb_pcg(apxb_engine* e, apxb_factor* f, apxb_operator* a, const double* b, 
 /* ---- batched solves: mixed precision, many right-hand sides, uneven instances ----
  * A batch binds S instances (factor + operator pairs of any sizes, solved as
  * one block-diagonal system in a single set of launches) and k right-hand-side
- * slots per instance (k = 1, 2, 4, 8, 16, 32 or 64). The preconditioner runs fp32
+ * slots per instance (k = 1, 2, 4, 8, 16, 32, 64 or 128). The preconditioner runs fp32
  * sweeps with fp32 accumulation; SpMV, residuals, dots and centring are fp64.
  * Each slot is an independent PCG with the semantics of apxb_pcg. No
  * counterpart in the reference (its GPU PCG solves one right-hand side). */

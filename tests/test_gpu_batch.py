@@ -30,7 +30,7 @@ def _objs(eng, name):
     return A, F, native.DeviceFactor(eng, F, precision=native.PREC_FP32), native.DeviceOperator(eng, A, F.perm)
 
 
-@pytest.mark.parametrize("k", [1, 4, 16, 32, 64])
+@pytest.mark.parametrize("k", [1, 4, 16, 32, 64, 128])
 def test_single_instance_multi_rhs(eng, k):
     A, F, D, Op = _objs(eng, "grid3d_24")
     bt = native.Batch(eng, [D], [Op], k)
