@@ -104,7 +104,7 @@ def test_threaded_preparation_matches_serial(name, monkeypatch):
 
 
 @pytest.mark.parametrize("name", ["grid2d_64", "grid3d_24", "rmat_12", "regular_3000", "path_200"])
-@pytest.mark.parametrize("k", [1, 4, 8, 16])
+@pytest.mark.parametrize("k", [1, 4, 8, 16, 32, 64, 128])
 def test_batch_plans_hold_their_invariants(name, k):
     """The batch sweep plans (column lanes, oldest-dependency-first entries,
     chunked claims) pass the same checks apxb_batch_create runs: every row once, items within one level in level order, every
