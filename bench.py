@@ -6,6 +6,7 @@ and the SpTRSV sweeps' HBM GB/s.
                     [--workload grid3d_128|rmat_22|instances_256|serving_8]
                     [--k K [--lanes L] [--sweep-grid B]] [--grid G]
                     [--no-serving] [--no-serving-mix] [--no-plain] [--no-cpu-baseline]
+                    [--storage fp32|fp16] [--serve-k K] [--serve-load F] [--mix-k K]
 
 Our arm. The headline is the batched mixed-precision form: one step is one
 batched PCG solve of k right-hand sides, with fp32 factor sweeps and fp64
@@ -557,9 +558,9 @@ def run_ours(args, rank, world, local_rank):
     mix = None
     if not args.no_serving_mix and rank == 0:
         try:   # the 8-matrix serving workload beside the headline (reported in its field)
-            rates, resident_gb = serving_mix(local_rank)
+            rates, resident_gb = serving_mix(local_rank, k=args.mix_k)
             mix = {"workload": "serving_8: 8 matrices (2 x 2D grid 1024^2, 2 x 3D grid 96^3, 2 x R-MAT scale 20 "
-                               "LCC, 2 x random 6-regular n=500k), Poisson arrivals, 60 GB budget, k=8",
+                               f"LCC, 2 x random 6-regular n=500k), Poisson arrivals, 60 GB budget, k={args.mix_k}",
                    "rates": rates, "resident_gb": resident_gb}
         except Exception as ex:
             mix = {"error": f"{type(ex).__name__}: {ex}"}
@@ -761,16 +762,16 @@ def run_instances256(args, rank, world, local_rank):
     return 0
 
 
-def serving_mix(device, sweep_grid=None, log_fn=log):
+def serving_mix(device, sweep_grid=None, log_fn=log, k: int = 8):
     """The 8-matrix serving workload (C5): 8 registered matrices, 6 resident at
     the start, open-loop Poisson requests at 50 / 200 / 800 req/s (matrix
     uniform, tolerance from {1e-6, 1e-8, 1e-10}, >= 1000 requests per rate);
     the two matrices not resident are admitted when their first request
-    arrives, under a 60 GB budget. Returns (rates, resident GB)."""
+    arrives, under a 60 GB budget; k slots per resident matrix. Returns (rates, resident GB)."""
     from apxchol_b200 import gen, workloads
     from apxchol_b200.serve import SolveServer, latency_stats
     mats = workloads.serving_8(log_fn)
-    srv = SolveServer(device=device, budget_bytes=60 * 10**9, k=8, iters_per_step=2, sweep_grid=sweep_grid or None)
+    srv = SolveServer(device=device, budget_bytes=60 * 10**9, k=k, iters_per_step=2, sweep_grid=sweep_grid or None)
     rates = []
     try:
         for name, A, F in mats:
@@ -812,11 +813,11 @@ def run_serving8(args, rank, world, local_rank):
     only when their first request arrives (60 GB budget)."""
     import torch
     torch.cuda.set_device(local_rank)
-    rates, resident_gb = serving_mix(local_rank, args.sweep_grid)
+    rates, resident_gb = serving_mix(local_rank, args.sweep_grid, k=args.mix_k)
     line = {"metric": METRIC, "value": rates[-1]["solves_s"], "unit": "solves/s", "n_gpus": world, "steps": len(rates),
             "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 sweeps / f64 outer", "data": "synthetic (seeded generator)",
-            "config": {"workload": "serving_8: 8 matrices, Poisson arrivals", "k": 8, "budget_gb": 60,
+            "config": {"workload": "serving_8: 8 matrices, Poisson arrivals", "k": args.mix_k, "budget_gb": 60,
                        "sweep_grid": args.sweep_grid or "auto (resident grid / 4)",
                        "resident_gb": resident_gb},
             "serving": rates}
@@ -836,6 +837,7 @@ def main():
     ap.add_argument("--lanes", type=int, default=1, help="concurrent batches (streams) with --k")
     ap.add_argument("--iters-per-step", type=int, default=2, help="serving: iterations per server step")
     ap.add_argument("--serve-requests", type=int, default=1000)
+    ap.add_argument("--mix-k", type=int, default=8, help="serving mix: slots per resident matrix")
     ap.add_argument("--storage", choices=["fp32", "fp16"], default="fp32",
                     help="batched factor storage: fp32 values, or the reference GPU default fp16 (column-scaled)")
     ap.add_argument("--serve-k", type=int, default=16,
