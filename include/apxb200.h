@@ -207,9 +207,10 @@ int apxb_apply(apxb_engine* e, apxb_factor* f, const double* b, double* z, int f
  * replacement header apxchol/solver/sptrsv/cuda_dataflow.h (include/apxchol_compat).
  * They report nothing themselves (the reference's return void): a launch whose
  * wait made no progress for one second (a plan or epoch that breaks the
- * contract) stops and records it. apxb_dataflow_status returns that record
- * (APXB_ERR_TIMEOUT or APXB_ERR_INVALID with apxb_last_error set, else APXB_OK)
- * and clears it; it synchronizes with the device. */
+ * contract) stops and records it, once per device. apxb_dataflow_status
+ * returns the current device's record (APXB_ERR_TIMEOUT or APXB_ERR_INVALID
+ * with apxb_last_error set, else APXB_OK) and clears it; it synchronizes with
+ * that device. */
 int apxb_dataflow_status(void);
 
 /* ---- operator: A in the factor's permuted ordering (cuda_pcg::setup, pcg_cuda.h:68-152) ----
