@@ -142,6 +142,28 @@ __device__ __forceinline__ void col_store(double (&a)[NV][2], double* dst) {
         }                                                                                      \
     }
 
+// The same walk for K >= 2 (the tile's [row][K] block starts and ends on an
+// even element, so every access is a pair), kU pairs per thread per step: the
+// step's loads are all issued (LOAD, for pair j at q = q_[j] while ok_[j])
+// before its arithmetic and stores (the rest, in the walk's order, so every sum
+// runs in the same order as FLAT_PAIRS).
+constexpr int kU = 4;
+#define FLAT_PAIRS_U(t, LOAD, ...)                                                           \
+    {                                                                                          \
+        const size_t lo_ = static_cast<size_t>(P.tile_lo[t]) * K;                             \
+        const size_t end_ = static_cast<size_t>(P.tile_hi[t]) * K;                            \
+        for (size_t s_ = lo_ + 2 * threadIdx.x; s_ < end_; s_ += 2 * kBT * kU) {             \
+            size_t q_[kU];                                                                     \
+            bool ok_[kU];                                                                      \
+            _Pragma("unroll") for (int j = 0; j < kU; ++j) {                                  \
+                q_[j] = s_ + static_cast<size_t>(j) * 2 * kBT;                                 \
+                ok_[j] = q_[j] < end_;                                                         \
+            }                                                                                  \
+            _Pragma("unroll") for (int j = 0; j < kU; ++j) if (ok_[j]) { const size_t q = q_[j]; LOAD } \
+            _Pragma("unroll") for (int j = 0; j < kU; ++j) if (ok_[j]) { const size_t q = q_[j]; (void)q; __VA_ARGS__ } \
+        }                                                                                      \
+    }
+
 // fp32-stored operator values widened into a combined fp64 array.
 __global__ void __launch_bounds__(kBT) k_b_widen(const float* src, double* dst, uint64_t n) {
     for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
@@ -455,6 +477,27 @@ __global__ void __launch_bounds__(kBT) k_b_xr(bp P) {
         const double a0 = P.xa[s0], a1 = P.xa[s1];
         const bool w0 = !centres_next(P, i, s0), w1 = !centres_next(P, i, s1);
         double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+        if constexpr (K >= 2) {
+            double2 rv[kU], av[kU];
+            FLAT_PAIRS_U(t, {
+                rv[j] = *reinterpret_cast<const double2*>(P.r + q);
+                av[j] = *reinterpret_cast<const double2*>(P.Ap + q);
+            }, {
+                double2 r = rv[j];
+                r.x = fma(-a0, av[j].x, r.x); r.y = fma(-a1, av[j].y, r.y);
+                *reinterpret_cast<double2*>(P.r + q) = r;
+                if (w0 && w1) {
+                    *reinterpret_cast<float2*>(P.rhs32 + q) = make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
+                } else {
+                    if (w0) P.rhs32[q] = static_cast<float>(r.x);
+                    if (w1) P.rhs32[q + 1] = static_cast<float>(r.y);
+                }
+                acc[0][0] = fma(r.x, r.x, acc[0][0]); acc[0][1] = fma(r.y, r.y, acc[0][1]);
+                acc[1][0] += r.x; acc[1][1] += r.y;
+            })
+            col_store<K, 2>(acc, P.partials + static_cast<size_t>(t) * K * 2);
+            continue;
+        }
         FLAT_PAIRS(t, {
             if (two) {
                 double2 r = *reinterpret_cast<const double2*>(P.r + q);
@@ -534,6 +577,19 @@ __global__ void __launch_bounds__(kBT) k_b_rz(bp P) {
         const unsigned i = P.tile_inst[t];
         const double h0 = P.shift[i * K + c0], h1 = P.shift[i * K + c1];
         double acc[1][2] = {{0.0, 0.0}};
+        if constexpr (K >= 2) {
+            double2 rv[kU];
+            float2 zv[kU];
+            FLAT_PAIRS_U(t, {
+                rv[j] = *reinterpret_cast<const double2*>(P.r + q);
+                zv[j] = *reinterpret_cast<const float2*>(P.z + q);
+            }, {
+                acc[0][0] = fma(rv[j].x, static_cast<double>(zv[j].x) - h0, acc[0][0]);
+                acc[0][1] = fma(rv[j].y, static_cast<double>(zv[j].y) - h1, acc[0][1]);
+            })
+            col_store<K, 1>(acc, P.partials + static_cast<size_t>(t) * K * 2);
+            continue;
+        }
         FLAT_PAIRS(t, {
             if (two) {
                 const double2 r = *reinterpret_cast<const double2*>(P.r + q);
@@ -569,6 +625,29 @@ __global__ void __launch_bounds__(kBT) k_b_up(bp P, unsigned long long handle, i
         if (!l0 && !l1 && !xs) continue;
         const double h0 = P.shift[s0], h1 = P.shift[s1], b0 = P.beta[s0], b1 = P.beta[s1];
         const bool cp0 = P.pmode[s0] == 1, cp1 = P.pmode[s1] == 1;
+        if constexpr (K >= 2) {
+            double2 pv[kU], xv[kU];
+            float2 zv[kU];
+            FLAT_PAIRS_U(t, {
+                pv[j] = *reinterpret_cast<const double2*>(P.p + q);
+                if (xs) xv[j] = *reinterpret_cast<const double2*>(P.x + q);
+                if (l0 || l1) zv[j] = *reinterpret_cast<const float2*>(P.z + q);
+            }, {
+                double2 p = pv[j];
+                if (xs) {
+                    double2 x = xv[j];
+                    x.x = fma(xa0, p.x, x.x); x.y = fma(xa1, p.y, x.y);
+                    *reinterpret_cast<double2*>(P.x + q) = x;
+                }
+                if (l0 || l1) {
+                    const double z0 = static_cast<double>(zv[j].x) - h0, z1 = static_cast<double>(zv[j].y) - h1;
+                    if (l0) p.x = cp0 ? z0 : fma(b0, p.x, z0);
+                    if (l1) p.y = cp1 ? z1 : fma(b1, p.y, z1);
+                    *reinterpret_cast<double2*>(P.p + q) = p;
+                }
+            })
+            continue;
+        }
         FLAT_PAIRS(t, {
             if (two) {
                 double2 p = *reinterpret_cast<const double2*>(P.p + q);
